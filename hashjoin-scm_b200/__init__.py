@@ -1,0 +1,300 @@
+"""Python binding of libhjscm, the B200 equi-join hot path (C ABI in include/hjscm.h).
+
+The library is the product; this module only loads it with ctypes and converts arguments. A join
+takes two relations of 16-byte tuples {uint64 key, uint64 row_id} - numpy arrays of shape (n, 2) and
+dtype uint64 on the host, or CUDA tensors / raw device pointers - and returns the reference's two
+result values (match count, wrapping 64-bit checksum of r.row_id + s.row_id) with phase times.
+
+The directory name contains a hyphen, so the package is loaded by path:
+    spec = importlib.util.spec_from_file_location("hashjoin_scm_b200", ".../hashjoin-scm_b200/__init__.py")
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "lib" / "libhjscm.so"
+MAIN_PATH = HERE / "bin" / "hj_main"
+
+ALGOS = {
+    "nphj_sc": 0,
+    "nphj_lp": 1,
+    "phj_radix_bc": 2,
+    "phj_radix_lp": 3,
+    # bandwidth-regulated aliases compute the same results (src/algo/phj_bw_reg.c:2874-2893)
+    "phj_radix_bw_reg_bc": 2,
+    "phj_radix_bw_reg_lp": 3,
+}
+
+STATUS = {
+    0: "HJ_OK",
+    1: "HJ_E_INVAL",
+    2: "HJ_E_OOM",
+    3: "HJ_E_DEVICE",
+    4: "HJ_E_PROBE_LIMIT",
+    5: "HJ_E_TIMEOUT",
+    6: "HJ_E_NOT_FOUND",
+    7: "HJ_E_IO",
+    8: "HJ_E_OVERFLOW",
+    9: "HJ_E_BUDGET",
+}
+HJ_OK, HJ_E_INVAL, HJ_E_OOM, HJ_E_DEVICE, HJ_E_PROBE_LIMIT, HJ_E_TIMEOUT = 0, 1, 2, 3, 4, 5
+HJ_E_NOT_FOUND, HJ_E_IO, HJ_E_OVERFLOW, HJ_E_BUDGET = 6, 7, 8, 9
+
+HJ_F_NO_TIMING = 0x1
+HJ_F_PINNED_HOST = 0x2
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("num_radix_bits", ctypes.c_int),
+        ("num_passes", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("inputs_on_device", ctypes.c_int),
+        ("stream", ctypes.c_void_p),
+        ("flags", ctypes.c_uint32),
+        ("table_load", ctypes.c_double),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("matched_cnt", ctypes.c_uint64),
+        ("checksum", ctypes.c_uint64),
+        ("buildpart", ctypes.c_double),
+        ("probejoin", ctypes.c_double),
+        ("total", ctypes.c_double),
+        ("h2d", ctypes.c_double),
+        ("status", ctypes.c_int),
+        ("physical_passes", ctypes.c_int),
+        ("large_partitions", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class JoinError(RuntimeError):
+    def __init__(self, status: int, what: str = "join"):
+        super().__init__(f"{what} failed: {STATUS.get(status, status)}")
+        self.status = status
+
+
+_lib = None
+
+
+def build(quiet: bool = True) -> None:
+    """Compile libhjscm.so and hj_main in-tree (make, nvcc for sm_100a)."""
+    out = subprocess.run(["make", "-C", str(HERE), "-j8"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("libhjscm build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
+    if not quiet:
+        print(out.stdout)
+
+
+def lib() -> ctypes.CDLL:
+    """Load libhjscm.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run build() (make -C hashjoin-scm_b200)")
+    L = ctypes.CDLL(str(LIB_PATH))
+    u64, sz, vp, i32 = ctypes.c_uint64, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int
+    L.hj_params_init.argtypes = [ctypes.POINTER(Params)]
+    L.hj_params_init.restype = None
+    L.hj_status_str.argtypes = [i32]
+    L.hj_status_str.restype = ctypes.c_char_p
+    L.hj_algo_from_name.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    L.hj_algo_from_name.restype = i32
+    L.hj_algo_name.argtypes = [i32]
+    L.hj_algo_name.restype = ctypes.c_char_p
+    L.hj_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
+    L.hj_ctx_create.restype = i32
+    L.hj_ctx_destroy.argtypes = [vp]
+    L.hj_ctx_destroy.restype = i32
+    L.hj_ctx_reserve.argtypes = [vp, i32, ctypes.POINTER(Params), sz, sz]
+    L.hj_ctx_reserve.restype = i32
+    L.hj_ctx_scratch_bytes.argtypes = [vp]
+    L.hj_ctx_scratch_bytes.restype = sz
+    L.hj_join_ctx.argtypes = [vp, i32, ctypes.POINTER(Params), vp, sz, vp, sz, ctypes.POINTER(Result)]
+    L.hj_join_ctx.restype = i32
+    L.hj_join.argtypes = [i32, ctypes.POINTER(Params), vp, sz, vp, sz, ctypes.POINTER(Result)]
+    L.hj_join.restype = i32
+    L.hj_gen_pkfk_uniform.argtypes = [sz, sz, ctypes.c_uint, i32, vp, vp]
+    L.hj_gen_pkfk_uniform.restype = i32
+    L.hj_gen_dup_uniform.argtypes = [sz, sz, ctypes.c_uint, vp, vp]
+    L.hj_gen_dup_uniform.restype = i32
+    L.hj_gen_zipf.argtypes = [sz, sz, ctypes.c_double, ctypes.c_uint, vp]
+    L.hj_gen_zipf.restype = i32
+    L.hj_gen_fast_host.argtypes = [sz, sz, u64, i32, ctypes.c_uint, i32, vp, vp]
+    L.hj_gen_fast_host.restype = i32
+    L.hj_gen_fast_device.argtypes = [sz, sz, u64, i32, ctypes.c_uint, vp, vp, vp]
+    L.hj_gen_fast_device.restype = i32
+    L.hj_gen_zipf_device.argtypes = [sz, sz, ctypes.c_double, u64, vp, vp]
+    L.hj_gen_zipf_device.restype = i32
+    L.hj_pkfk_closed_form.argtypes = [sz, sz, ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.hj_pkfk_closed_form.restype = None
+    L.hj_load_bin.argtypes = [ctypes.c_char_p, sz, vp]
+    L.hj_load_bin.restype = i32
+    L.hj_store_bin.argtypes = [ctypes.c_char_p, sz, vp]
+    L.hj_store_bin.restype = i32
+    _lib = L
+    return L
+
+
+def _ptr_len(rel, on_device: bool):
+    """(pointer, tuple count) of a relation: numpy (n, 2) uint64, a CUDA tensor, or (ptr, n)."""
+    if isinstance(rel, tuple):
+        return int(rel[0]), int(rel[1])
+    if on_device:
+        # torch tensor of shape (n, 2) int64/uint64 on the GPU
+        assert rel.is_cuda and rel.is_contiguous() and rel.element_size() == 8
+        return int(rel.data_ptr()), int(rel.numel() // 2)
+    arr = np.ascontiguousarray(rel)
+    assert arr.dtype == np.uint64 and arr.ndim == 2 and arr.shape[1] == 2, "relations are (n, 2) uint64"
+    return arr.ctypes.data, arr.shape[0]
+
+
+def make_params(bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
+                stream: int | None = None, flags: int = 0, load: float = 0.5) -> Params:
+    p = Params()
+    lib().hj_params_init(ctypes.byref(p))
+    p.num_radix_bits, p.num_passes, p.device = bits, passes, device
+    p.inputs_on_device = 1 if on_device else 0
+    p.stream = stream or None
+    p.flags = flags
+    p.table_load = load
+    return p
+
+
+def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
+         stream: int | None = None, flags: int = 0, load: float = 0.5, ctx: "Context | None" = None,
+         check: bool = True) -> Result:
+    """Run one join (synchronous). Raises JoinError on a non-zero status when check is set."""
+    L = lib()
+    a = ALGOS[algo]
+    p = make_params(bits, passes, device, on_device, stream, flags, load)
+    pr, nr = _ptr_len(R, on_device)
+    ps, ns = _ptr_len(S, on_device)
+    res = Result()
+    if ctx is not None:
+        rc = L.hj_join_ctx(ctx.handle, a, ctypes.byref(p), pr, nr, ps, ns, ctypes.byref(res))
+    else:
+        rc = L.hj_join(a, ctypes.byref(p), pr, nr, ps, ns, ctypes.byref(res))
+    if check and rc != 0:
+        raise JoinError(rc, algo)
+    res.status = rc
+    return res
+
+
+class Context:
+    """A library context: own stream, events and device scratch arena (hj_ctx_t)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        rc = lib().hj_ctx_create(device, ctypes.byref(h))
+        if rc:
+            raise JoinError(rc, "hj_ctx_create")
+        self.handle = h
+        self.device = device
+
+    def reserve(self, algo: str, nR: int, nS: int, **kw) -> None:
+        p = make_params(device=self.device, **kw)
+        rc = lib().hj_ctx_reserve(self.handle, ALGOS[algo], ctypes.byref(p), nR, nS)
+        if rc:
+            raise JoinError(rc, "hj_ctx_reserve")
+
+    def scratch_bytes(self) -> int:
+        return lib().hj_ctx_scratch_bytes(self.handle)
+
+    def close(self) -> None:
+        if self.handle:
+            lib().hj_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def empty_relation(n: int) -> np.ndarray:
+    return np.zeros((n, 2), dtype=np.uint64)
+
+
+def gen_pkfk_uniform(nR: int, nS: int, seed: int = 12345, payload: bool = False):
+    """Exact replay of the reference's gen_pkfk_uniform / payload_gen_pkfk_uniform (src/gen.c)."""
+    R, S = empty_relation(nR), empty_relation(nS)
+    rc = lib().hj_gen_pkfk_uniform(nR, nS, seed, 1 if payload else 0, R.ctypes.data, S.ctypes.data)
+    if rc:
+        raise JoinError(rc, "hj_gen_pkfk_uniform")
+    return R, S
+
+
+def gen_dup_uniform(nR: int, nS: int, seed: int = 12345):
+    """Exact replay of the reference's gen_dup_uniform (src/gen.c:286-331)."""
+    R, S = empty_relation(nR), empty_relation(nS)
+    rc = lib().hj_gen_dup_uniform(nR, nS, seed, R.ctypes.data, S.ctypes.data)
+    if rc:
+        raise JoinError(rc, "hj_gen_dup_uniform")
+    return R, S
+
+
+def gen_zipf(nS: int, nR: int, factor: float, seed: int = 12345):
+    """Exact replay of the reference's gen_zipf (src/inc/eth_genzipf.c:97-147) with the given factor."""
+    S = empty_relation(nS)
+    rc = lib().hj_gen_zipf(nS, nR, factor, seed, S.ctypes.data)
+    if rc:
+        raise JoinError(rc, "hj_gen_zipf")
+    return S
+
+
+def gen_fast_host(nR: int, nS: int, seed: int = 12345, payload: bool = False, dup: int = 1, threads: int = 0):
+    R, S = empty_relation(nR), empty_relation(nS)
+    rc = lib().hj_gen_fast_host(nR, nS, seed, 1 if payload else 0, dup, threads, R.ctypes.data, S.ctypes.data)
+    if rc:
+        raise JoinError(rc, "hj_gen_fast_host")
+    return R, S
+
+
+def gen_fast_device(nR: int, nS: int, R_ptr: int, S_ptr: int, seed: int = 12345, payload: bool = False,
+                    dup: int = 1, stream: int | None = None) -> None:
+    rc = lib().hj_gen_fast_device(nR, nS, seed, 1 if payload else 0, dup, R_ptr, S_ptr, stream or None)
+    if rc:
+        raise JoinError(rc, "hj_gen_fast_device")
+
+
+def gen_zipf_device(nS: int, nR: int, factor: float, S_ptr: int, seed: int = 12345,
+                    stream: int | None = None) -> None:
+    rc = lib().hj_gen_zipf_device(nS, nR, factor, seed, S_ptr, stream or None)
+    if rc:
+        raise JoinError(rc, "hj_gen_zipf_device")
+
+
+def pkfk_closed_form(nR: int, nS: int) -> tuple[int, int]:
+    m, c = ctypes.c_uint64(), ctypes.c_uint64()
+    lib().hj_pkfk_closed_form(nR, nS, ctypes.byref(m), ctypes.byref(c))
+    return m.value, c.value
+
+
+def header_functions() -> list[str]:
+    """Names of every function declared in include/*.h (for export checks)."""
+    import re
+
+    names = []
+    inc = HERE.parent / "include"
+    for h in sorted(inc.glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\)\s*;", text, flags=re.M):
+            name = m.group(1)
+            if name not in ("if", "while", "for", "return", "sizeof"):
+                names.append(name)
+    return sorted(set(names))

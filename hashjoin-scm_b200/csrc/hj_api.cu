@@ -1,0 +1,311 @@
+// hj_api.cu - the C ABI: contexts, scratch arena, and the synchronous join entry points.
+//
+// The reference's join_init_run (src/algo/phj.c:1875-2512) and nphj_sc/nphj_lp
+// (src/algo/nphj.c:677-1037, 1487-...) each allocate their buffers, spawn thread pools, join and free
+// everything per call. Here a context keeps a stream, events and a grow-only device arena; a join
+// carves its scratch out of the arena and enqueues the whole kernel pipeline on one stream, reading
+// back only the 64-byte accumulator at the end.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "hj_common.cuh"
+#include "hj_internal.h"
+
+using hj::JoinAccum;
+
+struct hj_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_h2d = nullptr, ev_start = nullptr, ev_mid = nullptr, ev_end = nullptr;
+    char *arena = nullptr;
+    size_t arena_bytes = 0;
+    JoinAccum *acc_host = nullptr;  // pinned
+    std::mutex mu;
+};
+
+#define CU_OR(call, code)                                                                   \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            fprintf(stderr, "hjscm: %s failed: %s\n", #call, cudaGetErrorString(e_));       \
+            return (code);                                                                  \
+        }                                                                                   \
+    } while (0)
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+std::mutex g_default_mu;
+hj_ctx *g_default[64] = {};
+
+constexpr size_t kAccBytes = 256;
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+void resolve_params(const hj_params_t *p, hj_params_t *out) {
+    hj_params_init(out);
+    if (p) *out = *p;
+    if (out->num_radix_bits == 0) out->num_radix_bits = 14;
+    if (out->num_passes == 0) out->num_passes = 2;
+    if (!(out->table_load > 0.0)) out->table_load = 0.5;
+}
+
+bool is_phj(hj_algo_t a) { return a == HJ_ALGO_PHJ_RADIX_BC || a == HJ_ALGO_PHJ_RADIX_LP; }
+
+int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, bool host_inputs,
+                 size_t *bytes) {
+    size_t need = kAccBytes;
+    if (host_inputs) need += align256(nR * 16) + align256(nS * 16);
+    if (is_phj(algo)) {
+        hj::RadixGeom g;
+        int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &g);
+        if (rc) return rc;
+        need += hj::phj_scratch_bytes(g, nR, nS);
+    } else {
+        need += align256(hj::nphj_scratch_bytes(nR, p.table_load));
+    }
+    *bytes = need;
+    return HJ_OK;
+}
+
+int ensure_arena(hj_ctx *c, size_t bytes) {
+    if (c->arena_bytes >= bytes) return HJ_OK;
+    CU_OR(cudaStreamSynchronize(c->stream), HJ_E_DEVICE);
+    if (c->arena) cudaFree(c->arena);
+    c->arena = nullptr;
+    c->arena_bytes = 0;
+    if (cudaMalloc(&c->arena, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        c->arena = nullptr;
+        return HJ_E_OOM;
+    }
+    c->arena_bytes = bytes;
+    return HJ_OK;
+}
+
+int map_error_bits(unsigned bits) {
+    if (!bits) return HJ_OK;
+    if (bits & hj::kErrSpinLimit) return HJ_E_TIMEOUT;
+    if (bits & hj::kErrProbeLimit) return HJ_E_PROBE_LIMIT;
+    return HJ_E_OVERFLOW;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hj_params_init(hj_params_t *p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->num_radix_bits = 14;
+    p->num_passes = 2;
+    p->table_load = 0.5;
+}
+
+const char *hj_status_str(int s) {
+    switch (s) {
+        case HJ_OK: return "ok";
+        case HJ_E_INVAL: return "invalid argument";
+        case HJ_E_OOM: return "out of memory";
+        case HJ_E_DEVICE: return "CUDA error";
+        case HJ_E_PROBE_LIMIT: return "table walk exceeded capacity";
+        case HJ_E_TIMEOUT: return "bounded wait gave up";
+        case HJ_E_NOT_FOUND: return "unknown algorithm";
+        case HJ_E_IO: return "i/o error";
+        case HJ_E_OVERFLOW: return "device bound check fired";
+        case HJ_E_BUDGET: return "over the HBM budget";
+        default: return "unknown status";
+    }
+}
+
+static const char *const k_algo_names[HJ_ALGO_COUNT] = {"nphj_sc", "nphj_lp", "phj_radix_bc", "phj_radix_lp"};
+
+const char *hj_algo_name(hj_algo_t a) {
+    return ((int)a >= 0 && a < HJ_ALGO_COUNT) ? k_algo_names[a] : "?";
+}
+
+int hj_algo_from_name(const char *name, hj_algo_t *algo) {
+    if (!name || !algo) return HJ_E_INVAL;
+    for (int i = 0; i < HJ_ALGO_COUNT; i++)
+        if (strcmp(name, k_algo_names[i]) == 0) {
+            *algo = (hj_algo_t)i;
+            return HJ_OK;
+        }
+    // Bandwidth-regulated variants compute identical results (src/algo/phj_bw_reg.c:2874-2893).
+    if (strcmp(name, "phj_radix_bw_reg_bc") == 0) {
+        *algo = HJ_ALGO_PHJ_RADIX_BC;
+        return HJ_OK;
+    }
+    if (strcmp(name, "phj_radix_bw_reg_lp") == 0) {
+        *algo = HJ_ALGO_PHJ_RADIX_LP;
+        return HJ_OK;
+    }
+    return HJ_E_NOT_FOUND;
+}
+
+int hj_ctx_create(int device, hj_ctx_t **out) {
+    if (!out) return HJ_E_INVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return HJ_E_DEVICE;
+    }
+    DeviceGuard g(device);
+    hj_ctx *c = new hj_ctx();
+    c->device = device;
+    CU_OR(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), HJ_E_DEVICE);
+    CU_OR(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), HJ_E_DEVICE);
+    CU_OR(cudaEventCreate(&c->ev_h2d), HJ_E_DEVICE);
+    CU_OR(cudaEventCreate(&c->ev_start), HJ_E_DEVICE);
+    CU_OR(cudaEventCreate(&c->ev_mid), HJ_E_DEVICE);
+    CU_OR(cudaEventCreate(&c->ev_end), HJ_E_DEVICE);
+    CU_OR(cudaMallocHost(&c->acc_host, sizeof(JoinAccum)), HJ_E_OOM);
+    *out = c;
+    return HJ_OK;
+}
+
+int hj_ctx_destroy(hj_ctx_t *c) {
+    if (!c) return HJ_E_INVAL;
+    {
+        DeviceGuard g(c->device);
+        std::lock_guard<std::mutex> lk(c->mu);
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        if (c->arena) cudaFree(c->arena);
+        if (c->acc_host) cudaFreeHost(c->acc_host);
+        cudaEventDestroy(c->ev_h2d);
+        cudaEventDestroy(c->ev_start);
+        cudaEventDestroy(c->ev_mid);
+        cudaEventDestroy(c->ev_end);
+        if (c->stream) cudaStreamDestroy(c->stream);
+    }
+    delete c;
+    return HJ_OK;
+}
+
+size_t hj_ctx_scratch_bytes(const hj_ctx_t *c) { return c ? c->arena_bytes : 0; }
+
+int hj_ctx_reserve(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, size_t nR, size_t nS) {
+    if (!c || (int)algo < 0 || algo >= HJ_ALGO_COUNT) return HJ_E_INVAL;
+    hj_params_t p;
+    resolve_params(pin, &p);
+    size_t need = 0;
+    int rc = scratch_need(algo, p, nR, nS, !p.inputs_on_device, &need);
+    if (rc) return rc;
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    return ensure_arena(c, need);
+}
+
+int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tuple_t *R, size_t nR,
+                const hj_tuple_t *S, size_t nS, hj_result_t *out) {
+    if (!c || !out || (int)algo < 0 || algo >= HJ_ALGO_COUNT) return HJ_E_INVAL;
+    memset(out, 0, sizeof(*out));
+    if ((nR && !R) || (nS && !S)) return out->status = HJ_E_INVAL;
+    hj_params_t p;
+    resolve_params(pin, &p);
+    if (p.device != c->device) return out->status = HJ_E_INVAL;
+    hj::RadixGeom geom = {};
+    if (is_phj(algo)) {
+        int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &geom);
+        if (rc) return out->status = rc;
+        out->physical_passes = geom.passes;
+    }
+    if (nR == 0 || nS == 0) return out->status = HJ_OK;  // no join task (src/algo/phj.c:1290)
+
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    const bool host_in = !p.inputs_on_device;
+    size_t need = 0;
+    int rc = scratch_need(algo, p, nR, nS, host_in, &need);
+    if (rc) return out->status = rc;
+    rc = ensure_arena(c, need);
+    if (rc) return out->status = rc;
+    cudaStream_t st = p.stream ? (cudaStream_t)p.stream : c->stream;
+    const bool timing = !(p.flags & HJ_F_NO_TIMING);
+
+    char *cur = c->arena;
+    JoinAccum *acc = reinterpret_cast<JoinAccum *>(cur);
+    cur += kAccBytes;
+    const ulonglong2 *dR = reinterpret_cast<const ulonglong2 *>(R);
+    const ulonglong2 *dS = reinterpret_cast<const ulonglong2 *>(S);
+    if (host_in) {
+        ulonglong2 *r = reinterpret_cast<ulonglong2 *>(cur);
+        cur += align256(nR * 16);
+        ulonglong2 *s = reinterpret_cast<ulonglong2 *>(cur);
+        cur += align256(nS * 16);
+        if (timing) CU_OR(cudaEventRecord(c->ev_h2d, st), out->status = HJ_E_DEVICE);
+        CU_OR(cudaMemcpyAsync(r, R, nR * 16, cudaMemcpyHostToDevice, st), out->status = HJ_E_DEVICE);
+        CU_OR(cudaMemcpyAsync(s, S, nS * 16, cudaMemcpyHostToDevice, st), out->status = HJ_E_DEVICE);
+        dR = r;
+        dS = s;
+    }
+    CU_OR(cudaMemsetAsync(acc, 0, sizeof(JoinAccum), st), out->status = HJ_E_DEVICE);
+    if (timing) CU_OR(cudaEventRecord(c->ev_start, st), out->status = HJ_E_DEVICE);
+    if (is_phj(algo)) {
+        hj::PhjScratch s;
+        hj::phj_carve(geom, nR, nS, cur, &s);
+        rc = hj::phj_enqueue(geom, algo == HJ_ALGO_PHJ_RADIX_LP, dR, nR, dS, nS, s, acc, st,
+                             timing ? c->ev_mid : nullptr, c->num_sms);
+    } else {
+        const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
+        rc = hj::nphj_enqueue(algo == HJ_ALGO_NPHJ_LP, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
+                              timing ? c->ev_mid : nullptr, c->num_sms);
+    }
+    if (rc) {
+        cudaStreamSynchronize(st);
+        return out->status = rc;
+    }
+    if (timing) CU_OR(cudaEventRecord(c->ev_end, st), out->status = HJ_E_DEVICE);
+    CU_OR(cudaMemcpyAsync(c->acc_host, acc, sizeof(JoinAccum), cudaMemcpyDeviceToHost, st),
+          out->status = HJ_E_DEVICE);
+    CU_OR(cudaStreamSynchronize(st), out->status = HJ_E_DEVICE);
+    out->matched_cnt = c->acc_host->matched;
+    out->checksum = c->acc_host->checksum;
+    out->large_partitions = c->acc_host->large_parts;
+    if (timing) {
+        float a = 0, b = 0, h = 0;
+        cudaEventElapsedTime(&a, c->ev_start, c->ev_mid);
+        cudaEventElapsedTime(&b, c->ev_mid, c->ev_end);
+        if (host_in) cudaEventElapsedTime(&h, c->ev_h2d, c->ev_start);
+        out->buildpart = a * 1e-3;
+        out->probejoin = b * 1e-3;
+        out->total = out->buildpart + out->probejoin;
+        out->h2d = h * 1e-3;
+    }
+    out->status = map_error_bits(c->acc_host->error);
+    return out->status;
+}
+
+int hj_join(hj_algo_t algo, const hj_params_t *pin, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,
+            size_t nS, hj_result_t *out) {
+    hj_params_t p;
+    resolve_params(pin, &p);
+    if (p.device < 0 || p.device >= 64) return HJ_E_INVAL;
+    hj_ctx *c;
+    {
+        std::lock_guard<std::mutex> lk(g_default_mu);
+        if (!g_default[p.device]) {
+            int rc = hj_ctx_create(p.device, &g_default[p.device]);
+            if (rc) return rc;
+        }
+        c = g_default[p.device];
+    }
+    return hj_join_ctx(c, algo, &p, R, nR, S, nS, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// hj_internal.h - host-side interfaces between the C ABI layer and the kernel launchers.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/hjscm.h"
+
+namespace hj {
+
+struct JoinAccum;
+
+// Geometry of the radix plan: total bits B split into physical passes of <= 8 bits each
+// (src/algo/params.h:34-35: FANOUT_PASS1 = 1 << (B/P), FANOUT_PASS2 = 1 << (B - B/P)).
+struct RadixGeom {
+    int bits;       // B
+    int passes;     // physical passes (1 or 2)
+    int b1, b2;     // bits of pass 1 / pass 2 (b2 = 0 for one pass)
+    int F1, F2;     // fanouts (F2 = 1 for one pass)
+    int nparts() const { return 1 << bits; }
+};
+
+int radix_geom(int bits, int passes, RadixGeom *g);
+
+// Tile and work-item constants shared by the plan and the kernels.
+constexpr int kScatterThreads = 256;
+constexpr int kScatterItems = 8;
+constexpr int kTile = kScatterThreads * kScatterItems;  // tuples per partition tile
+constexpr int kJoinThreads = 1024;
+constexpr int kSmemCap = 10240;        // largest build partition joined in shared memory
+constexpr int kProbeChunk = 1 << 16;   // S tuples per join work item
+constexpr int kMaxPass2Segs = 512;     // 2 relations x 256 pass-1 partitions
+
+// Device scratch layout of one partitioned join, carved out of a context arena.
+struct PhjScratch {
+    uint32_t *hist;         // [2][2^B]
+    uint64_t *start;        // [2][2^B + 1] final partition starts
+    void *segs;             // pass segment tables (2 passes)
+    uint64_t *obase;        // [2 passes][max segs][256] digit output bases
+    uint32_t *counters;     // tile counters, tile totals, item counts (memset per join)
+    uint32_t *status;       // look-back status words (memset per pass)
+    size_t status_words;
+    void *items;            // join work items
+    size_t max_items;
+    void *large;            // large-partition descriptors
+    size_t max_large;
+    uint32_t *large_table;  // head/next chains for large partitions (>= 12 B per R tuple)
+    size_t large_table_words;
+    ulonglong2 *tmp1;       // pass-1 output [nR + nS]
+    ulonglong2 *tmp2;       // pass-2 output [nR + nS] (== tmp1 for one pass)
+};
+
+size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS);
+void phj_carve(const RadixGeom &g, size_t nR, size_t nS, char *base, PhjScratch *s);
+
+// Enqueue a full partitioned join on `st`; matches/checksum accumulate into acc (zeroed by caller).
+// ev_mid, if non-null, is recorded between the partition phase and the join phase.
+int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
+                size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
+                int num_sms);
+
+// Non-partitioned joins on a global open-addressing table.
+size_t nphj_scratch_bytes(size_t nR, double load);
+int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
+                 size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
+                 int num_sms);
+
+}  // namespace hj

@@ -1,0 +1,233 @@
+// hj_nphj.cu - non-partitioned joins (nphj_sc / nphj_lp) on one global open-addressing table.
+//
+// Reference (src/algo/nphj.c):
+//   nphj_sc  build_hashtable_nphj_sc (nphj.c:132-301): |R|/2 buckets of two tuples plus overflow
+//            buckets, a spinlock per bucket; probe_hashtable_nphj_sc (nphj.c:304-442) walks the whole
+//            chain and counts every equal key.
+//   nphj_lp  lp_insert_with_pos (nphj.c:1056-1070): CAS on hashkey (stored as h+1) claims a slot;
+//            lp_lookup_with_pos (nphj.c:1146-1167) stops at the first equal key. With duplicate R keys
+//            the winner is a thread race; the contract here is the single-thread outcome, the first R
+//            tuple in input order.
+//
+// B200 design: one table of 16-byte slots {key, val} with capacity ~|R|/load, hashed by a
+// multiply-xorshift and linear probing. A slot is claimed by a 64-bit CAS of its key from EMPTY
+// (all ones). The build notices any key inserted twice (the later inserter always walks over the
+// earlier one's slot, because slots never empty). Without duplicates both algorithms stop at the
+// first match; with duplicates sc keeps walking to the empty slot and lp rebuilds the table with the
+// minimum input position per key (atomicMin) and resolves row ids in one gather pass. R tuples whose
+// key equals the EMPTY pattern are kept in a side record instead of the table.
+#include <cstdio>
+
+#include "hj_common.cuh"
+#include "hj_internal.h"
+
+namespace hj {
+
+constexpr unsigned long long kEmpty = ~0ull;
+
+struct NphjSide {
+    unsigned long long cnt;      // R tuples with key == kEmpty
+    unsigned long long sum;      // sum of their row ids
+    unsigned long long minpos;   // smallest input position among them
+    unsigned int dup;            // the build saw an equal key twice
+    unsigned int err;
+};
+
+struct NphjArgs {
+    const tuple_v *R, *S;
+    unsigned long long nR, nS;
+    tuple_v *table;
+    unsigned long long cap;
+    NphjSide *side;
+    JoinAccum *acc;
+    int lp;
+};
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
+    return *reinterpret_cast<const volatile unsigned long long *>(p);
+}
+
+// Insert R tuple (k, rid) at its own slot; records duplicates.
+__global__ void nphj_build(NphjArgs a) {
+    bool seen_dup = false;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.nR;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const tuple_v t = ld_stream(a.R + i);
+        if (t.x == kEmpty) {
+            if (atomicAdd(&a.side->cnt, 1ull) >= 1ull) seen_dup = true;
+            atomicAdd(&a.side->sum, (unsigned long long)t.y);
+            atomicMin(&a.side->minpos, i);
+            continue;
+        }
+        unsigned long long h = table_hash(t.x, a.cap);
+        unsigned long long steps = 0;
+        for (;;) {
+            unsigned long long *kp = &a.table[h].x;
+            unsigned long long cur = ld_volatile_u64(kp);
+            if (cur == kEmpty) {
+                cur = atomicCAS(kp, kEmpty, (unsigned long long)t.x);
+                if (cur == kEmpty) {
+                    a.table[h].y = t.y;
+                    break;
+                }
+            }
+            if (cur == t.x) seen_dup = true;
+            if (++h == a.cap) h = 0;
+            if (++steps >= a.cap) {
+                set_error(&a.acc->error, kErrProbeLimit);
+                break;
+            }
+        }
+    }
+    if (__syncthreads_or(seen_dup) && threadIdx.x == 0) atomicOr(&a.side->dup, 1u);
+}
+
+// Duplicate-key rebuild for nphj_lp: one slot per distinct key holding the minimum input position.
+__global__ void nphj_lp_refill(NphjArgs a) {
+    if (!(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.cap;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        a.table[i] = make_ulonglong2(kEmpty, kEmpty);
+}
+
+__global__ void nphj_lp_dedup_build(NphjArgs a) {
+    if (!(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.nR;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = a.R[i].x;
+        if (k == kEmpty) continue;
+        unsigned long long h = table_hash(k, a.cap);
+        unsigned long long steps = 0;
+        for (;;) {
+            unsigned long long *kp = &a.table[h].x;
+            unsigned long long cur = ld_volatile_u64(kp);
+            if (cur == kEmpty) cur = atomicCAS(kp, kEmpty, k);
+            if (cur == kEmpty || cur == k) {
+                atomicMin(&a.table[h].y, i);
+                break;
+            }
+            if (++h == a.cap) h = 0;
+            if (++steps >= a.cap) {
+                set_error(&a.acc->error, kErrProbeLimit);
+                break;
+            }
+        }
+    }
+}
+
+__global__ void nphj_lp_resolve(NphjArgs a) {
+    if (!(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.cap;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        tuple_v s = a.table[i];
+        if (s.x != kEmpty) {
+            if (s.y < a.nR)
+                a.table[i].y = a.R[s.y].y;
+            else
+                set_error(&a.acc->error, kErrBounds);
+        }
+    }
+}
+
+__global__ void nphj_probe(NphjArgs a) {
+    __shared__ unsigned long long red[64];
+    const bool dup = *reinterpret_cast<volatile unsigned int *>(&a.side->dup) != 0;
+    const bool first_only = a.lp || !dup;
+    const unsigned long long side_cnt = a.side->cnt;
+    unsigned long long cnt = 0, sum = 0;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long j0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j0 < a.nS;
+         j0 += 2 * stride) {
+        tuple_v sv[2];
+        sv[0] = ld_stream(a.S + j0);
+        sv[1] = j0 + stride < a.nS ? ld_stream(a.S + j0 + stride) : make_ulonglong2(0, 0);
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            if (u == 1 && j0 + stride >= a.nS) break;
+            const tuple_v s = sv[u];
+            if (s.x == kEmpty) {
+                if (side_cnt) {
+                    if (a.lp) {
+                        cnt++;
+                        sum += a.R[a.side->minpos].y + s.y;
+                    } else {
+                        cnt += side_cnt;
+                        sum += a.side->sum + side_cnt * s.y;
+                    }
+                }
+                continue;
+            }
+            unsigned long long h = table_hash(s.x, a.cap);
+            unsigned long long steps = 0;
+            for (;;) {
+                const tuple_v e = a.table[h];
+                if (e.x == kEmpty) break;
+                if (e.x == s.x) {
+                    cnt++;
+                    sum += e.y + s.y;
+                    if (first_only) break;
+                }
+                if (++h == a.cap) h = 0;
+                if (++steps >= a.cap) {
+                    set_error(&a.acc->error, kErrProbeLimit);
+                    break;
+                }
+            }
+        }
+    }
+    block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
+}
+
+static unsigned long long nphj_cap(size_t nR, double load) {
+    if (!(load > 0.05 && load < 0.95)) load = 0.5;
+    unsigned long long cap = (unsigned long long)((double)nR / load) + 2;
+    if (cap < 16) cap = 16;
+    return cap;
+}
+
+size_t nphj_scratch_bytes(size_t nR, double load) {
+    return (size_t)nphj_cap(nR, load) * 16 + 256;
+}
+
+#define HJ_CU(call)                                                                   \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            fprintf(stderr, "hjscm: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
+            return HJ_E_DEVICE;                                                       \
+        }                                                                             \
+    } while (0)
+
+int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
+                 size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
+                 int num_sms) {
+    const unsigned long long cap = nphj_cap(nR, load);
+    if (cap * 16 + 256 > table_bytes) return HJ_E_INVAL;
+    NphjArgs a;
+    a.R = R;
+    a.S = S;
+    a.nR = nR;
+    a.nS = nS;
+    a.table = reinterpret_cast<tuple_v *>(table);
+    a.cap = cap;
+    a.side = reinterpret_cast<NphjSide *>(reinterpret_cast<char *>(table) + cap * 16);
+    a.acc = acc;
+    a.lp = lp ? 1 : 0;
+    HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
+    HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
+    HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));
+    const int grid = num_sms * 8;
+    nphj_build<<<grid, 256, 0, st>>>(a);
+    if (lp) {
+        nphj_lp_refill<<<grid, 256, 0, st>>>(a);
+        nphj_lp_dedup_build<<<grid, 256, 0, st>>>(a);
+        nphj_lp_resolve<<<grid, 256, 0, st>>>(a);
+    }
+    HJ_CU(cudaGetLastError());
+    if (ev_mid) HJ_CU(cudaEventRecord(ev_mid, st));
+    nphj_probe<<<grid, 256, 0, st>>>(a);
+    HJ_CU(cudaGetLastError());
+    return HJ_OK;
+}
+
+}  // namespace hj

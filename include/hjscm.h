@@ -1,0 +1,173 @@
+/*
+ * hjscm.h - C ABI of the B200-native equi-join hot path.
+ *
+ * The library joins two relations of 16-byte tuples {uint64 key, uint64 row_id} on the key and
+ * reports the two numbers every join of the reference reports: the match count and the wrapping
+ * 64-bit sum of (r.row_id + s.row_id) over all matches. Four join algorithms are provided under the
+ * reference's --algo names:
+ *
+ *   nphj_sc        non-partitioned join, separate-chaining table, every match counted
+ *                  (replaces src/algo/nphj.c:677 nphj_sc)
+ *   nphj_lp        non-partitioned join, linear-probing table, first match per probe tuple
+ *                  (replaces src/algo/nphj.c:1487 nphj_lp)
+ *   phj_radix_bc   radix-partitioned join, bucket-chain partition tables, every match counted
+ *                  (replaces src/algo/phj.c:2515 phj_radix_bc -> join_init_run(..., bc_join))
+ *   phj_radix_lp   radix-partitioned join, linear-probing partition tables, first match per probe
+ *                  (replaces src/algo/phj.c phj_radix_lp -> join_init_run(..., lp_join))
+ *
+ * plus the bandwidth-regulated aliases phj_radix_bw_reg_bc / phj_radix_bw_reg_lp, which compute the
+ * same results (src/algo/phj_bw_reg.c:2874-2893).
+ *
+ * All entry points return an int status (HJ_OK or an HJ_E_* code) instead of exiting, and no entry
+ * point frees memory it does not own.
+ */
+#ifndef HJSCM_H
+#define HJSCM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* 16-byte tuple, byte-identical to the reference's tuple_t (src/inc/store.h:87-96) at the default
+ * TUPLE_T_SIZE of 16: {size_t key; size_t row_id;} packed and 16-byte aligned. */
+typedef struct {
+    uint64_t key;
+    uint64_t row_id;
+} hj_tuple_t;
+
+/* Materialised result pair, byte-identical to row_id_pair_t (src/inc/store.h:99-102). */
+typedef struct {
+    uint64_t r_row_id;
+    uint64_t s_row_id;
+} hj_pair_t;
+
+typedef enum {
+    HJ_ALGO_NPHJ_SC = 0,
+    HJ_ALGO_NPHJ_LP = 1,
+    HJ_ALGO_PHJ_RADIX_BC = 2,
+    HJ_ALGO_PHJ_RADIX_LP = 3,
+    HJ_ALGO_COUNT = 4
+} hj_algo_t;
+
+/* Status codes. The reference exit()s on every failure (src/main.c:215-218, src/inc/utils.c:501-518). */
+enum {
+    HJ_OK = 0,
+    HJ_E_INVAL = 1,       /* bad argument: unknown algo, unsupported radix bits, NULL pointer ... */
+    HJ_E_OOM = 2,         /* device or pinned-host allocation failed */
+    HJ_E_DEVICE = 3,      /* a CUDA call failed */
+    HJ_E_PROBE_LIMIT = 4, /* a table walk exceeded the table's capacity (full table, absent key) */
+    HJ_E_TIMEOUT = 5,     /* a bounded device wait gave up, or the host watchdog expired */
+    HJ_E_NOT_FOUND = 6,   /* unknown --algo name */
+    HJ_E_IO = 7,          /* a relation file could not be read */
+    HJ_E_OVERFLOW = 8,    /* a device-side bound check fired (internal error, results invalid) */
+    HJ_E_BUDGET = 9       /* a request does not fit the serving HBM budget */
+};
+
+/* Runtime knobs. The reference fixes these at compile time with -D (CMakeLists.txt:51-373,
+ * src/algo/params.h:14-35); here they are per call. */
+typedef struct {
+    int num_radix_bits;   /* NUM_RADIX_BITS, 1..16; 0 selects 14 */
+    int num_passes;       /* NUM_PASSES, 1 or 2; 0 selects 2 */
+    int device;           /* CUDA device ordinal */
+    int inputs_on_device; /* 1: R and S are device pointers; 0: host pointers (copied inside) */
+    void *stream;         /* cudaStream_t to run on; NULL selects the context's own stream */
+    uint32_t flags;       /* HJ_F_* bits */
+    double table_load;    /* NPHJ global table load factor (0 selects 0.5) */
+} hj_params_t;
+
+#define HJ_F_NO_TIMING   0x1u /* skip the per-phase CUDA events (buildpart/probejoin stay 0) */
+#define HJ_F_PINNED_HOST 0x2u /* host inputs are already page-locked */
+
+/* Result of one join. matched_cnt/checksum are the reference's two printed values
+ * (`matched_cnt: %zu\tcheck_sum: %zu`, src/algo/phj.c:2206); the times follow its timekeeper_t
+ * (src/inc/store.h:74-78): buildpart = partition (PHJ) or build (NPHJ) phase, probejoin = join or
+ * probe phase, total = their sum, all in seconds measured with CUDA events on the join's stream. */
+typedef struct {
+    uint64_t matched_cnt;
+    uint64_t checksum;
+    double buildpart;
+    double probejoin;
+    double total;
+    double h2d;       /* seconds spent copying host inputs to the device (0 for device inputs) */
+    int status;
+    int physical_passes; /* partition passes the device ran (PHJ only) */
+    uint64_t large_partitions; /* partitions joined through the global-memory path (PHJ only) */
+} hj_result_t;
+
+typedef struct hj_ctx hj_ctx_t;
+
+/* Fill p with the defaults (14 radix bits, 2 passes, device 0, host inputs). */
+void hj_params_init(hj_params_t *p);
+
+/* Human-readable name of a status code. */
+const char *hj_status_str(int status);
+
+/* --algo name -> algorithm, the lookup of src/main.c:202-220 (exact strcmp over the algos[] table
+ * of src/main.c:72-143, restricted to the names this library implements). */
+int hj_algo_from_name(const char *name, hj_algo_t *algo);
+const char *hj_algo_name(hj_algo_t algo);
+
+/* Contexts own a CUDA stream, events and a grow-only device scratch arena; joins on one context are
+ * serialised, joins on different contexts may run concurrently. */
+int hj_ctx_create(int device, hj_ctx_t **out);
+int hj_ctx_destroy(hj_ctx_t *ctx);
+/* Pre-size the scratch arena for a join of the given shape, so that later joins allocate nothing. */
+int hj_ctx_reserve(hj_ctx_t *ctx, hj_algo_t algo, const hj_params_t *p, size_t nR, size_t nS);
+/* Bytes of device scratch the context currently holds. */
+size_t hj_ctx_scratch_bytes(const hj_ctx_t *ctx);
+
+/* One join, synchronous: returns after the result is on the host. Replaces the body of
+ * join_init_run (src/algo/phj.c:1875-2512) and nphj_sc/nphj_lp (src/algo/nphj.c:677,1487) minus
+ * their file loading. R and S are caller-owned and never modified. */
+int hj_join_ctx(hj_ctx_t *ctx, hj_algo_t algo, const hj_params_t *p,
+                const hj_tuple_t *R, size_t nR, const hj_tuple_t *S, size_t nS, hj_result_t *out);
+
+/* hj_join_ctx on a per-device default context (created on first use, guarded by a mutex). */
+int hj_join(hj_algo_t algo, const hj_params_t *p,
+            const hj_tuple_t *R, size_t nR, const hj_tuple_t *S, size_t nS, hj_result_t *out);
+
+/* ----------------------------------------------------------------------------------------------
+ * Data generation. The seeded generators replay the reference's src/gen.c exactly (glibc srand/rand,
+ * Knuth shuffle), so the relations are byte-identical to the .bin files bin/gen writes.
+ * payload = 0: row_id = key (gen_pkfk_uniform, src/gen.c:199-223);
+ * payload = 1: row_id = 1-based position (payload_gen_pkfk_uniform, src/gen.c:258-283).
+ * Reference constraints kept: nS must be a multiple of nR and nR*16 a multiple of 4096
+ * (src/gen.c:178-179 copy FK blocks of 4096 bytes), else HJ_E_INVAL.
+ * -------------------------------------------------------------------------------------------- */
+int hj_gen_pkfk_uniform(size_t nR, size_t nS, unsigned seed, int payload, hj_tuple_t *R, hj_tuple_t *S);
+/* gen_dup_uniform (src/gen.c:286-331): R keys uniform in [1, nR] from a Park-Miller stream, S = FK
+ * copies of R, both shuffled. */
+int hj_gen_dup_uniform(size_t nR, size_t nS, unsigned seed, hj_tuple_t *R, hj_tuple_t *S);
+/* gen_fk_zipfian_eth -> gen_zipf (src/gen.c:375-391, src/inc/eth_genzipf.c:31-147): S keys Zipf over
+ * an alphabet of nR keys with the given zipf factor, row_id = position. The reference passes
+ * 1 + theta as the factor; this function takes the factor itself. */
+int hj_gen_zipf(size_t nS, size_t nR, double zipf_factor, unsigned seed, hj_tuple_t *S);
+
+/* Parallel seeded generators with the reference's value distributions, for sizes where the
+ * sequential shuffle is too slow. Keys of R are a seeded permutation of 1..nR (a Feistel bijection
+ * with cycle walking); S holds each of R's keys nS/nR times (+1 for the first nS%nR keys of a second
+ * bijection) in seeded order. row_id follows `payload` as above. dup > 1 makes R keys repeat: R holds
+ * keys 1..ceil(nR/dup) (the FK side draws from those); payload is forced to positions then.
+ * The host version runs on `threads` threads (0 = all cores); the device version runs on `stream`
+ * and writes device pointers. Both produce identical bytes. */
+int hj_gen_fast_host(size_t nR, size_t nS, uint64_t seed, int payload, unsigned dup, int threads,
+                     hj_tuple_t *R, hj_tuple_t *S);
+int hj_gen_fast_device(size_t nR, size_t nS, uint64_t seed, int payload, unsigned dup,
+                       hj_tuple_t *R_dev, hj_tuple_t *S_dev, void *stream);
+/* Zipf FK keys over an alphabet of nR keys drawn with a counter-based uniform stream on the device
+ * (same alphabet permutation / CDF-table / binary-search rule as gen_zipf); row_id = position. */
+int hj_gen_zipf_device(size_t nS, size_t nR, double zipf_factor, uint64_t seed,
+                       hj_tuple_t *S_dev, void *stream);
+
+/* Closed-form result of a PK-FK join on hj_gen_pkfk_uniform / hj_gen_fast_* data with payload 0 and
+ * nS a multiple of nR: matched = nS, checksum = m*n*(n+1) mod 2^64 with m = nS/nR. */
+void hj_pkfk_closed_form(size_t nR, size_t nS, uint64_t *matched, uint64_t *checksum);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HJSCM_H */

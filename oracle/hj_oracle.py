@@ -1,0 +1,287 @@
+"""CPU oracle for the equi-join hot path - TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker; the product
+(hashjoin-scm_b200/) never imports it.
+
+Contents
+- GlibcRandom: restatement of glibc's default random()/rand() generator (TYPE_3 additive feedback,
+  r[i] = r[i-3] + r[i-31] mod 2^32, output r >> 1, seeded by the 16807 LCG with 310 discards), the
+  generator the reference's bin/gen draws from after srand(12345) (src/gen.c:144).
+- gen_pkfk / gen_dup / gen_zipf: pure-Python restatements of src/gen.c:161-331 and
+  src/inc/eth_genzipf.c:31-147 on top of GlibcRandom (small sizes only: they are Python loops).
+- join / phj_literal / join_dense: ctypes front-ends of hj_oracle.c (the C restatement of the joins).
+- ref_*: run the reference's own code (built from its sources by oracle/Makefile into oracle/_ref).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import pathlib
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+REF_DIR = HERE / "_ref"
+
+ALL, FIRST, FIRST_NP = 0, 1, 2  # hj_oracle.c modes: bc/sc, phj lp, nphj lp
+MODE_OF_ALGO = {"nphj_sc": ALL, "phj_radix_bc": ALL, "nphj_lp": FIRST_NP, "phj_radix_lp": FIRST,
+                "phj_radix_bw_reg_bc": ALL, "phj_radix_bw_reg_lp": FIRST}
+RAND_MAX = 2147483647
+MASK64 = (1 << 64) - 1
+
+
+# ------------------------------------------------------------------------------------------------
+# glibc random()
+# ------------------------------------------------------------------------------------------------
+class GlibcRandom:
+    """glibc random_r with the default 128-byte state (TYPE_3: degree 31, separation 3)."""
+
+    def __init__(self, seed: int):
+        seed &= 0xFFFFFFFF
+        if seed == 0:
+            seed = 1
+        r = [0] * 31
+        r[0] = seed
+        word = seed if seed < 2**31 else seed - 2**32
+        for i in range(1, 31):
+            hi, lo = divmod(word, 127773) if word >= 0 else (-((-word) // 127773), -((-word) % 127773))
+            word = 16807 * lo - 2836 * hi
+            if word < 0:
+                word += 2147483647
+            r[i] = word & 0xFFFFFFFF
+        self.r = r
+        self.f = 3  # front pointer index
+        self.b = 0  # rear pointer index
+        for _ in range(310):
+            self._step()
+
+    def _step(self) -> int:
+        r = self.r
+        r[self.f] = (r[self.f] + r[self.b]) & 0xFFFFFFFF
+        out = r[self.f] >> 1
+        self.f = (self.f + 1) % 31
+        self.b = (self.b + 1) % 31
+        return out
+
+    def rand(self) -> int:
+        return self._step()
+
+
+# ------------------------------------------------------------------------------------------------
+# Generator restatements (src/gen.c, src/inc/eth_genzipf.c)
+# ------------------------------------------------------------------------------------------------
+def _knuth_shuffle(g: GlibcRandom, t: np.ndarray) -> None:
+    """src/gen.c:161-171: for i in 0..n-1: j = rand() % n; swap(t[i], t[j])."""
+    n = t.shape[0]
+    for i in range(n):
+        j = g.rand() % n
+        if i != j:
+            tmp = t[j].copy()
+            t[j] = t[i]
+            t[i] = tmp
+
+
+def gen_pkfk(nR: int, nS: int, seed: int = 12345, payload: bool = False):
+    """gen_pkfk_uniform (src/gen.c:199-223) / payload_gen_pkfk_uniform (src/gen.c:258-283)."""
+    assert nS % nR == 0 and (nR * 16) % 4096 == 0
+    g = GlibcRandom(seed)
+    R = np.empty((nR, 2), dtype=np.uint64)
+    R[:, 0] = np.arange(1, nR + 1, dtype=np.uint64)
+    R[:, 1] = R[:, 0]
+    _knuth_shuffle(g, R)
+    S = np.concatenate([R] * (nS // nR))  # gen_fk_from_pk copies (src/gen.c:178-182)
+    _knuth_shuffle(g, S)
+    if payload:
+        S[:, 1] = np.arange(1, nS + 1, dtype=np.uint64)
+        R[:, 1] = np.arange(1, nR + 1, dtype=np.uint64)
+    return R, S
+
+
+def gen_dup(nR: int, nS: int, seed: int = 12345):
+    """gen_dup_uniform (src/gen.c:286-331)."""
+    assert nS % nR == 0 and (nR * 16) % 4096 == 0
+    g = GlibcRandom(seed)
+    uni = g.rand() % RAND_MAX
+    R = np.empty((nR, 2), dtype=np.uint64)
+    for i in range(nR):
+        k = int(uni / 127773) if uni >= 0 else -int(-uni / 127773)
+        uni = 16807 * (uni - k * 127773) - k * 2836
+        # the reference computes this in 32-bit int arithmetic
+        uni = ((uni + 2**31) % 2**32) - 2**31
+        if uni < 0:
+            uni += 2147483647
+        r = uni * 4.656612875e-10
+        r = (1.0 - r) * (1 - 0.5) + r * (nR + 0.5)
+        key = int(_c_round(r))
+        key = min(max(key, 1), nR)
+        R[i, 0] = key
+        R[i, 1] = i + 1
+    _knuth_shuffle(g, R)
+    S = np.concatenate([R] * (nS // nR))
+    _knuth_shuffle(g, S)
+    return R, S
+
+
+def _c_round(x: float) -> float:
+    """C round(): half away from zero."""
+    return math.floor(x + 0.5) if x >= 0 else -math.floor(-x + 0.5)
+
+
+def gen_zipf(nS: int, nR: int, factor: float, seed: int = 12345):
+    """gen_zipf (src/inc/eth_genzipf.c:97-147) after gen_alphabet and gen_zipf_lut."""
+    g = GlibcRandom(seed)
+    alphabet = list(range(1, nR + 1))
+    for i in range(nR - 1, 0, -1):
+        k = (i * g.rand()) // RAND_MAX
+        alphabet[i], alphabet[k] = alphabet[k], alphabet[i]
+    scale = 0.0
+    for i in range(1, nR + 1):
+        scale += 1.0 / math.pow(i, factor)
+    lut = []
+    s = 0.0
+    for i in range(1, nR + 1):
+        s += 1.0 / math.pow(i, factor)
+        lut.append(s / scale)
+    S = np.empty((nS, 2), dtype=np.uint64)
+    for j in range(nS):
+        r = g.rand() / RAND_MAX
+        if lut[0] >= r:
+            pos = 0
+        else:
+            left, right = 1, nR
+            while right - left > 1:
+                m = (left + right) // 2
+                if lut[m] < r:
+                    left = m
+                else:
+                    right = m
+            pos = right
+        S[j, 0] = alphabet[pos]
+        S[j, 1] = j + 1
+    return S
+
+
+# ------------------------------------------------------------------------------------------------
+# C oracle
+# ------------------------------------------------------------------------------------------------
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-C", str(HERE), "liboracle.so"], check=True, capture_output=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        vp, sz, u64p = ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)
+        L.hjo_join.argtypes = [ctypes.c_int, vp, sz, vp, sz, u64p, u64p]
+        L.hjo_join.restype = ctypes.c_int
+        L.hjo_phj_literal.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, sz, vp, sz, u64p, u64p]
+        L.hjo_phj_literal.restype = ctypes.c_int
+        L.hjo_join_dense.argtypes = [ctypes.c_int, vp, sz, vp, sz, ctypes.c_uint64, u64p, u64p]
+        L.hjo_join_dense.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _arr(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    assert a.ndim == 2 and a.shape[1] == 2
+    return a
+
+
+def join(mode_or_algo, R: np.ndarray, S: np.ndarray) -> tuple[int, int]:
+    """(matched_cnt, check_sum) from the definition of the join (hj_oracle.c hjo_join)."""
+    mode = MODE_OF_ALGO[mode_or_algo] if isinstance(mode_or_algo, str) else mode_or_algo
+    R, S = _arr(R), _arr(S)
+    c, s = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib().hjo_join(mode, R.ctypes.data, R.shape[0], S.ctypes.data, S.shape[0], ctypes.byref(c),
+                        ctypes.byref(s))
+    assert rc == 0, rc
+    return c.value, s.value
+
+
+def join_dense(mode_or_algo, R: np.ndarray, S: np.ndarray, max_key: int) -> tuple[int, int]:
+    mode = MODE_OF_ALGO[mode_or_algo] if isinstance(mode_or_algo, str) else mode_or_algo
+    R, S = _arr(R), _arr(S)
+    c, s = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib().hjo_join_dense(mode, R.ctypes.data, R.shape[0], S.ctypes.data, S.shape[0], max_key,
+                              ctypes.byref(c), ctypes.byref(s))
+    assert rc == 0, rc
+    return c.value, s.value
+
+
+def phj_literal(bits: int, passes: int, lp: bool, R: np.ndarray, S: np.ndarray) -> tuple[int, int, int]:
+    """Step-by-step restatement of the reference's radix join; returns (cnt, sum, rc)."""
+    R, S = _arr(R), _arr(S)
+    c, s = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib().hjo_phj_literal(bits, passes, 1 if lp else 0, R.ctypes.data, R.shape[0], S.ctypes.data,
+                               S.shape[0], ctypes.byref(c), ctypes.byref(s))
+    return c.value, s.value, rc
+
+
+# ------------------------------------------------------------------------------------------------
+# The reference itself (oracle/_ref, built from its sources by oracle/Makefile)
+# ------------------------------------------------------------------------------------------------
+def ref_available(passes: int = 2) -> bool:
+    return (REF_DIR / f"hjref_p{passes}").exists()
+
+
+def ref_build() -> bool:
+    if not pathlib.Path("/root/reference/src").exists():
+        return ref_available(1) and ref_available(2)
+    out = subprocess.run(["make", "-C", str(HERE), "ref"], capture_output=True, text=True)
+    return out.returncode == 0
+
+
+def ref_gen(kind: str, nR: int, nS: int, factor: float = 1.05, seed: int = 12345):
+    """Relations written by the reference's own generator functions (src/gen.c)."""
+    with tempfile.TemporaryDirectory() as d:
+        cmd = [str(REF_DIR / "hjref_p2"), f"--gen={kind}", f"--prefix={d}", f"--nr={nR}", f"--ns={nS}",
+               f"--seed={seed}", f"--factor={factor}"]
+        subprocess.run(cmd, check=True, capture_output=True, timeout=600)
+        if kind == "zipf":
+            path = pathlib.Path(d) / "zipfian" / f"fk_{factor:.3f}_AS.bin"
+            return np.fromfile(path, dtype=np.uint64).reshape(-1, 2)
+        prefix = "dup" if kind == "dup" else "pk"
+        R = np.fromfile(pathlib.Path(d) / "gen" / f"{prefix}_R.bin", dtype=np.uint64).reshape(-1, 2)
+        S = np.fromfile(pathlib.Path(d) / "gen" / "fk_S.bin", dtype=np.uint64).reshape(-1, 2)
+        return R, S
+
+
+_REF_LINE = re.compile(r"matched_cnt: (\d+)\s+check_sum: (\d+)")
+_TRIAL_LINE = re.compile(r"hjref_trial: (\d+) buildpart: ([\d.eE+-]+) probejoin: ([\d.eE+-]+) total: ([\d.eE+-]+)")
+
+
+def ref_run_files(algo: str, prefix: str, rfile: str, sfile: str, nR: int, nS: int, bits: int = 14,
+                  passes: int = 2, threads: int | None = None, trials: int = 1, timeout: float = 900):
+    """Run the reference's join on .bin files; returns [(cnt, sum, buildpart, probejoin, total)]."""
+    threads = threads or os.cpu_count() or 1
+    cmd = [str(REF_DIR / f"hjref_p{passes}"), f"--algo={algo}", f"--prefix={prefix}", f"--r={rfile}",
+           f"--s={sfile}", f"--nr={nR}", f"--ns={nS}", f"--bits={bits}", f"--threads={threads}",
+           f"--trials={trials}"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if out.returncode != 0:
+        raise RuntimeError(f"reference run failed ({out.returncode}): {out.stderr[-2000:]}")
+    res = [(int(a), int(b)) for a, b in _REF_LINE.findall(out.stdout)]
+    tim = [(float(b), float(c), float(d)) for _, b, c, d in _TRIAL_LINE.findall(out.stdout)]
+    return [r + t for r, t in zip(res, tim)]
+
+
+def ref_join(algo: str, R: np.ndarray, S: np.ndarray, bits: int = 14, passes: int = 2,
+             threads: int | None = None) -> tuple[int, int]:
+    """(matched_cnt, check_sum) printed by the reference's own join on these relations."""
+    with tempfile.TemporaryDirectory() as d:
+        _arr(R).tofile(os.path.join(d, "r.bin"))
+        _arr(S).tofile(os.path.join(d, "s.bin"))
+        runs = ref_run_files(algo, d, "r.bin", "s.bin", R.shape[0], S.shape[0], bits, passes, threads)
+        return runs[0][0], runs[0][1]

@@ -1,0 +1,110 @@
+/*
+ * ref_driver.c - command-line driver around the reference's own join and generator functions, built
+ * from the reference sources by oracle/Makefile into oracle/_ref. TEST / BASELINE INFRASTRUCTURE ONLY.
+ *
+ * It replaces src/main.c's libconfig-driven setup (src/main.c:147-255) with flags and calls the
+ * reference functions unmodified:
+ *   hjref_pN --algo=<nphj_sc|nphj_lp|phj_radix_bc|phj_radix_lp> --prefix=DIR --r=REL --s=REL
+ *            --nr=N --ns=M [--bits=14] [--threads=T] [--trials=K]
+ *       Each trial prints the reference's "matched_cnt: ..\tcheck_sum: .." line, then
+ *       "hjref_trial: <k> buildpart: <s> probejoin: <s> total: <s>".
+ *   hjref_pN --gen=<pkfk|payload|dup|zipf> --prefix=DIR --nr=N --ns=M [--factor=F] [--seed=12345]
+ *       srand(seed), then gen_pkfk_uniform / payload_gen_pkfk_uniform / gen_dup_uniform /
+ *       gen_fk_zipfian_eth exactly as generate_workload does (src/gen.c:29-117); files land under DIR.
+ * N (1 or 2) is the reference's compile-time NUM_PASSES.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include "inc/store.h"
+
+int hjref_threads = 1;
+int hjref_radix_bits = 14;
+const char *hjref_data_prefix = ".";
+const char *hjref_work_prefix = "/tmp";
+
+extern int local_cores[];
+extern int remote_cores[];
+
+void nphj_sc(const datameta_t, timekeeper_t *const);
+void nphj_lp(const datameta_t, timekeeper_t *const);
+void phj_radix_bc(const datameta_t, timekeeper_t *const);
+void phj_radix_lp(const datameta_t, timekeeper_t *const);
+void gen_pkfk_uniform(const size_t, const size_t, const char *, const char *, const char *);
+void payload_gen_pkfk_uniform(const size_t, const size_t, const char *, const char *, const char *);
+void gen_dup_uniform(const size_t, const size_t, const char *, const char *, const char *);
+void gen_fk_zipfian_eth(const size_t, const size_t, double);
+
+static const char *arg(int argc, char **argv, const char *name) {
+    size_t L = strlen(name);
+    for (int i = 1; i < argc; i++)
+        if (!strncmp(argv[i], "--", 2) && !strncmp(argv[i] + 2, name, L) && argv[i][2 + L] == '=')
+            return argv[i] + 3 + L;
+    return NULL;
+}
+
+int main(int argc, char **argv) {
+    const char *v;
+    long nproc = sysconf(_SC_NPROCESSORS_ONLN);
+    if (nproc < 1) nproc = 1;
+    for (int i = 0; i < 1024; i++) local_cores[i] = remote_cores[i] = (int)(i % nproc);
+    hjref_threads = (v = arg(argc, argv, "threads")) ? atoi(v) : (int)nproc;
+    if (hjref_threads < 1) hjref_threads = 1;
+    hjref_radix_bits = (v = arg(argc, argv, "bits")) ? atoi(v) : 14;
+    hjref_data_prefix = (v = arg(argc, argv, "prefix")) ? v : ".";
+    const size_t nR = (v = arg(argc, argv, "nr")) ? strtoull(v, NULL, 10) : 0;
+    const size_t nS = (v = arg(argc, argv, "ns")) ? strtoull(v, NULL, 10) : 0;
+    const unsigned seed = (v = arg(argc, argv, "seed")) ? (unsigned)strtoul(v, NULL, 10) : 12345u;
+
+    if ((v = arg(argc, argv, "gen"))) {
+        srand(seed);
+        if (!strcmp(v, "pkfk")) gen_pkfk_uniform(nR, nS, "gen", "R", "S");
+        else if (!strcmp(v, "payload")) payload_gen_pkfk_uniform(nR, nS, "gen", "R", "S");
+        else if (!strcmp(v, "dup")) gen_dup_uniform(nR, nS, "gen", "R", "S");
+        else if (!strcmp(v, "zipf")) {
+            const char *f = arg(argc, argv, "factor");
+            /* gen_fk_zipfian_eth adds 1 to its theta argument (src/gen.c:379-380). */
+            gen_fk_zipfian_eth(nS, nR, (f ? atof(f) : 1.05) - 1.0);
+        } else {
+            fprintf(stderr, "unknown --gen=%s\n", v);
+            return 2;
+        }
+        return 0;
+    }
+
+    const char *algo = arg(argc, argv, "algo");
+    void (*fn)(const datameta_t, timekeeper_t *const) = NULL;
+    if (algo && !strcmp(algo, "nphj_sc")) fn = nphj_sc;
+    else if (algo && !strcmp(algo, "nphj_lp")) fn = nphj_lp;
+    else if (algo && !strcmp(algo, "phj_radix_bc")) fn = phj_radix_bc;
+    else if (algo && !strcmp(algo, "phj_radix_lp")) fn = phj_radix_lp;
+    if (!fn) {
+        fprintf(stderr, "unknown or missing --algo\n");
+        return 2;
+    }
+    datameta_t d;
+    memset(&d, 0, sizeof(d));
+    d.r_path_suffix = (char *)arg(argc, argv, "r");
+    d.s_path_suffix = (char *)arg(argc, argv, "s");
+    d.r_tuple_num = nR;
+    d.s_tuple_num = nS;
+    d.r_tuple_size = d.s_tuple_size = 16;
+    d.min_key = 1;
+    d.max_key = nR;
+    d.workload_name = (char *)"hjref";
+    if (!d.r_path_suffix || !d.s_path_suffix) {
+        fprintf(stderr, "missing --r/--s\n");
+        return 2;
+    }
+    const int trials = (v = arg(argc, argv, "trials")) ? atoi(v) : 1;
+    for (int t = 0; t < trials; t++) {
+        timekeeper_t tk = {0.0, 0.0, 0.0};
+        fn(d, &tk);
+        printf("hjref_trial: %d buildpart: %.9f probejoin: %.9f total: %.9f\n", t, tk.buildpart, tk.probejoin,
+               tk.total);
+        fflush(stdout);
+    }
+    return 0;
+}

@@ -1,0 +1,179 @@
+"""CPU tests of the oracle and of the host-side generators, pinned against the reference.
+
+Pins, in order of strength:
+  1. golden fixtures produced by the reference's own generator and joins (tests/golden/
+     reference_small.json, made by tests/golden/make_golden.py);
+  2. the reference's published log values (closed forms, logs/*/*.log);
+  3. the reference binary itself (oracle/_ref), when it has been built on this machine.
+"""
+import ctypes
+import hashlib
+import json
+import os
+import pathlib
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+GOLDEN = json.loads((ROOT / "tests" / "golden" / "reference_small.json").read_text())
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_glibc_random_restatement_matches_libc():
+    """The oracle's restated generator equals glibc's rand() after srand(seed)."""
+    from conftest import load_oracle
+
+    orc = load_oracle()
+    libc = ctypes.CDLL("libc.so.6")
+    for seed in (12345, 1, 0, 7, 2**31 + 5, 2**32 - 1):
+        libc.srand(ctypes.c_uint(seed))
+        want = [libc.rand() for _ in range(2000)]
+        g = orc.GlibcRandom(seed)
+        got = [g.rand() for _ in range(2000)]
+        assert got == want, seed
+
+
+@pytest.mark.parametrize("case", GOLDEN["cases"], ids=lambda c: c["name"])
+def test_product_generator_matches_reference_bytes(hj, case):
+    """hj_gen_* replays the reference generator byte for byte (sha256 of the reference's .bin files)."""
+    nR, nS = case["nR"], case["nS"]
+    if case["gen"] == "zipf":
+        R, _ = hj.gen_pkfk_uniform(nR, nR)
+        S = hj.gen_zipf(nS, nR, case["factor"])
+    elif case["gen"] == "dup":
+        R, S = hj.gen_dup_uniform(nR, nS)
+    else:
+        R, S = hj.gen_pkfk_uniform(nR, nS, payload=case["gen"] == "payload")
+    assert sha(R) == case["r_sha256"]
+    assert sha(S) == case["s_sha256"]
+
+
+@pytest.mark.parametrize("case", [c for c in GOLDEN["cases"] if c["nS"] <= 1 << 14], ids=lambda c: c["name"])
+def test_python_generator_restatement_matches_reference_bytes(oracle, case):
+    """The oracle's independent Python restatement of src/gen.c gives the same bytes."""
+    nR, nS = case["nR"], case["nS"]
+    if case["gen"] == "zipf":
+        R, _ = oracle.gen_pkfk(nR, nR)
+        S = oracle.gen_zipf(nS, nR, case["factor"])
+    elif case["gen"] == "dup":
+        R, S = oracle.gen_dup(nR, nS)
+    else:
+        R, S = oracle.gen_pkfk(nR, nS, payload=case["gen"] == "payload")
+    assert sha(R) == case["r_sha256"]
+    assert sha(S) == case["s_sha256"]
+
+
+def _golden_relations(hj, case):
+    nR, nS = case["nR"], case["nS"]
+    if case["gen"] == "zipf":
+        R, _ = hj.gen_pkfk_uniform(nR, nR)
+        return R, hj.gen_zipf(nS, nR, case["factor"])
+    if case["gen"] == "dup":
+        return hj.gen_dup_uniform(nR, nS)
+    return hj.gen_pkfk_uniform(nR, nS, payload=case["gen"] == "payload")
+
+
+@pytest.mark.parametrize("case", GOLDEN["cases"], ids=lambda c: c["name"])
+def test_oracle_matches_reference_golden(hj, oracle, case):
+    """Both oracle restatements reproduce every reference join result in the fixture."""
+    R, S = _golden_relations(hj, case)
+    for algo, (cnt, chk) in case["results"].items():
+        assert oracle.join(algo, R, S) == (cnt, chk), algo
+        if algo.startswith("phj"):
+            c, s, rc = oracle.phj_literal(case["bits"], case["passes"], algo.endswith("lp"), R, S)
+            assert rc == 0 and (c, s) == (cnt, chk), algo
+
+
+# Values printed by the reference in its shipped logs (matched_cnt, check_sum).
+LOG_KATS = [
+    # nR, nS, matched, checksum, source
+    (1 << 24, 1 << 28, 268435456, 4503599895805952, "logs/pkfkA-logs/rdx_bc_nvm.log:2"),
+    (1 << 26, 1 << 28, 268435456, 18014398777917440, "logs/size-difference-logs/rdx_bc_pkfk_nvm.log:32"),
+    (1 << 28, 1 << 28, 268435456, 72057594306363392, "logs/size-difference-logs/rdx_bc_pkfk_nvm.log:52"),
+    (1 << 30, 1 << 34, 17179869184, 17179869184, "logs/billion-logs/rdx_bc_billion_nvm.log:12"),
+]
+
+
+@pytest.mark.parametrize("kat", LOG_KATS, ids=lambda k: k[4])
+def test_closed_form_matches_reference_logs(hj, kat):
+    nR, nS, m, c, _ = kat
+    assert hj.pkfk_closed_form(nR, nS) == (m, c)
+
+
+def test_closed_form_matches_oracle_small(hj, oracle):
+    for nR, nS in [(256, 256), (1024, 4096), (4096, 8192)]:
+        R, S = hj.gen_pkfk_uniform(nR, nS)
+        assert oracle.join("phj_radix_bc", R, S) == hj.pkfk_closed_form(nR, nS)
+
+
+def _random_relations(rng, nR, nS, key_range, zero_keys=False):
+    R = np.empty((nR, 2), dtype=np.uint64)
+    S = np.empty((nS, 2), dtype=np.uint64)
+    lo = 0 if zero_keys else 1
+    R[:, 0] = rng.integers(lo, key_range + 1, nR, dtype=np.uint64)
+    S[:, 0] = rng.integers(lo, key_range + 1, nS, dtype=np.uint64)
+    R[:, 1] = rng.integers(0, 2**64 - 1, nR, dtype=np.uint64)
+    S[:, 1] = rng.integers(0, 2**64 - 1, nS, dtype=np.uint64)
+    return R, S
+
+
+@pytest.mark.parametrize("bits,passes", [(1, 1), (3, 1), (5, 2), (8, 1), (9, 2), (12, 2)])
+def test_literal_restatement_equals_definition(oracle, bits, passes):
+    """The step-by-step radix join equals the direct definition, duplicates and key 0 included."""
+    rng = np.random.default_rng(bits * 10 + passes)
+    for key_range, zero in [(50, False), (3000, True), (1 << 40, False)]:
+        R, S = _random_relations(rng, 3000, 5000, key_range, zero)
+        c, s, rc = oracle.phj_literal(bits, passes, False, R, S)
+        assert rc == 0 and (c, s) == oracle.join(oracle.ALL, R, S)
+        c, s, rc = oracle.phj_literal(bits, passes, True, R, S)
+        if rc == 0:  # rc != 0: a full partition table with an absent key (loops in the reference)
+            assert (c, s) == oracle.join(oracle.FIRST, R, S)
+
+
+def test_dense_oracle_equals_hash_oracle(oracle):
+    rng = np.random.default_rng(3)
+    R, S = _random_relations(rng, 5000, 9000, 4000)
+    for mode in (oracle.ALL, oracle.FIRST, oracle.FIRST_NP):
+        assert oracle.join_dense(mode, R, S, 4000) == oracle.join(mode, R, S)
+
+
+def test_key_zero_rule(oracle):
+    """phj_radix_lp ignores key 0 (it marks an empty slot); nphj_lp and the all-match joins do not."""
+    R = np.array([[0, 5], [1, 7], [0, 9]], dtype=np.uint64)
+    S = np.array([[0, 100], [1, 200]], dtype=np.uint64)
+    assert oracle.join(oracle.ALL, R, S) == (3, 5 + 100 + 9 + 100 + 7 + 200)
+    assert oracle.join(oracle.FIRST, R, S) == (1, 7 + 200)
+    assert oracle.join(oracle.FIRST_NP, R, S) == (2, 5 + 100 + 7 + 200)
+
+
+@pytest.mark.skipif(not pathlib.Path("/root/reference/src").exists(), reason="reference sources absent")
+def test_oracle_matches_reference_binary_random(oracle):
+    """Random keys with heavy duplication, straight through the reference's own joins."""
+    if not (oracle.ref_available(1) and oracle.ref_available(2)):
+        pytest.skip("reference not built")
+    rng = np.random.default_rng(11)
+    R, S = _random_relations(rng, 4096, 16384, 900)
+    # Probe keys are drawn from R's keys: the reference's linear-probing joins loop forever on an absent
+    # key when a table is full (src/algo/phj.c:655-658, src/algo/nphj.c:1162-1164).
+    S[:, 0] = R[rng.integers(0, R.shape[0], S.shape[0]), 0]
+    for algo in ("nphj_sc", "phj_radix_bc", "phj_radix_lp"):
+        for bits, passes in ((6, 1), (10, 2)):
+            assert oracle.ref_join(algo, R, S, bits=bits, passes=passes, threads=4) == oracle.join(algo, R, S)
+    assert oracle.ref_join("nphj_lp", R, S, threads=1) == oracle.join("nphj_lp", R, S)
+
+
+@pytest.mark.skipif(os.environ.get("HJ_SLOW") != "1", reason="minutes of CPU; set HJ_SLOW=1")
+def test_generator_reproduces_published_skew_and_dup_logs(hj, oracle):
+    """Full-size replays of the reference's published skew/dup datasets (2^24 x 2^28)."""
+    R, S = hj.gen_dup_uniform(1 << 24, 1 << 28)
+    # logs/dupfk-logs/rdx_bc_dupfk_nvm.log:12
+    assert oracle.join_dense(oracle.ALL, R, S, 1 << 24) == (534841984, 8973526820846944)
+    del R, S
+    R, _ = hj.gen_pkfk_uniform(1 << 24, 1 << 24)
+    S = hj.gen_zipf(1 << 28, 1 << 24, 1.05)
+    # logs/skew-logs/rdx_bc_zipf_nvm.log:12
+    assert oracle.join_dense(oracle.ALL, R, S, 1 << 24) == (268435456, 38229679500325349)
