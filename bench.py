@@ -1,0 +1,389 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 equi-join hot path (one JSON line on rank 0).
+
+Workload (the headline configuration): phj_radix_bc, R = 2^27 and S = 2^29 tuples of 16 bytes
+{int64 key, int64 row_id}; R keys a seeded permutation of 1..2^27, S holds every R key 4 times in
+seeded order (the reference's gen_pkfk_uniform distribution, generated in parallel on the device);
+14 radix bits in 2 passes. One step = one full join (histogram, two partition passes, partition
+joins). Metric: (|R| + |S|) / join time, the reference's throughput definition (phases timed as
+buildpart + probejoin, src/algo/phj.c:2509-2511).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own multithreaded CPU join (compiled from its sources into
+oracle/_ref) on the host cores, on the same workload, and prints the same line with impl=reference.
+With N > 1 (torchrun) every rank joins its own relations: independent joins, no collective on the
+data path (weak scaling); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG_DIR = ROOT / "hashjoin-scm_b200"
+METRIC = "join throughput (|R|+|S|)/s and % HBM roofline at 1 B200; batched joins/s; p99"
+UNIT = "tuples/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def load_module(name, path):
+    spec = importlib.util.spec_from_file_location(name, path, submodule_search_locations=[str(path.parent)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--algo", default="phj_radix_bc")
+    ap.add_argument("--nr-log", type=int, default=27)
+    ap.add_argument("--ns-log", type=int, default=29)
+    ap.add_argument("--bits", type=int, default=14)
+    ap.add_argument("--passes", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-log", type=int, default=0,
+                    help="log2 |R| of the CPU-baseline sample (0: pick by host memory)")
+    return ap.parse_args()
+
+
+def workload_config(a, n_gpus):
+    return {
+        "workload": f"{a.algo} PK-FK uniform, R=2^{a.nr_log} S=2^{a.ns_log} tuples of 16 B "
+                    f"(int64 key + int64 row_id), {a.bits} radix bits, {a.passes} passes",
+        "algo": a.algo,
+        "r_tuples": 1 << a.nr_log,
+        "s_tuples": 1 << a.ns_log,
+        "num_radix_bits": a.bits,
+        "num_passes": a.passes,
+        "parallelism": f"{n_gpus} independent joins, one per GPU" if n_gpus > 1 else "1 GPU",
+        "l2": "inputs (R+S = %.1f GB) larger than L2 (126 MB); no flush between steps"
+              % (((1 << a.nr_log) + (1 << a.ns_log)) * 16 / 1e9),
+        "generator": "seeded Feistel permutation on the device (gen_pkfk_uniform distribution)",
+    }
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU clock sampling during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = (bus_id or "").lower()
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        rows = []
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 10:
+                continue
+            if self.bus_id and not parts[1].lower().endswith(self.bus_id):
+                continue
+            rows.append(parts)
+        if not rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x.split()[0])
+            except (ValueError, IndexError):
+                return None
+
+        sm = [num(r[2]) for r in rows if num(r[2]) is not None]
+        mx = [num(r[3]) for r in rows if num(r[3]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_profile(kernel: str):
+    """Per-tuple DRAM traffic of a kernel from a committed ncu summary (profiles/<kernel>.json)."""
+    p = ROOT / "profiles" / f"{kernel}.json"
+    if not p.exists():
+        return None
+    return json.loads(p.read_text())
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline: the reference's own multithreaded join (oracle/_ref) on the host cores
+# ---------------------------------------------------------------------------------------------
+def host_mem_available_gb() -> float:
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                return int(ln.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
+
+
+def cpu_reference_run(hj, a, trials: int, sample_log: int = 0):
+    """Returns (throughput tuples/s list over timed trials, sample description, threads, kind)."""
+    orc = load_module("hj_oracle", ROOT / "oracle" / "hj_oracle.py")
+    nr_log, ns_log = a.nr_log, a.ns_log
+    if sample_log:
+        ns_log = sample_log + (a.ns_log - a.nr_log)
+        nr_log = sample_log
+    else:
+        # R+S files, the reference's private copy and its partition buffers: 3 x 16 B per tuple.
+        need_gb = 3 * 16 * ((1 << nr_log) + (1 << ns_log)) / 1e9 + 4
+        while host_mem_available_gb() < need_gb and nr_log > 20:
+            nr_log -= 1
+            ns_log -= 1
+            need_gb /= 2
+    nR, nS = 1 << nr_log, 1 << ns_log
+    threads = os.cpu_count() or 1
+    passes = a.passes
+    tmpdir = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        R, S = hj.gen_fast_host(nR, nS, seed=12345)
+        R.tofile(os.path.join(d, "r.bin"))
+        S.tofile(os.path.join(d, "s.bin"))
+        del R, S
+        if orc.ref_available(passes):
+            runs = orc.ref_run_files(a.algo.replace("_bw_reg", ""), d, "r.bin", "s.bin", nR, nS, bits=a.bits,
+                                     passes=passes, threads=threads, trials=trials + 1, timeout=1800)
+            kind = "reference"
+        else:
+            raise RuntimeError("oracle/_ref is not built")
+    want = hj.pkfk_closed_form(nR, nS)
+    for r in runs:
+        if (r[0], r[1]) != want:
+            raise RuntimeError(f"reference result {r[:2]} != closed form {want}")
+    timed = runs[1:]  # the reference drops its first trial as warm-up (src/main.c:434)
+    thr = [(nR + nS) / r[4] for r in timed]
+    sample = f"{a.algo} R=2^{nr_log} S=2^{ns_log}, {len(timed)} timed trials after 1 warm-up, reference timekeeper total"
+    return thr, sample, threads, kind
+
+
+# ---------------------------------------------------------------------------------------------
+def run_reference_arm(a, rank, world):
+    if rank != 0:
+        return 0
+    hj = load_module("hashjoin_scm_b200", PKG_DIR / "__init__.py")
+    thr, sample, threads, kind = cpu_reference_run(hj, a, trials=max(a.steps, 1), sample_log=a.cpu_sample_log)
+    value = statistics.mean(thr)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": len(thr),
+        "warmup": 1, "ms_per_step": ((1 << a.nr_log) + (1 << a.ns_log)) / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic", "config": workload_config(a, a.gpus),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(a, rank, world, local_rank):
+    import torch
+
+    hj = load_module("hashjoin_scm_b200", PKG_DIR / "__init__.py")
+    hj.lib()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+    nR, nS = 1 << a.nr_log, 1 << a.ns_log
+    stream = torch.cuda.current_stream(dev)
+    R = torch.empty((nR, 2), dtype=torch.int64, device=dev)
+    S = torch.empty((nS, 2), dtype=torch.int64, device=dev)
+    hj.gen_fast_device(nR, nS, R.data_ptr(), S.data_ptr(), seed=12345 + rank, stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    want = hj.pkfk_closed_form(nR, nS)
+    ctx = hj.Context(local_rank)
+    flags = hj.HJ_F_PHASE_TIMES
+
+    def step():
+        r = hj.join(a.algo, R, S, on_device=True, bits=a.bits, passes=a.passes, device=local_rank,
+                    stream=stream.cuda_stream, flags=flags, ctx=ctx)
+        if (r.matched_cnt, r.checksum) != want:
+            raise RuntimeError(f"wrong result {(r.matched_cnt, r.checksum)} != {want}")
+        return r
+
+    for _ in range(a.warmup):
+        step()
+    bus = None
+    try:
+        pr = torch.cuda.get_device_properties(dev)
+        bus = "%02x:%02x.0" % (int(pr.pci_bus_id), int(pr.pci_device_id))
+    except (AttributeError, TypeError, ValueError):
+        pass
+    sampler = ClockSampler(bus)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    results = [step() for _ in range(a.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * (nR + nS) * a.steps / (ms / 1e3)
+    phases = {name: statistics.mean(r.phase[i] for r in results) for i, name in enumerate(hj.PHASES)}
+    launches = sum(r.kernel_launches for r in results)
+
+    # Roofline of the dominant kernel: a partition pass reads and writes every tuple once (32 B).
+    peak, peak_kind = measured_peaks()
+    pass_s = statistics.mean([phases["pass1"], phases["pass2"]]) if a.passes == 2 else phases["pass1"]
+    scatter_bytes = 32 * (nR + nS)
+    achieved = scatter_bytes / pass_s / 1e9
+    prof = traffic_profile("scatter_kernel")
+    traffic = prof["dram_bytes_per_tuple"] * (nR + nS) if prof else None
+    roofline = {"kernel": "scatter_kernel (one radix partition pass)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": scatter_bytes, "launch_ms": pass_s * 1e3}
+    pipe_bytes = 16 * (2 * a.passes + 1) * (nR + nS)
+    step_s = ms / 1e3 / a.steps
+    pipeline = {"algorithmic_bytes_per_tuple": 16 * (2 * a.passes + 1), "bytes_per_step": pipe_bytes,
+                "achieved_gbs": pipe_bytes / step_s / 1e9, "frac": pipe_bytes / step_s / 1e9 / peak,
+                "phase_ms": {k: v * 1e3 for k, v in phases.items()}}
+
+    # End to end through the public C ABI with pinned host relations: copy in, join, read result.
+    e2e = None
+    if not a.no_e2e:
+        Rh = torch.empty((nR, 2), dtype=torch.int64, pin_memory=True)
+        Sh = torch.empty((nS, 2), dtype=torch.int64, pin_memory=True)
+        Rh.copy_(R)
+        Sh.copy_(S)
+        del R, S
+        torch.cuda.empty_cache()
+        host_ctx = hj.Context(local_rank)
+
+        def e2e_step():
+            r = hj.join(a.algo, (Rh.data_ptr(), nR), (Sh.data_ptr(), nS), bits=a.bits, passes=a.passes,
+                        device=local_rank, flags=hj.HJ_F_PINNED_HOST, ctx=host_ctx)
+            if (r.matched_cnt, r.checksum) != want:
+                raise RuntimeError("wrong e2e result")
+            return r
+
+        e2e_step()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            e2e_step()
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": world * (nR + nS) * a.e2e_steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": (nR + nS) * 16, "d2h_bytes_per_step": 64,
+               "steps": a.e2e_steps, "ms_per_step": el / a.e2e_steps * 1e3}
+        host_ctx.close()
+        del Rh, Sh
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            thr, sample, threads, kind = cpu_reference_run(hj, a, trials=2, sample_log=a.cpu_sample_log)
+            cpu = {"value": statistics.mean(thr), "unit": UNIT, "cores": threads, "kind": kind, "sample": sample}
+        except Exception as exc:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {exc}"}
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": workload_config(a, world),
+            "roofline": roofline, "pipeline": pipeline, "e2e": e2e, "cpu_baseline": cpu,
+            "clocks": clocks, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference_arm(a, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        return run_ours(a, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -49,6 +49,8 @@ HJ_E_NOT_FOUND, HJ_E_IO, HJ_E_OVERFLOW, HJ_E_BUDGET = 6, 7, 8, 9
 
 HJ_F_NO_TIMING = 0x1
 HJ_F_PINNED_HOST = 0x2
+HJ_F_PHASE_TIMES = 0x4
+PHASES = ("hist", "plan", "pass1", "pass2", "join", "large")
 
 
 class Params(ctypes.Structure):
@@ -74,10 +76,15 @@ class Result(ctypes.Structure):
         ("status", ctypes.c_int),
         ("physical_passes", ctypes.c_int),
         ("large_partitions", ctypes.c_uint64),
+        ("phase", ctypes.c_double * 6),
+        ("kernel_launches", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("phase", "pad")}
+        d["phase"] = list(self.phase)
+        return d
 
 
 class JoinError(RuntimeError):

@@ -19,6 +19,7 @@ struct hj_ctx {
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_h2d = nullptr, ev_start = nullptr, ev_mid = nullptr, ev_end = nullptr;
+    cudaEvent_t ev_ph[HJ_PH_COUNT + 1] = {};
     char *arena = nullptr;
     size_t arena_bytes = 0;
     JoinAccum *acc_host = nullptr;  // pinned
@@ -66,7 +67,7 @@ void resolve_params(const hj_params_t *p, hj_params_t *out) {
 
 bool is_phj(hj_algo_t a) { return a == HJ_ALGO_PHJ_RADIX_BC || a == HJ_ALGO_PHJ_RADIX_LP; }
 
-int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, bool host_inputs,
+int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, bool host_inputs, int num_sms,
                  size_t *bytes) {
     size_t need = kAccBytes;
     if (host_inputs) need += align256(nR * 16) + align256(nS * 16);
@@ -74,7 +75,7 @@ int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, boo
         hj::RadixGeom g;
         int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &g);
         if (rc) return rc;
-        need += hj::phj_scratch_bytes(g, nR, nS);
+        need += hj::phj_scratch_bytes(g, nR, nS, num_sms);
     } else {
         need += align256(hj::nphj_scratch_bytes(nR, p.table_load));
     }
@@ -174,6 +175,7 @@ int hj_ctx_create(int device, hj_ctx_t **out) {
     CU_OR(cudaEventCreate(&c->ev_start), HJ_E_DEVICE);
     CU_OR(cudaEventCreate(&c->ev_mid), HJ_E_DEVICE);
     CU_OR(cudaEventCreate(&c->ev_end), HJ_E_DEVICE);
+    for (int i = 0; i <= HJ_PH_COUNT; i++) CU_OR(cudaEventCreate(&c->ev_ph[i]), HJ_E_DEVICE);
     CU_OR(cudaMallocHost(&c->acc_host, sizeof(JoinAccum)), HJ_E_OOM);
     *out = c;
     return HJ_OK;
@@ -191,6 +193,7 @@ int hj_ctx_destroy(hj_ctx_t *c) {
         cudaEventDestroy(c->ev_start);
         cudaEventDestroy(c->ev_mid);
         cudaEventDestroy(c->ev_end);
+        for (int i = 0; i <= HJ_PH_COUNT; i++) cudaEventDestroy(c->ev_ph[i]);
         if (c->stream) cudaStreamDestroy(c->stream);
     }
     delete c;
@@ -204,7 +207,7 @@ int hj_ctx_reserve(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, size_t n
     hj_params_t p;
     resolve_params(pin, &p);
     size_t need = 0;
-    int rc = scratch_need(algo, p, nR, nS, !p.inputs_on_device, &need);
+    int rc = scratch_need(algo, p, nR, nS, !p.inputs_on_device, c->num_sms, &need);
     if (rc) return rc;
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
@@ -231,12 +234,15 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     std::lock_guard<std::mutex> lk(c->mu);
     const bool host_in = !p.inputs_on_device;
     size_t need = 0;
-    int rc = scratch_need(algo, p, nR, nS, host_in, &need);
+    int rc = scratch_need(algo, p, nR, nS, host_in, c->num_sms, &need);
     if (rc) return out->status = rc;
     rc = ensure_arena(c, need);
     if (rc) return out->status = rc;
     cudaStream_t st = p.stream ? (cudaStream_t)p.stream : c->stream;
     const bool timing = !(p.flags & HJ_F_NO_TIMING);
+    const bool phases = (p.flags & HJ_F_PHASE_TIMES) != 0;
+    cudaEvent_t *ph = phases ? c->ev_ph : nullptr;
+    uint32_t launches = 0;
 
     char *cur = c->arena;
     JoinAccum *acc = reinterpret_cast<JoinAccum *>(cur);
@@ -258,13 +264,13 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     if (timing) CU_OR(cudaEventRecord(c->ev_start, st), out->status = HJ_E_DEVICE);
     if (is_phj(algo)) {
         hj::PhjScratch s;
-        hj::phj_carve(geom, nR, nS, cur, &s);
+        hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s);
         rc = hj::phj_enqueue(geom, algo == HJ_ALGO_PHJ_RADIX_LP, dR, nR, dS, nS, s, acc, st,
-                             timing ? c->ev_mid : nullptr, c->num_sms);
+                             timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
     } else {
         const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
         rc = hj::nphj_enqueue(algo == HJ_ALGO_NPHJ_LP, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
-                              timing ? c->ev_mid : nullptr, c->num_sms);
+                              timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
     }
     if (rc) {
         cudaStreamSynchronize(st);
@@ -287,6 +293,14 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
         out->total = out->buildpart + out->probejoin;
         out->h2d = h * 1e-3;
     }
+    if (phases) {
+        for (int i = 0; i < HJ_PH_COUNT; i++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, c->ev_ph[i], c->ev_ph[i + 1]);
+            out->phase[i] = ms * 1e-3;
+        }
+    }
+    out->kernel_launches = launches;
     out->status = map_error_bits(c->acc_host->error);
     return out->status;
 }

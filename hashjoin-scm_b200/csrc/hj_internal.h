@@ -30,40 +30,43 @@ constexpr int kTile = kScatterThreads * kScatterItems;  // tuples per partition 
 constexpr int kJoinThreads = 1024;
 constexpr int kSmemCap = 10240;        // largest build partition joined in shared memory
 constexpr int kProbeChunk = 1 << 16;   // S tuples per join work item
-constexpr int kMaxPass2Segs = 512;     // 2 relations x 256 pass-1 partitions
 
 // Device scratch layout of one partitioned join, carved out of a context arena.
 struct PhjScratch {
-    uint32_t *hist;         // [2][2^B]
-    uint64_t *start;        // [2][2^B + 1] final partition starts
-    void *segs;             // pass segment tables (2 passes)
-    uint64_t *obase;        // [2 passes][max segs][256] digit output bases
-    uint32_t *counters;     // tile counters, tile totals, item counts (memset per join)
-    uint32_t *status;       // look-back status words (memset per pass)
-    size_t status_words;
-    void *items;            // join work items
+    uint64_t chunk;          // tuples per input chunk
+    uint32_t cR, cS;         // chunks of R and of S
+    uint32_t *chunk_hist;    // [chunk][2^B] joint digit histogram of each chunk
+    uint32_t *prefix;        // [chunk][2^B] exclusive prefix over the chunks of the same relation
+    uint32_t *total;         // [2][2^B]
+    uint64_t *start;         // [2][2^B + 1] final partition starts
+    uint64_t *unit_off;      // [chunk][F1] start of (chunk, d1) in the pass-1 output
+    uint32_t *unit_cnt;      // [chunk][F1] its size
+    uint32_t *counters;      // work-item counters, totals, error word (memset per join)
+    void *items;             // join work items
     size_t max_items;
-    void *large;            // large-partition descriptors
+    void *large;             // large-partition descriptors
     size_t max_large;
-    uint32_t *large_table;  // head/next chains for large partitions (>= 12 B per R tuple)
+    uint32_t *large_table;   // head/next chains for large partitions (>= 12 B per R tuple)
     size_t large_table_words;
-    ulonglong2 *tmp1;       // pass-1 output [nR + nS]
-    ulonglong2 *tmp2;       // pass-2 output [nR + nS] (== tmp1 for one pass)
+    ulonglong2 *tmp1;        // pass-1 output [nR + nS]
+    ulonglong2 *tmp2;        // pass-2 output [nR + nS] (== tmp1 for one pass)
 };
 
-size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS);
-void phj_carve(const RadixGeom &g, size_t nR, size_t nS, char *base, PhjScratch *s);
+size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms);
+void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base, PhjScratch *s);
 
 // Enqueue a full partitioned join on `st`; matches/checksum accumulate into acc (zeroed by caller).
 // ev_mid, if non-null, is recorded between the partition phase and the join phase.
+// ph, if non-null, holds HJ_PH_COUNT + 1 events recorded at the phase boundaries; *launches receives
+// the number of kernels enqueued.
 int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                int num_sms);
+                int num_sms, cudaEvent_t *ph, uint32_t *launches);
 
 // Non-partitioned joins on a global open-addressing table.
 size_t nphj_scratch_bytes(size_t nR, double load);
 int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                 int num_sms);
+                 int num_sms, cudaEvent_t *ph, uint32_t *launches);
 
 }  // namespace hj

@@ -200,7 +200,7 @@ size_t nphj_scratch_bytes(size_t nR, double load) {
 
 int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                 int num_sms) {
+                 int num_sms, cudaEvent_t *ph, uint32_t *launches) {
     const unsigned long long cap = nphj_cap(nR, load);
     if (cap * 16 + 256 > table_bytes) return HJ_E_INVAL;
     NphjArgs a;
@@ -217,6 +217,8 @@ int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, s
     HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
     HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));
     const int grid = num_sms * 8;
+    // Phase slots: build spans [0, 1], probe spans [4, 5]; the others stay empty.
+    if (ph) HJ_CU(cudaEventRecord(ph[0], st));
     nphj_build<<<grid, 256, 0, st>>>(a);
     if (lp) {
         nphj_lp_refill<<<grid, 256, 0, st>>>(a);
@@ -225,8 +227,16 @@ int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, s
     }
     HJ_CU(cudaGetLastError());
     if (ev_mid) HJ_CU(cudaEventRecord(ev_mid, st));
+    if (ph) {
+        for (int i = 1; i <= 4; i++) HJ_CU(cudaEventRecord(ph[i], st));
+    }
     nphj_probe<<<grid, 256, 0, st>>>(a);
     HJ_CU(cudaGetLastError());
+    if (ph) {
+        HJ_CU(cudaEventRecord(ph[5], st));
+        HJ_CU(cudaEventRecord(ph[6], st));
+    }
+    if (launches) *launches = lp ? 5u : 2u;
     return HJ_OK;
 }
 

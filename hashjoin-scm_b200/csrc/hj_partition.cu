@@ -10,18 +10,25 @@
 //           counted; lp_join (phj.c:574-680): open addressing, the probe stops at the first equal key,
 //           which is the first R tuple of the partition in input order.
 //
-// B200 pipeline (all on one stream, no host round trip):
-//   hist_kernel     one read of R and S: joint histogram of the low B key bits in shared memory
-//   plan_kernel     exclusive scans -> final partition starts, pass segment tables, join work items
-//   scatter_kernel  per pass: persistent CTAs take 2048-tuple tiles in order, rank tuples per digit with
-//                   warp match (stable), publish per-digit counts and resolve the tile's output offsets
-//                   with a decoupled look-back over predecessor tiles, stage the tile in shared memory
-//                   sorted by digit and write each digit run with coalesced 16-byte streaming stores
-//                   (the shared-memory analogue of the reference's SWWCB + non-temporal flush)
-//   join_small      persistent CTAs take (partition, S chunk) items; R_p arrives in shared memory by one
-//                   TMA bulk copy; the bucket chains (u16 head/next) are built with shared-memory atomics;
-//                   S is streamed with evict-first vector loads
-//   join_large_*    partitions whose R side exceeds shared memory: chains in global memory
+// B200 pipeline (one stream, no host round trip). Each relation is cut into equal chunks (about three
+// per SM); a chunk plays the role of one reference thread's contiguous input slice.
+//   hist_chunk_kernel  one read of R and S: per chunk, the joint histogram of the low B key bits (the
+//                      pass-1 digit and the pass-2 digit together) in shared memory
+//   colscan_kernel     per bin, exclusive prefix over the chunks of a relation (the reference's
+//                      cross-thread output_offset sums, phj.c:188-200, for both passes at once)
+//   plan_kernel        final partition starts, join work items, large partitions
+//   units_kernel       per (chunk, pass-1 partition): its size and its start in the pass-1 output
+//   scatter_kernel     per pass: persistent CTAs take work items (pass 1: chunks; pass 2: (chunk,
+//                      pass-1 partition) units) whose per-digit output offsets are known in advance;
+//                      each 2048-tuple tile arrives by a TMA bulk copy (the next one is in flight while the
+//                      current one is processed), is ranked per digit with warp match (stable), staged
+//                      in shared memory sorted by digit and written back as coalesced 16-byte streaming
+//                      stores per digit run (the shared-memory analogue of the reference's SWWCB +
+//                      non-temporal flush). No inter-CTA waiting.
+//   join_small         persistent CTAs take (partition, S chunk) items; R_p arrives in shared memory by one
+//                      TMA bulk copy; the bucket chains (u16 head/next) are built with shared-memory atomics;
+//                      S is streamed with evict-first vector loads
+//   join_large_*       partitions whose R side exceeds shared memory: chains in global memory
 #include <cstdio>
 
 #include "hj_common.cuh"
@@ -32,15 +39,6 @@ namespace hj {
 // ------------------------------------------------------------------------------------------------
 // Device-side plan structures
 // ------------------------------------------------------------------------------------------------
-struct Seg {
-    const tuple_v *in;
-    tuple_v *out;
-    uint64_t count;
-    uint64_t out_len;     // bound for output indices
-    uint32_t first_tile;  // first global tile of this segment
-    uint32_t pad;
-};
-
 struct JoinItem {
     uint64_t r_begin;  // index into the final R buffer
     uint64_t s_begin;  // index into the final S buffer
@@ -60,15 +58,11 @@ struct LargePart {
 
 // counters[] slots
 enum : int {
-    kCtrTile1 = 0,
-    kCtrTile2 = 1,
-    kCtrNTiles1 = 2,
-    kCtrNTiles2 = 3,
-    kCtrNSegs1 = 4,
-    kCtrNSegs2 = 5,
+    kCtrItem1 = 0,       // scatter pass-1 work-item counter
+    kCtrItem2 = 1,       // scatter pass-2 work-item counter
     kCtrNItems = 6,
     kCtrNLarge = 7,
-    kCtrItem = 8,
+    kCtrItem = 8,        // join work-item counter
     kCtrLargeR = 9,      // total R tuples in large partitions (u32 pairs: lo, hi)
     kCtrLargeS = 11,     // total S tuples in large partitions (lo, hi)
     kCtrLargeWords = 13, // table words used (lo, hi)
@@ -76,10 +70,11 @@ enum : int {
     kNumCounters = 16
 };
 
-constexpr uint32_t kFlagAgg = 1u << 30;
-constexpr uint32_t kFlagPrefix = 2u << 30;
-constexpr uint32_t kValueMask = (1u << 30) - 1;
-constexpr int kSpinLimit = 1 << 22;
+// Chunking of the two relations (identical for the histogram and both scatter passes).
+struct ChunkGeom {
+    uint64_t chunk;  // tuples per chunk (a multiple of the tile)
+    uint32_t cR, cS; // chunks of R, chunks of S (R's come first)
+};
 
 __device__ __forceinline__ uint64_t ld_u64_pair(const uint32_t *p) {
     return (uint64_t)p[0] | ((uint64_t)p[1] << 32);
@@ -87,15 +82,6 @@ __device__ __forceinline__ uint64_t ld_u64_pair(const uint32_t *p) {
 __device__ __forceinline__ void st_u64_pair(uint32_t *p, uint64_t v) {
     p[0] = (uint32_t)v;
     p[1] = (uint32_t)(v >> 32);
-}
-
-__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
-    uint32_t v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed_u32(uint32_t *p, uint32_t v) {
-    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 __host__ __device__ __forceinline__ uint32_t ceil_div_u64(uint64_t a, uint64_t b) {
@@ -106,30 +92,69 @@ __device__ __forceinline__ uint32_t next_pow2_u32(uint32_t x) {
     return x <= 1 ? 1u : 1u << (32 - __clz(x - 1));
 }
 
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Bounded wait for the completion of phase `parity` of an mbarrier.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 24); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// TMA bulk copy global -> shared of `bytes` (a multiple of 16, <= 1 MiB per phase), completing on
+// `bar`. Issued by one thread.
+__device__ __forceinline__ void tma_load_1d(void *dst_smem, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    const char *s = reinterpret_cast<const char *>(src);
+    const uint32_t d = smem_addr(dst_smem);
+    for (uint32_t off = 0; off < bytes; off += 32768u) {
+        const uint32_t sz = bytes - off < 32768u ? bytes - off : 32768u;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d + off),
+            "l"(s + off), "r"(sz), "r"(bar)
+            : "memory");
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
-// 1. Histogram of the low `bits` key bits over R (blocks [0, gR)) and S (blocks [gR, grid)).
+// 1. Per-chunk joint histogram of the low `bits` key bits. One CTA per chunk; every bin is written.
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) hist_kernel(const tuple_v *__restrict__ R, size_t nR,
-                                                    const tuple_v *__restrict__ S, size_t nS, int bits,
-                                                    uint32_t *__restrict__ hist, int gR) {
+__global__ void __launch_bounds__(512) hist_chunk_kernel(const tuple_v *__restrict__ R, size_t nR,
+                                                         const tuple_v *__restrict__ S, size_t nS, int bits,
+                                                         ChunkGeom cg, uint32_t *__restrict__ chunk_hist) {
     extern __shared__ uint32_t sh_hist[];
     const int nbins = 1 << bits;
     const uint64_t mask = (uint64_t)nbins - 1;
-    const int rel = (int)blockIdx.x < gR ? 0 : 1;
-    const int b = rel ? (int)blockIdx.x - gR : (int)blockIdx.x;
-    const int G = rel ? (int)gridDim.x - gR : gR;
+    const uint32_t c = blockIdx.x;
+    const int rel = c < cg.cR ? 0 : 1;
+    const uint64_t lc = rel ? c - cg.cR : c;
     const tuple_v *in = rel ? S : R;
-    const size_t n = rel ? nS : nR;
+    const uint64_t n = rel ? nS : nR;
     for (int v = threadIdx.x; v < nbins; v += blockDim.x) sh_hist[v] = 0;
     __syncthreads();
-    const size_t chunk = (n + G - 1) / G;
-    const size_t lo = (size_t)b * chunk;
-    const size_t hi = lo + chunk < n ? lo + chunk : n;
-    const size_t step = (size_t)blockDim.x;
-    size_t i = lo + threadIdx.x;
+    const uint64_t lo = lc * cg.chunk;
+    const uint64_t hi = lo + cg.chunk < n ? lo + cg.chunk : n;
+    const uint64_t step = blockDim.x;
+    uint64_t i = lo + threadIdx.x;
     for (; i + 3 * step < hi; i += 4 * step) {
-        tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + step);
-        tuple_v t2 = ld_stream(in + i + 2 * step), t3 = ld_stream(in + i + 3 * step);
+        const tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + step);
+        const tuple_v t2 = ld_stream(in + i + 2 * step), t3 = ld_stream(in + i + 3 * step);
         atomicAdd(&sh_hist[t0.x & mask], 1u);
         atomicAdd(&sh_hist[t1.x & mask], 1u);
         atomicAdd(&sh_hist[t2.x & mask], 1u);
@@ -137,27 +162,51 @@ __global__ void __launch_bounds__(1024) hist_kernel(const tuple_v *__restrict__ 
     }
     for (; i < hi; i += step) atomicAdd(&sh_hist[ld_stream(in + i).x & mask], 1u);
     __syncthreads();
-    uint32_t *out = hist + (size_t)rel * nbins;
-    for (int v = threadIdx.x; v < nbins; v += blockDim.x) {
-        uint32_t c = sh_hist[v];
-        if (c) atomicAdd(&out[v], c);
-    }
+    uint32_t *out = chunk_hist + (size_t)c * nbins;
+    for (int v = threadIdx.x; v < nbins; v += blockDim.x) out[v] = sh_hist[v];
 }
 
 // ------------------------------------------------------------------------------------------------
-// 2. Plan: partition starts, segment tables of both passes, join work items, large partitions.
-//    One CTA of 1024 threads.
+// 2. Per bin, exclusive prefix over the chunks of its relation, and the relation totals.
+// ------------------------------------------------------------------------------------------------
+__global__ void colscan_kernel(const uint32_t *__restrict__ chunk_hist, uint32_t *__restrict__ prefix,
+                               uint32_t *__restrict__ total, int nbins, ChunkGeom cg) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= 2u * (uint32_t)nbins) return;
+    const int rel = g >= (uint32_t)nbins;
+    const uint32_t v = rel ? g - nbins : g;
+    const uint32_t c0 = rel ? cg.cR : 0, c1 = rel ? cg.cR + cg.cS : cg.cR;
+    uint32_t run = 0;
+    uint32_t c = c0;
+    constexpr int U = 16;
+    for (; c + U <= c1; c += U) {
+        uint32_t x[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) x[u] = chunk_hist[(size_t)(c + u) * nbins + v];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            prefix[(size_t)(c + u) * nbins + v] = run;
+            run += x[u];
+        }
+    }
+    for (; c < c1; c++) {
+        const uint32_t x = chunk_hist[(size_t)c * nbins + v];
+        prefix[(size_t)c * nbins + v] = run;
+        run += x;
+    }
+    total[(size_t)rel * nbins + v] = run;
+}
+
+// ------------------------------------------------------------------------------------------------
+// 3. Plan: final partition starts (in (pass-1 digit, pass-2 digit) order), join work items, large
+//    partitions. One CTA of 1024 threads.
 // ------------------------------------------------------------------------------------------------
 struct PlanArgs {
     int bits, passes, b1, F1, F2;
-    const tuple_v *R, *S;
     uint64_t nR, nS;
-    const uint32_t *hist;
-    uint64_t *start;
-    Seg *segs;        // [2][kMaxPass2Segs + 1]
-    uint64_t *obase;  // [2][kMaxPass2Segs][256]
+    const uint32_t *total;  // [2][2^B]
+    uint64_t *start;        // [2][2^B + 1]
     uint32_t *counters;
-    tuple_v *tmp1, *tmp2;
     JoinItem *items;
     uint64_t max_items;
     LargePart *large;
@@ -175,99 +224,26 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
     __shared__ uint32_t tmp[32];
     const int tid = threadIdx.x;
     const int nparts = 1 << a.bits;
-    const uint64_t nrel[2] = {a.nR, a.nS};
-
-    // Final partition starts in (d1, d2) order.
     for (int rel = 0; rel < 2; rel++) {
         uint64_t *start = a.start + (size_t)rel * (nparts + 1);
-        const uint32_t *hist = a.hist + (size_t)rel * nparts;
+        const uint32_t *tot = a.total + (size_t)rel * nparts;
         uint64_t running = 0;
         for (int c = 0; c < nparts; c += 1024) {
             const int f = c + tid;
-            const uint32_t cnt = f < nparts ? hist[part_to_value(f, a.passes, a.b1, a.F2)] : 0u;
-            uint32_t tot;
-            const uint32_t ex = block_excl_scan_u32(cnt, tmp, &tot);
+            const uint32_t cnt = f < nparts ? tot[part_to_value(f, a.passes, a.b1, a.F2)] : 0u;
+            uint32_t tsum;
+            const uint32_t ex = block_excl_scan_u32(cnt, tmp, &tsum);
             if (f < nparts) start[f] = running + ex;
-            running += tot;
+            running += tsum;
         }
         if (tid == 0) start[nparts] = running;
     }
     __syncthreads();
 
-    tuple_v *fin = a.passes == 2 ? a.tmp2 : a.tmp1;
-    const tuple_v *inrel[2] = {a.R, a.S};
-    // Pass-1 segments: one per relation.
-    if (tid == 0) {
-        uint32_t ft = 0;
-        for (int rel = 0; rel < 2; rel++) {
-            Seg s;
-            s.in = inrel[rel];
-            s.out = a.tmp1 + (rel ? a.nR : 0);
-            s.count = nrel[rel];
-            s.out_len = nrel[rel];
-            s.first_tile = ft;
-            s.pad = 0;
-            a.segs[rel] = s;
-            ft += ceil_div_u64(nrel[rel], kTile);
-        }
-        Seg sentinel = {};
-        sentinel.first_tile = ft;
-        a.segs[2] = sentinel;
-        a.counters[kCtrNTiles1] = ft;
-        a.counters[kCtrNSegs1] = 2;
-    }
-    for (int idx = tid; idx < 2 * a.F1; idx += blockDim.x) {
-        const int rel = idx / a.F1, d1 = idx % a.F1;
-        a.obase[(size_t)rel * 256 + d1] = a.start[(size_t)rel * (nparts + 1) + (size_t)d1 * a.F2];
-    }
-    // Pass-2 segments: one per (relation, pass-1 partition).
-    if (a.passes == 2) {
-        Seg *segs2 = a.segs + (kMaxPass2Segs + 1);
-        uint64_t *obase2 = a.obase + (size_t)kMaxPass2Segs * 256;
-        const int nseg = 2 * a.F1;  // <= 512 <= blockDim
-        uint32_t ntile = 0;
-        uint64_t b0 = 0, b1e = 0;
-        int rel = 0, d1 = 0;
-        if (tid < nseg) {
-            rel = tid / a.F1;
-            d1 = tid % a.F1;
-            const uint64_t *st = a.start + (size_t)rel * (nparts + 1);
-            b0 = st[(size_t)d1 * a.F2];
-            b1e = st[(size_t)(d1 + 1) * a.F2];
-            ntile = ceil_div_u64(b1e - b0, kTile);
-        }
-        uint32_t tot;
-        const uint32_t ft = block_excl_scan_u32(ntile, tmp, &tot);
-        if (tid < nseg) {
-            Seg s;
-            s.in = a.tmp1 + (rel ? a.nR : 0) + b0;
-            s.out = fin + (rel ? a.nR : 0);
-            s.count = b1e - b0;
-            s.out_len = nrel[rel];
-            s.first_tile = ft;
-            s.pad = 0;
-            segs2[tid] = s;
-        }
-        if (tid == 0) {
-            Seg sentinel = {};
-            sentinel.first_tile = tot;
-            segs2[nseg] = sentinel;
-            a.counters[kCtrNTiles2] = tot;
-            a.counters[kCtrNSegs2] = nseg;
-        }
-        for (int idx = tid; idx < nseg * a.F2; idx += blockDim.x) {
-            const int s = idx / a.F2, d2 = idx % a.F2;
-            const int r2 = s / a.F1, q1 = s % a.F1;
-            obase2[(size_t)s * 256 + d2] =
-                a.start[(size_t)r2 * (nparts + 1) + (size_t)q1 * a.F2 + d2];
-        }
-    }
-    __syncthreads();
-
-    // Join work items and large partitions.
+    // Join work items (partitions with both sides non-empty, src/algo/phj.c:459-491) and large
+    // partitions.
     const uint64_t *stR = a.start, *stS = a.start + (nparts + 1);
     uint64_t item_run = 0, large_run = 0;
-    __syncthreads();
     for (int c = 0; c < nparts; c += 1024) {
         const int f = c + tid;
         uint64_t nr = 0, ns = 0;
@@ -322,7 +298,6 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
         large_run += ltot;
         __syncthreads();
     }
-    // Offsets of the large partitions (sequential: there are few).
     __syncthreads();
     if (tid == 0) {
         const uint64_t nl = large_run < a.max_large ? large_run : a.max_large;
@@ -336,83 +311,225 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
             rf += lp.r_len;
             sf += lp.s_len;
         }
-        if (off > a.large_table_words) atomicOr(&a.counters[kCtrErr], kErrCapacity);
+        const bool fits = off <= a.large_table_words;
+        if (!fits) atomicOr(&a.counters[kCtrErr], kErrCapacity);
         a.counters[kCtrNItems] = (uint32_t)(item_run < a.max_items ? item_run : a.max_items);
         a.counters[kCtrNLarge] = (uint32_t)nl;
-        st_u64_pair(&a.counters[kCtrLargeR], off > a.large_table_words ? 0 : rf);
-        st_u64_pair(&a.counters[kCtrLargeS], off > a.large_table_words ? 0 : sf);
-        st_u64_pair(&a.counters[kCtrLargeWords], off > a.large_table_words ? 0 : off);
+        st_u64_pair(&a.counters[kCtrLargeR], fits ? rf : 0);
+        st_u64_pair(&a.counters[kCtrLargeS], fits ? sf : 0);
+        st_u64_pair(&a.counters[kCtrLargeWords], fits ? off : 0);
     }
 }
 
 // ------------------------------------------------------------------------------------------------
-// 3. Stable scatter of one pass with decoupled look-back.
+// 4. Units: for every chunk c and pass-1 digit d1, the number of the chunk's tuples with that digit
+//    and where they start in the pass-1 output: start[d1 * F2] + sum over d2 of prefix[c][(d1, d2)].
+//    One warp per (c, d1).
+// ------------------------------------------------------------------------------------------------
+__global__ void units_kernel(const uint32_t *__restrict__ chunk_hist, const uint32_t *__restrict__ prefix,
+                             const uint64_t *__restrict__ start, int bits, int b1, int F1, int F2,
+                             ChunkGeom cg, uint64_t *__restrict__ unit_off, uint32_t *__restrict__ unit_cnt) {
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nchunks = cg.cR + cg.cS;
+    if (wid >= nchunks * (uint32_t)F1) return;
+    const uint32_t c = wid / F1, d1 = wid % F1;
+    const int rel = c < cg.cR ? 0 : 1;
+    const int nbins = 1 << bits;
+    const uint32_t *h = chunk_hist + (size_t)c * nbins;
+    const uint32_t *p = prefix + (size_t)c * nbins;
+    uint64_t cnt = 0, pre = 0;
+    for (int d2 = lane; d2 < F2; d2 += 32) {
+        const uint32_t v = d1 | ((uint32_t)d2 << b1);
+        cnt += h[v];
+        pre += p[v];
+    }
+    cnt = warp_sum_u64(cnt);
+    pre = warp_sum_u64(pre);
+    if (lane == 0) {
+        unit_cnt[wid] = (uint32_t)cnt;
+        unit_off[wid] = start[(size_t)rel * (nbins + 1) + (size_t)d1 * F2] + pre;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// 5. Stable scatter of one pass, from precomputed per-item digit offsets.
 // ------------------------------------------------------------------------------------------------
 struct ScatterArgs {
-    const Seg *segs;
-    const uint64_t *obase;  // [seg][256]
+    int pass;        // 0: by the pass-1 digit, per chunk; 1: by the pass-2 digit, per (chunk, d1) unit
+    int F, shift;    // digit of this pass: (key >> shift) & (F - 1)
+    int bits, b1, F1, F2;
+    ChunkGeom cg;
+    const tuple_v *inR, *inS;   // pass input (pass 0: the relations; pass 1: the pass-1 output)
+    tuple_v *outR, *outS;       // pass output
+    uint64_t nR, nS;
+    const uint32_t *prefix;     // [chunk][2^B]
+    const uint64_t *start;      // [2][2^B + 1]
+    const uint64_t *unit_off;   // [chunk][F1]
+    const uint32_t *unit_cnt;   // [chunk][F1]
     uint32_t *counters;
-    int ctr_tile, ctr_ntiles, ctr_nsegs;
-    int F, shift;
-    uint32_t *status;  // [tile][F]
-    uint64_t status_words;
+    int ctr_item;
 };
 
+// A tile claimed for processing: its source, length, output region and owning work item.
+struct TileSlot {
+    const tuple_v *in;
+    tuple_v *out;
+    uint64_t out_len;
+    uint32_t item;   // work item (valid flag: item != ~0u)
+    uint32_t cnt;    // tuples in this tile
+    uint32_t first;  // first tile of its item: the item's digit offsets must be loaded
+    uint32_t pad;
+};
+
+// Thread-0 state of the work-item iterator.
+struct ItemIter {
+    uint32_t item = ~0u;
+    const tuple_v *in = nullptr;
+    tuple_v *out = nullptr;
+    uint64_t len = 0, out_len = 0, done = 0;
+};
+
+__device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item, ItemIter &it) {
+    const ChunkGeom &cg = a.cg;
+    it.item = item;
+    it.done = 0;
+    if (a.pass == 0) {
+        const uint32_t c = item;
+        const int rel = c < cg.cR ? 0 : 1;
+        const uint64_t lc = rel ? c - cg.cR : c;
+        const uint64_t n = rel ? a.nS : a.nR;
+        const uint64_t lo = lc * cg.chunk;
+        it.len = lo < n ? (n - lo < cg.chunk ? n - lo : cg.chunk) : 0;
+        it.in = (rel ? a.inS : a.inR) + lo;
+        it.out = rel ? a.outS : a.outR;
+        it.out_len = n;
+    } else {
+        const uint32_t c = item / a.F1;
+        const int rel = c < cg.cR ? 0 : 1;
+        it.len = a.unit_cnt[item];
+        it.in = (rel ? a.inS : a.inR) + a.unit_off[item];
+        it.out = rel ? a.outS : a.outR;
+        it.out_len = rel ? a.nS : a.nR;
+    }
+}
+
+// Claim the next tile (thread 0 only): continue the current item or claim new items until one has
+// tuples. Returns a slot with item == ~0u when the work is exhausted.
+template <int T>
+__device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it, uint32_t nitems) {
+    TileSlot s;
+    while (it.item == ~0u || it.done >= it.len) {
+        const uint32_t item = atomicAdd(&a.counters[a.ctr_item], 1u);
+        if (item >= nitems) {
+            s.item = ~0u;
+            s.in = nullptr;
+            s.out = nullptr;
+            s.out_len = 0;
+            s.cnt = 0;
+            s.first = 0;
+            s.pad = 0;
+            it.item = ~0u;
+            it.len = 0;
+            it.done = 0;
+            return s;
+        }
+        item_decode(a, item, it);
+    }
+    s.item = it.item;
+    s.in = it.in + it.done;
+    s.out = it.out;
+    s.out_len = it.out_len;
+    s.cnt = (uint32_t)(it.len - it.done < (uint64_t)T ? it.len - it.done : (uint64_t)T);
+    s.first = it.done == 0;
+    s.pad = 0;
+    it.done += s.cnt;
+    return s;
+}
+
 template <int THREADS, int ITEMS>
-__global__ void __launch_bounds__(THREADS, 4) scatter_kernel(ScatterArgs a) {
+__global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
     constexpr int T = THREADS * ITEMS;
     constexpr int NW = THREADS / 32;
-    extern __shared__ __align__(16) unsigned char smem[];
-    tuple_v *stage = reinterpret_cast<tuple_v *>(smem);
-    long long *gbase = reinterpret_cast<long long *>(stage + T);  // [256]
-    uint32_t *whist = reinterpret_cast<uint32_t *>(gbase + 256);  // [NW][F]
-    uint32_t *tdstart = whist + NW * a.F;                         // [256]
-    uint32_t *segft = tdstart + 256;                              // [nsegs + 1]
+    extern __shared__ __align__(128) unsigned char smem[];
+    tuple_v *inbuf = reinterpret_cast<tuple_v *>(smem);                // [2][T]
+    long long *gbase = reinterpret_cast<long long *>(inbuf + 2 * T);     // [256]
+    long long *running = gbase + 256;                                   // [256]
+    uint32_t *tdstart = reinterpret_cast<uint32_t *>(running + 256);    // [256]
+    uint16_t *whist = reinterpret_cast<uint16_t *>(tdstart + 256);      // [NW][F]
+    __shared__ __align__(8) unsigned long long bars[2];
     __shared__ uint32_t scan_tmp[32];
-    __shared__ uint32_t s_tile;
+    __shared__ TileSlot slots[2];
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int F = a.F;
     const uint64_t dmask = (uint64_t)F - 1;
-    const uint32_t ntiles = a.counters[a.ctr_ntiles];
-    const int nsegs = (int)a.counters[a.ctr_nsegs];
+    const uint32_t nchunks = a.cg.cR + a.cg.cS;
+    const uint32_t nitems = a.pass == 0 ? nchunks : nchunks * (uint32_t)a.F1;
     unsigned int *err = &a.counters[kCtrErr];
-    for (int s = tid; s <= nsegs; s += THREADS) segft[s] = a.segs[s].first_tile;
     const unsigned ltmask = lanemask_lt();
+    const uint32_t bar0 = smem_addr(&bars[0]);
+    const int nbins = 1 << a.bits;
+    ItemIter it;  // used by thread 0 only
 
-    for (;;) {
-        if (tid == 0) s_tile = atomicAdd(&a.counters[a.ctr_tile], 1u);
-        __syncthreads();
-        const uint32_t tile = s_tile;
-        if (tile >= ntiles) break;
-        // Segment of this tile: largest s with segft[s] <= tile.
-        int lo = 0, hi = nsegs;  // invariant segft[lo] <= tile < segft[hi]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (segft[mid] <= tile) lo = mid; else hi = mid;
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const TileSlot s0 = next_tile<T>(a, it, nitems);
+        slots[0] = s0;
+        if (s0.item != ~0u) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
+    }
+    __syncthreads();
+
+    for (uint32_t k = 0;; k++) {
+        const uint32_t cur = k & 1u;
+        const TileSlot sl = slots[cur];
+        if (sl.item == ~0u) break;
+        tuple_v *buf = inbuf + (size_t)cur * T;
+        // Prefetch the next tile into the other buffer; its previous contents were consumed before
+        // the barrier that ended the previous iteration.
+        if (tid == 0) {
+            const TileSlot sn = next_tile<T>(a, it, nitems);
+            slots[cur ^ 1u] = sn;
+            if (sn.item != ~0u) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
         }
-        const int seg = lo;
-        const Seg sg = a.segs[seg];
-        const uint32_t ltile = tile - segft[seg];
-        const uint64_t begin = (uint64_t)ltile * T;
-        const uint32_t cnt = (uint32_t)(sg.count - begin < (uint64_t)T ? sg.count - begin : (uint64_t)T);
+        // First tile of a work item: load the item's per-digit output offsets.
+        if (sl.first && tid < F) {
+            long long off;
+            if (a.pass == 0) {
+                off = (long long)a.unit_off[(size_t)sl.item * a.F1 + tid];
+            } else {
+                const uint32_t c = sl.item / a.F1, d1 = sl.item % a.F1;
+                const int rel = c < a.cg.cR ? 0 : 1;
+                const uint32_t v = d1 | ((uint32_t)tid << a.b1);
+                off = (long long)(a.start[(size_t)rel * (nbins + 1) + (size_t)d1 * a.F2 + tid] +
+                                  a.prefix[(size_t)c * nbins + v]);
+            }
+            running[tid] = off;
+        }
+        const uint32_t cnt = sl.cnt;
+        const bool ok = mbar_wait(bar0 + 8u * cur, (k >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) set_error(err, kErrSpinLimit);
+            break;
+        }
 
-        // Load: warp w owns tuples [w*32*ITEMS, (w+1)*32*ITEMS) of the tile, one coalesced 512-byte
-        // row per item.
+        // Tuples of this tile: warp w owns [w*32*ITEMS, (w+1)*32*ITEMS), one 512-byte row per item.
         tuple_v v[ITEMS];
         uint32_t d[ITEMS];
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
             if (idx < cnt) {
-                v[i] = ld_stream(sg.in + begin + idx);
+                v[i] = buf[idx];
                 d[i] = (uint32_t)((v[i].x >> a.shift) & dmask);
             } else {
                 v[i] = make_ulonglong2(0, 0);
                 d[i] = (uint32_t)F;
             }
         }
-        uint32_t *wh = whist + w * F;
+        uint16_t *wh = whist + w * F;
         for (int j = lane; j < F; j += 32) wh[j] = 0;
         __syncwarp();
         // Stable rank within the warp: items in order, lanes in order.
@@ -425,7 +542,7 @@ __global__ void __launch_bounds__(THREADS, 4) scatter_kernel(ScatterArgs a) {
             if (valid) pre = wh[d[i]];
             rk[i] = pre + __popc(peers & ltmask);
             __syncwarp();
-            if (valid && (peers & ltmask) == 0) wh[d[i]] = pre + __popc(peers);
+            if (valid && (peers & ltmask) == 0) wh[d[i]] = (uint16_t)(pre + __popc(peers));
             __syncwarp();
         }
         __syncthreads();
@@ -434,60 +551,33 @@ __global__ void __launch_bounds__(THREADS, 4) scatter_kernel(ScatterArgs a) {
         if (tid < F) {
             for (int q = 0; q < NW; q++) {
                 const uint32_t c = whist[q * F + tid];
-                whist[q * F + tid] = h;
+                whist[q * F + tid] = (uint16_t)h;
                 h += c;
             }
         }
-        const bool first = ltile == 0;
-        uint32_t *my_status = a.status + (size_t)tile * F;
-        if (tid < F && (uint64_t)tile * F + F <= a.status_words)
-            st_relaxed_u32(&my_status[tid], (first ? kFlagPrefix : kFlagAgg) | h);
         const uint32_t ex = block_excl_scan_u32(tid < F ? h : 0u, scan_tmp, nullptr);
-        if (tid < F) tdstart[tid] = ex;
+        if (tid < F) {
+            tdstart[tid] = ex;
+            gbase[tid] = running[tid] - (long long)ex;
+            running[tid] += h;
+        }
         __syncthreads();
-        // Stage the tile sorted by digit (stable).
+        // Stage the tile sorted by digit (stable), in place.
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             if (d[i] < (uint32_t)F) {
                 const uint32_t pos = tdstart[d[i]] + wh[d[i]] + rk[i];
-                stage[pos] = v[i];
+                buf[pos] = v[i];
             }
-        }
-        // Look-back: exclusive prefix of this digit over the segment's earlier tiles.
-        if (tid < F) {
-            uint64_t excl = 0;
-            if (!first) {
-                int64_t t2 = (int64_t)tile - 1;
-                int spins = 0;
-                const int64_t tmin = (int64_t)segft[seg];
-                while (t2 >= tmin) {
-                    const uint32_t s = ld_relaxed_u32(&a.status[(size_t)t2 * F + tid]);
-                    const uint32_t flag = s & ~kValueMask;
-                    if (flag == 0) {
-                        if (++spins > kSpinLimit) {
-                            set_error(err, kErrSpinLimit);
-                            break;
-                        }
-                        __nanosleep(32);
-                        continue;
-                    }
-                    excl += s & kValueMask;
-                    if (flag == kFlagPrefix) break;
-                    t2--;
-                }
-                if ((uint64_t)tile * F + F <= a.status_words)
-                    st_relaxed_u32(&my_status[tid], kFlagPrefix | (uint32_t)((excl + h) & kValueMask));
-            }
-            gbase[tid] = (long long)a.obase[(size_t)seg * 256 + tid] + (long long)excl - (long long)ex;
         }
         __syncthreads();
         // Write each digit run: consecutive threads write consecutive 16-byte tuples.
         for (uint32_t j = tid; j < cnt; j += THREADS) {
-            const tuple_v t = stage[j];
+            const tuple_v t = buf[j];
             const uint32_t dd = (uint32_t)((t.x >> a.shift) & dmask);
             const long long dst = gbase[dd] + (long long)j;
-            if (dst >= 0 && (uint64_t)dst < sg.out_len)
-                st_stream(sg.out + dst, t);
+            if (dst >= 0 && (uint64_t)dst < sl.out_len)
+                st_stream(sl.out + dst, t);
             else
                 set_error(err, kErrBounds);
         }
@@ -495,12 +585,9 @@ __global__ void __launch_bounds__(THREADS, 4) scatter_kernel(ScatterArgs a) {
     }
 }
 
-// ------------------------------------------------------------------------------------------------
 // 4. Partition join in shared memory.
 // ------------------------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return smem_addr(p); }
 
 // 16-bit exchange on a shared-memory halfword through a 32-bit CAS on its word (lock-free: every
 // failed CAS means another thread's CAS succeeded).
@@ -527,26 +614,11 @@ struct JoinArgs {
     JoinAccum *acc;
 };
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    for (int it = 0; it < (1 << 24); it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
 constexpr int kHeadMax = 16384;  // next_pow_2(kSmemCap)
 constexpr size_t kJoinSmem = (size_t)kSmemCap * 16 + kHeadMax * 2 + (size_t)kSmemCap * 2;
 
 __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     tuple_v *rt = reinterpret_cast<tuple_v *>(smem);                      // [kSmemCap]
     uint16_t *head = reinterpret_cast<uint16_t *>(rt + kSmemCap);         // [kHeadMax]
     uint16_t *nxt = head + kHeadMax;                                       // [kSmemCap]
@@ -741,8 +813,8 @@ __global__ void copy_error(const uint32_t *counters, JoinAccum *acc) {
 int radix_geom(int bits, int passes, RadixGeom *g) {
     if (bits < 1 || bits > 15) return HJ_E_INVAL;
     if (passes != 1 && passes != 2) return HJ_E_INVAL;
-    // Partition results do not depend on how the bits are split across passes; a single pass is
-    // run as one physical pass only while its fanout fits the shared-memory staging (<= 256).
+    // Partition contents do not depend on how the bits are split across passes; a single pass runs
+    // as one physical pass only while its fanout fits the shared-memory staging (<= 256 digits).
     int P = passes;
     if (P == 1 && bits > 8) P = 2;
     if (P == 2 && bits < 2) P = 1;
@@ -758,23 +830,37 @@ int radix_geom(int bits, int passes, RadixGeom *g) {
 
 static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+static ChunkGeom chunk_geom(size_t nR, size_t nS, int num_sms) {
+    // About three chunks per SM (the scatter kernel's residency), each a whole number of tiles.
+    const uint64_t tiles = (uint64_t)ceil_div_u64(nR, kTile) + ceil_div_u64(nS, kTile);
+    const uint64_t target = (uint64_t)(num_sms > 0 ? num_sms : 148) * 3;
+    uint64_t ct = (tiles + target - 1) / target;
+    if (ct < 1) ct = 1;
+    ChunkGeom cg;
+    cg.chunk = ct * kTile;
+    cg.cR = ceil_div_u64(nR, cg.chunk);
+    cg.cS = ceil_div_u64(nS, cg.chunk);
+    return cg;
+}
+
 struct PhjSizes {
-    size_t hist, start, segs, obase, counters, status, items, large, large_table, tmp1, tmp2;
-    size_t max_items, max_large, status_words, large_table_words;
+    size_t chunk_hist, prefix, total, start, units_off, units_cnt, counters, items, large, large_table, tmp1, tmp2;
+    size_t max_items, max_large, large_table_words;
+    ChunkGeom cg;
 };
 
-static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS) {
+static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms) {
     PhjSizes z;
     const size_t np = (size_t)g.nparts();
-    z.hist = align_up(2 * np * 4, 256);
+    z.cg = chunk_geom(nR, nS, num_sms);
+    const size_t nchunks = (size_t)z.cg.cR + z.cg.cS;
+    z.chunk_hist = align_up(nchunks * np * 4, 256);
+    z.prefix = z.chunk_hist;
+    z.total = align_up(2 * np * 4, 256);
     z.start = align_up(2 * (np + 1) * 8, 256);
-    z.segs = align_up(2 * (kMaxPass2Segs + 1) * sizeof(Seg), 256);
-    z.obase = align_up((size_t)2 * kMaxPass2Segs * 256 * 8, 256);
+    z.units_off = align_up(nchunks * (size_t)g.F1 * 8, 256);
+    z.units_cnt = align_up(nchunks * (size_t)g.F1 * 4, 256);
     z.counters = 256;
-    const size_t max_tiles = (nR + nS) / kTile + 2 * (size_t)kMaxPass2Segs + 4;
-    const size_t maxF = (size_t)(g.F1 > g.F2 ? g.F1 : g.F2);
-    z.status_words = max_tiles * maxF;
-    z.status = align_up(z.status_words * 4, 256);
     z.max_items = np + nS / kProbeChunk + 2;
     z.items = align_up(z.max_items * sizeof(JoinItem), 256);
     z.max_large = np < nR / kSmemCap + 1 ? np : nR / kSmemCap + 1;
@@ -788,22 +874,25 @@ static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS) {
     return z;
 }
 
-size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS) {
-    PhjSizes z = phj_sizes(g, nR, nS);
-    return z.hist + z.start + z.segs + z.obase + z.counters + z.status + z.items + z.large +
-           z.large_table + z.tmp1 + z.tmp2;
+size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms) {
+    PhjSizes z = phj_sizes(g, nR, nS, num_sms);
+    return z.chunk_hist + z.prefix + z.total + z.start + z.units_off + z.units_cnt + z.counters + z.items +
+           z.large + z.large_table + z.tmp1 + z.tmp2;
 }
 
-void phj_carve(const RadixGeom &g, size_t nR, size_t nS, char *base, PhjScratch *s) {
-    PhjSizes z = phj_sizes(g, nR, nS);
+void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base, PhjScratch *s) {
+    PhjSizes z = phj_sizes(g, nR, nS, num_sms);
     char *p = base;
-    s->hist = reinterpret_cast<uint32_t *>(p); p += z.hist;
+    s->chunk = z.cg.chunk;
+    s->cR = z.cg.cR;
+    s->cS = z.cg.cS;
+    s->chunk_hist = reinterpret_cast<uint32_t *>(p); p += z.chunk_hist;
+    s->prefix = reinterpret_cast<uint32_t *>(p); p += z.prefix;
+    s->total = reinterpret_cast<uint32_t *>(p); p += z.total;
     s->start = reinterpret_cast<uint64_t *>(p); p += z.start;
-    s->segs = p; p += z.segs;
-    s->obase = reinterpret_cast<uint64_t *>(p); p += z.obase;
+    s->unit_off = reinterpret_cast<uint64_t *>(p); p += z.units_off;
+    s->unit_cnt = reinterpret_cast<uint32_t *>(p); p += z.units_cnt;
     s->counters = reinterpret_cast<uint32_t *>(p); p += z.counters;
-    s->status = reinterpret_cast<uint32_t *>(p); p += z.status;
-    s->status_words = z.status_words;
     s->items = p; p += z.items;
     s->max_items = z.max_items;
     s->large = p; p += z.large;
@@ -820,101 +909,114 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, char *base, PhjScratch 
     }
 }
 
-#define HJ_CU(call)                                  \
-    do {                                             \
-        cudaError_t e_ = (call);                     \
-        if (e_ != cudaSuccess) {                     \
+#define HJ_CU(call)                                                                   \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
             fprintf(stderr, "hjscm: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
-            return HJ_E_DEVICE;                      \
-        }                                            \
+            return HJ_E_DEVICE;                                                       \
+        }                                                                             \
     } while (0)
 
 static bool g_attr_done[64] = {};
 
 int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                int num_sms) {
-    if (nR >= (1ull << 30) || nS >= (1ull << 30)) return HJ_E_INVAL;
+                int num_sms, cudaEvent_t *ph, uint32_t *launches) {
+    uint32_t nlaunch = 0;
+#define HJ_PH(i) \
+    if (ph) HJ_CU(cudaEventRecord(ph[i], st))
+    if (nR >= (1ull << 32) || nS >= (1ull << 32)) return HJ_E_INVAL;
     const int np = g.nparts();
     const int F1 = g.F1, F2 = g.F2;
-    const int maxF = F1 > F2 ? F1 : F2;
     constexpr int T = kTile;
-    const size_t scatter_smem = (size_t)T * 16 + 256 * 8 + (kScatterThreads / 32) * 256 * 4 + 256 * 4 +
-                                (kMaxPass2Segs + 1) * 4;
+    const size_t scatter_smem = (size_t)2 * T * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
     const size_t hist_smem = (size_t)np * 4;
+    ChunkGeom cg;
+    cg.chunk = s.chunk;
+    cg.cR = s.cR;
+    cg.cS = s.cS;
+    const uint32_t nchunks = cg.cR + cg.cS;
     int cur_dev = 0;
     HJ_CU(cudaGetDevice(&cur_dev));
     if (cur_dev < 0 || cur_dev >= 64) return HJ_E_INVAL;
     if (!g_attr_done[cur_dev]) {
-        HJ_CU(cudaFuncSetAttribute(hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
+        HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
         HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
         HJ_CU(cudaFuncSetAttribute(join_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)kJoinSmem));
         g_attr_done[cur_dev] = true;
     }
-    (void)maxF;
-    HJ_CU(cudaMemsetAsync(s.hist, 0, (size_t)2 * np * 4, st));
     HJ_CU(cudaMemsetAsync(s.counters, 0, kNumCounters * 4, st));
 
-    // 1. histogram
-    {
-        const int hist_blocks = num_sms * (hist_smem > 64 * 1024 ? 1 : 2);
-        int gR = (int)((double)hist_blocks * (double)nR / (double)(nR + nS + 1));
-        if (nR && gR < 1) gR = 1;
-        if (nS && gR > hist_blocks - 1) gR = hist_blocks - 1;
-        hist_kernel<<<hist_blocks, 1024, hist_smem, st>>>(R, nR, S, nS, g.bits, s.hist, gR);
-        HJ_CU(cudaGetLastError());
-    }
-    // 2. plan
+    // 1. per-chunk histograms
+    HJ_PH(0);
+    hist_chunk_kernel<<<nchunks, 512, hist_smem, st>>>(R, nR, S, nS, g.bits, cg, s.chunk_hist);
+    HJ_CU(cudaGetLastError());
+    HJ_PH(1);
+    // 2. prefix over chunks, 3. plan, 4. units
+    colscan_kernel<<<(2 * np + 255) / 256, 256, 0, st>>>(s.chunk_hist, s.prefix, s.total, np, cg);
     PlanArgs pa;
     pa.bits = g.bits;
     pa.passes = g.passes;
     pa.b1 = g.b1;
     pa.F1 = F1;
     pa.F2 = F2;
-    pa.R = R;
-    pa.S = S;
     pa.nR = nR;
     pa.nS = nS;
-    pa.hist = s.hist;
+    pa.total = s.total;
     pa.start = s.start;
-    pa.segs = reinterpret_cast<Seg *>(s.segs);
-    pa.obase = s.obase;
     pa.counters = s.counters;
-    pa.tmp1 = s.tmp1;
-    pa.tmp2 = s.tmp2;
     pa.items = reinterpret_cast<JoinItem *>(s.items);
     pa.max_items = s.max_items;
     pa.large = reinterpret_cast<LargePart *>(s.large);
     pa.max_large = s.max_large;
     pa.large_table_words = s.large_table_words;
     plan_kernel<<<1, 1024, 0, st>>>(pa);
+    {
+        const uint32_t warps = nchunks * (uint32_t)F1;
+        units_kernel<<<(warps * 32 + 255) / 256, 256, 0, st>>>(s.chunk_hist, s.prefix, s.start, g.bits, g.b1, F1,
+                                                               g.passes == 2 ? F2 : 1, cg, s.unit_off, s.unit_cnt);
+    }
     HJ_CU(cudaGetLastError());
+    nlaunch += 4;
+    HJ_PH(2);
 
-    // 3. scatter passes
-    const int scatter_grid = num_sms * 4;
+    // 5. scatter passes
+    const int scatter_grid = num_sms * 3;
     for (int pass = 0; pass < g.passes; pass++) {
-        const int F = pass == 0 ? F1 : F2;
-        const size_t words = s.status_words;
-        HJ_CU(cudaMemsetAsync(s.status, 0, words * 4, st));
         ScatterArgs sa;
-        sa.segs = reinterpret_cast<const Seg *>(s.segs) + (size_t)pass * (kMaxPass2Segs + 1);
-        sa.obase = s.obase + (size_t)pass * kMaxPass2Segs * 256;
-        sa.counters = s.counters;
-        sa.ctr_tile = pass == 0 ? kCtrTile1 : kCtrTile2;
-        sa.ctr_ntiles = pass == 0 ? kCtrNTiles1 : kCtrNTiles2;
-        sa.ctr_nsegs = pass == 0 ? kCtrNSegs1 : kCtrNSegs2;
-        sa.F = F;
+        sa.pass = pass;
+        sa.F = pass == 0 ? F1 : F2;
         sa.shift = pass == 0 ? 0 : g.b1;
-        sa.status = s.status;
-        sa.status_words = words;
+        sa.bits = g.bits;
+        sa.b1 = g.b1;
+        sa.F1 = F1;
+        sa.F2 = g.passes == 2 ? F2 : 1;
+        sa.cg = cg;
+        sa.inR = pass == 0 ? R : s.tmp1;
+        sa.inS = pass == 0 ? S : s.tmp1 + nR;
+        tuple_v *out = pass == 0 ? s.tmp1 : s.tmp2;
+        sa.outR = out;
+        sa.outS = out + nR;
+        sa.nR = nR;
+        sa.nS = nS;
+        sa.prefix = s.prefix;
+        sa.start = s.start;
+        sa.unit_off = s.unit_off;
+        sa.unit_cnt = s.unit_cnt;
+        sa.counters = s.counters;
+        sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
         scatter_kernel<kScatterThreads, kScatterItems><<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
         HJ_CU(cudaGetLastError());
+        nlaunch++;
+        HJ_PH(3 + pass);
     }
+    if (ph && g.passes == 1) HJ_CU(cudaEventRecord(ph[4], st));
     if (ev_mid) HJ_CU(cudaEventRecord(ev_mid, st));
 
-    // 4. joins
+    // 6. joins
     JoinArgs ja;
     ja.items = reinterpret_cast<const JoinItem *>(s.items);
     ja.large = reinterpret_cast<const LargePart *>(s.large);
@@ -927,11 +1029,16 @@ int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, con
     ja.acc = acc;
     join_small_kernel<<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
     HJ_CU(cudaGetLastError());
+    HJ_PH(5);
     join_large_clear<<<num_sms * 2, 256, 0, st>>>(ja);
     join_large_build<<<num_sms * 2, 256, 0, st>>>(ja);
     join_large_probe<<<num_sms * 2, 256, 0, st>>>(ja);
     copy_error<<<1, 32, 0, st>>>(s.counters, acc);
     HJ_CU(cudaGetLastError());
+    HJ_PH(6);
+    nlaunch += 5;
+    if (launches) *launches = nlaunch;
+#undef HJ_PH
     return HJ_OK;
 }
 

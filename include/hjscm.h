@@ -80,6 +80,13 @@ typedef struct {
 
 #define HJ_F_NO_TIMING   0x1u /* skip the per-phase CUDA events (buildpart/probejoin stay 0) */
 #define HJ_F_PINNED_HOST 0x2u /* host inputs are already page-locked */
+#define HJ_F_PHASE_TIMES 0x4u /* also time each kernel group (fills hj_result_t.phase) */
+
+/* hj_result_t.phase[] slots (seconds), filled with HJ_F_PHASE_TIMES. PHJ: histogram, plan, partition
+ * pass 1, partition pass 2, shared-memory partition joins, global-memory (large) partition joins.
+ * NPHJ: build, -, -, -, probe, -. */
+enum { HJ_PH_HIST = 0, HJ_PH_PLAN = 1, HJ_PH_PASS1 = 2, HJ_PH_PASS2 = 3, HJ_PH_JOIN = 4, HJ_PH_LARGE = 5,
+       HJ_PH_COUNT = 6 };
 
 /* Result of one join. matched_cnt/checksum are the reference's two printed values
  * (`matched_cnt: %zu\tcheck_sum: %zu`, src/algo/phj.c:2206); the times follow its timekeeper_t
@@ -95,6 +102,9 @@ typedef struct {
     int status;
     int physical_passes; /* partition passes the device ran (PHJ only) */
     uint64_t large_partitions; /* partitions joined through the global-memory path (PHJ only) */
+    double phase[HJ_PH_COUNT]; /* per-kernel-group seconds (HJ_F_PHASE_TIMES) */
+    uint32_t kernel_launches;  /* kernels this join launched */
+    uint32_t pad;
 } hj_result_t;
 
 typedef struct hj_ctx hj_ctx_t;
