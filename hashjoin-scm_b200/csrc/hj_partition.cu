@@ -358,6 +358,7 @@ __global__ void units_kernel(const uint32_t *__restrict__ chunk_hist, const uint
 struct ScatterArgs {
     int pass;        // 0: by the pass-1 digit, per chunk; 1: by the pass-2 digit, per (chunk, d1) unit
     int F, shift;    // digit of this pass: (key >> shift) & (F - 1)
+    int logF;        // log2(F)
     int bits, b1, F1, F2;
     ChunkGeom cg;
     const tuple_v *inR, *inS;   // pass input (pass 0: the relations; pass 1: the pass-1 output)
@@ -532,11 +533,22 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
         uint16_t *wh = whist + w * F;
         for (int j = lane; j < F; j += 32) wh[j] = 0;
         __syncwarp();
-        // Stable rank within the warp: items in order, lanes in order.
+        // Stable rank within the warp: items in order, lanes in order. The lanes holding the same
+        // digit are found with one ballot per digit bit (plus the bit that marks padding lanes of a
+        // partial tile), which is cheaper here than match.any.
+        const int nbits = a.logF + (cnt < (uint32_t)T ? 1 : 0);
         uint32_t rk[ITEMS];
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
-            const unsigned peers = __match_any_sync(0xffffffffu, d[i]);
+            unsigned peers = 0xffffffffu;
+#pragma unroll
+            for (int b = 0; b < 9; b++) {
+                if (b < nbits) {
+                    const unsigned bit = (d[i] >> b) & 1u;
+                    const unsigned bal = __ballot_sync(0xffffffffu, bit);
+                    peers &= bit ? bal : ~bal;
+                }
+            }
             const bool valid = d[i] < (uint32_t)F;
             uint32_t pre = 0;
             if (valid) pre = wh[d[i]];
@@ -571,7 +583,24 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
             }
         }
         __syncthreads();
-        // Write each digit run: consecutive threads write consecutive 16-byte tuples.
+        // Write each digit run: consecutive threads write consecutive 16-byte tuples. Full tiles load
+        // all their staged tuples first so that the stores issue back to back.
+        if (cnt == (uint32_t)T) {
+            tuple_v t[ITEMS];
+            long long dst[ITEMS];
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) t[i] = buf[tid + i * THREADS];
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++)
+                dst[i] = gbase[(uint32_t)((t[i].x >> a.shift) & dmask)] + (long long)(tid + i * THREADS);
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len)
+                    st_stream(sl.out + dst[i], t[i]);
+                else
+                    set_error(err, kErrBounds);
+            }
+        } else
         for (uint32_t j = tid; j < cnt; j += THREADS) {
             const tuple_v t = buf[j];
             const uint32_t dd = (uint32_t)((t.x >> a.shift) & dmask);
@@ -989,6 +1018,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, con
         ScatterArgs sa;
         sa.pass = pass;
         sa.F = pass == 0 ? F1 : F2;
+        sa.logF = pass == 0 ? g.b1 : g.b2;
         sa.shift = pass == 0 ? 0 : g.b1;
         sa.bits = g.bits;
         sa.b1 = g.b1;
