@@ -176,6 +176,37 @@ int hj_gen_zipf_device(size_t nS, size_t nR, double zipf_factor, uint64_t seed,
  * nS a multiple of nR: matched = nS, checksum = m*n*(n+1) mod 2^64 with m = nS/nR. */
 void hj_pkfk_closed_form(size_t nR, size_t nS, uint64_t *matched, uint64_t *checksum);
 
+/* ----------------------------------------------------------------------------------------------
+ * Allocation-free join. This entry point has no counterpart in the reference, whose joins allocate
+ * their tables per call (src/algo/nphj.c:745-757).
+ *
+ * Some callers cannot allocate device memory: a host engine that has already reserved the GPU's memory
+ * for its own buffer pool, or a request loop that must not call the CUDA allocator (cudaMalloc and
+ * cudaFree synchronise the device and have unbounded latency). hj_nphj_join_noalloc runs nphj_sc or
+ * nphj_lp on device-resident relations with its hash table in a fixed 16 MiB array that is part of the
+ * library image (every GPU that loads the library holds it until the process exits); it calls no
+ * allocator. Limits and rules:
+ *   - nR (build side) <= 524286 tuples; larger builds return HJ_E_INVAL with a message on stderr.
+ *   - R_dev, S_dev: device pointers; out_dev: a caller-owned device hj_device_result_t, zeroed and then
+ *     filled on `stream` (cudaStream_t, NULL = legacy default stream); the call only enqueues work.
+ *   - The first call on a device looks up the array's device address (once per device, with that device
+ *     current); make that first call before any stream capture.
+ *   - All calls share the one array and each clears it on its stream; calls whose GPU work overlaps
+ *     (different streams or host threads) race and must be serialised by the caller.
+ *   - After the stream completes, out_dev->error_bits != 0 means the result is invalid (1: a probe
+ *     walked the whole table, 4: an index fell outside its buffer).
+ * -------------------------------------------------------------------------------------------- */
+typedef struct {
+    uint64_t matched_cnt;
+    uint64_t checksum;
+    uint32_t error_bits;
+    uint32_t reserved0;
+    uint64_t reserved[5];
+} hj_device_result_t;
+
+int hj_nphj_join_noalloc(hj_algo_t algo, const hj_tuple_t *R_dev, size_t nR, const hj_tuple_t *S_dev,
+                         size_t nS, hj_device_result_t *out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
