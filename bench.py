@@ -50,6 +50,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["join", "batch"], default="join",
+                    help="join: the headline 2^27 x 2^29 join; batch: 512 independent joins (config 4)")
+    ap.add_argument("--batch-jobs", type=int, default=512)
+    ap.add_argument("--calibrate", action="store_true", help="batch mode: calibrate the autotuner first")
     ap.add_argument("--algo", default="phj_radix_bc")
     ap.add_argument("--nr-log", type=int, default=27)
     ap.add_argument("--ns-log", type=int, default=29)
@@ -360,6 +364,109 @@ def run_ours(a, rank, world, local_rank):
     return 0
 
 
+def batch_workload(hj, torch, dev, njobs, seed=12345):
+    """512 PK-FK joins: |R| log-uniform in [2^10, 2^22] (rounded up to a multiple of 256), |S| = k|R| with
+    k uniform in 1..16, keys a seeded permutation per join (seed 12345 + i), uniform FKs."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    sizes = []
+    for i in range(njobs):
+        nR = int(2 ** rng.uniform(10, 22))
+        nR = (nR + 255) // 256 * 256
+        k = int(rng.integers(1, 17))
+        sizes.append((nR, k * nR, k))
+    total = sum(r + s for r, s, _ in sizes)
+    buf = torch.empty((total, 2), dtype=torch.int64, device=dev)
+    jobs, want, off = [], [], 0
+    for i, (nR, nS, k) in enumerate(sizes):
+        R = buf[off:off + nR]
+        S = buf[off + nR:off + nR + nS]
+        off += nR + nS
+        hj.gen_fast_device(nR, nS, R.data_ptr(), S.data_ptr(), seed=seed + i)
+        jobs.append(("phj_radix_bc", R, S))
+        want.append(hj.pkfk_closed_form(nR, nS))
+    torch.cuda.synchronize(dev)
+    return jobs, want, total, buf
+
+
+def run_batch_mode(a, rank, world, local_rank):
+    import torch
+
+    hj = load_module("hashjoin_scm_b200", PKG_DIR / "__init__.py")
+    hj.lib()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    jobs, want, total, buf = batch_workload(hj, torch, dev, a.batch_jobs, seed=12345 + 1000 * rank)
+    ctx = hj.Context(local_rank)
+    calib = hj.tuner_calibrate(ctx) if a.calibrate else None
+    tuner = hj.tuner_get(ctx)
+
+    def check(results):
+        for r, w in zip(results, want):
+            if (r.matched_cnt, r.checksum) != w:
+                raise RuntimeError("batched join result differs from the closed form")
+
+    # 1. plain per-join loop: every join through hj_join with the default algorithm and radix settings
+    def loop(decided):
+        out = []
+        for algo, R, S in jobs:
+            kw = {}
+            if decided:
+                import ctypes
+                impl, bits, passes = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+                hj._bind_batch().hj_tuner_decide(ctx.handle, R.shape[0], S.shape[0], ctypes.byref(impl),
+                                                 ctypes.byref(bits), ctypes.byref(passes))
+                if impl.value == 0:
+                    algo = "nphj_sc"
+                else:
+                    kw = {"bits": bits.value, "passes": passes.value}
+            out.append(hj.join(algo, R, S, on_device=True, device=local_rank, ctx=ctx, flags=hj.HJ_F_NO_TIMING, **kw))
+        return out
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(reps):
+            res = fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / 1e3 / reps, res
+
+    check(loop(False))
+    t_loop, res = timed(lambda: loop(False), max(1, a.steps // 5))
+    check(res)
+    check(loop(True))
+    t_loop_tuned, res = timed(lambda: loop(True), max(1, a.steps // 5))
+    check(res)
+    with hj.Batch(ctx, jobs) as b:
+        for _ in range(a.warmup):
+            res, st = b.run()
+            check(res)
+        t_batch, (res, st) = timed(b.run, a.steps)
+        check(res)
+    n = len(jobs)
+    if rank == 0:
+        line = {
+            "metric": "batched joins/s", "value": world * n / t_batch, "unit": "joins/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": f"{n} PK-FK joins, |R| log-uniform in [2^10, 2^22] (multiple of 256), "
+                                   "|S| = k|R|, k uniform in 1..16, 16-B tuples", "tuples": total},
+            "per_join_loop": {"joins_per_s": n / t_loop, "ms": t_loop * 1e3, "algo": "phj_radix_bc, 14 bits, 2 passes"},
+            "per_join_loop_tuned": {"joins_per_s": n / t_loop_tuned, "ms": t_loop_tuned * 1e3},
+            "speedup_vs_loop": t_loop / t_batch, "speedup_vs_tuned_loop": t_loop_tuned / t_batch,
+            "tuples_per_s": total / t_batch, "batch_stats": {"nphj_jobs": st.nphj_jobs, "phj_jobs": st.phj_jobs,
+                                                             "waves": st.waves, "kernels": st.kernel_launches},
+            "tuner": {"nphj_max_table_bytes": tuner.nphj_max_table_bytes, "calibrated": tuner.calibrated,
+                      "calibration": calib},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     a = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -377,6 +484,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     try:
+        if a.mode == "batch":
+            return run_batch_mode(a, rank, world, local_rank)
         return run_ours(a, rank, world, local_rank)
     finally:
         if world > 1:

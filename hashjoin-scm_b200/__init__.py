@@ -305,3 +305,115 @@ def header_functions() -> list[str]:
             if name not in ("if", "while", "for", "return", "sizeof"):
                 names.append(name)
     return sorted(set(names))
+
+
+# ---------------------------------------------------------------------------------------------
+# Batched joins and the autotuner (include/hjscm.h, "Batched joins")
+# ---------------------------------------------------------------------------------------------
+HJ_F_NO_GRAPH = 0x8
+IMPL_NAMES = {0: "nphj", 1: "phj"}
+
+
+class Tuner(ctypes.Structure):
+    _fields_ = [("nphj_max_table_bytes", ctypes.c_double), ("wave_table_bytes", ctypes.c_double),
+                ("partition_target", ctypes.c_int), ("calibrated", ctypes.c_int)]
+
+
+class BatchJob(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_int), ("R", ctypes.c_void_p), ("nR", ctypes.c_size_t), ("S", ctypes.c_void_p),
+                ("nS", ctypes.c_size_t)]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [("matched_cnt", ctypes.c_uint64), ("checksum", ctypes.c_uint64), ("status", ctypes.c_int),
+                ("impl", ctypes.c_int), ("num_radix_bits", ctypes.c_int), ("num_passes", ctypes.c_int)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("kernel_launches", ctypes.c_uint32), ("waves", ctypes.c_int),
+                ("nphj_jobs", ctypes.c_int), ("phj_jobs", ctypes.c_int)]
+
+
+def _bind_batch():
+    L = lib()
+    if getattr(L, "_batch_bound", False):
+        return L
+    vp, i32, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    L.hj_tuner_get.argtypes = [vp, ctypes.POINTER(Tuner)]
+    L.hj_tuner_set.argtypes = [vp, ctypes.POINTER(Tuner)]
+    L.hj_tuner_decide.argtypes = [vp, sz, sz, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]
+    L.hj_tuner_calibrate.argtypes = [vp, ctypes.POINTER(ctypes.c_double), i32]
+    L.hj_batch_plan.argtypes = [vp, ctypes.POINTER(BatchJob), i32, ctypes.POINTER(Params), ctypes.POINTER(vp)]
+    L.hj_batch_run.argtypes = [vp, ctypes.POINTER(BatchResult), ctypes.POINTER(BatchStats)]
+    L.hj_batch_destroy.argtypes = [vp]
+    for f in ("hj_tuner_get", "hj_tuner_set", "hj_tuner_decide", "hj_tuner_calibrate", "hj_batch_plan",
+              "hj_batch_run", "hj_batch_destroy"):
+        getattr(L, f).restype = i32
+    L._batch_bound = True
+    return L
+
+
+def tuner_get(ctx: "Context") -> Tuner:
+    t = Tuner()
+    _bind_batch().hj_tuner_get(ctx.handle, ctypes.byref(t))
+    return t
+
+
+def tuner_set(ctx: "Context", **kw) -> Tuner:
+    t = tuner_get(ctx)
+    for k, v in kw.items():
+        setattr(t, k, v)
+    rc = _bind_batch().hj_tuner_set(ctx.handle, ctypes.byref(t))
+    if rc:
+        raise JoinError(rc, "hj_tuner_set")
+    return t
+
+
+def tuner_calibrate(ctx: "Context"):
+    """Time both implementations on the device and set the crossover; returns [(|R|, t_nphj, t_phj)]."""
+    rep = (ctypes.c_double * 24)()
+    rc = _bind_batch().hj_tuner_calibrate(ctx.handle, rep, 24)
+    if rc:
+        raise JoinError(rc, "hj_tuner_calibrate")
+    return [(int(rep[3 * i]), rep[3 * i + 1], rep[3 * i + 2]) for i in range(8) if rep[3 * i] > 0]
+
+
+class Batch:
+    """A planned batch of joins on device-resident relations (hj_batch_plan); run() launches it once.
+
+    jobs: list of (algo name, R, S) where R and S are CUDA tensors of shape (n, 2) or (pointer, n)."""
+
+    def __init__(self, ctx: "Context", jobs, graph: bool = True):
+        L = _bind_batch()
+        arr = (BatchJob * max(len(jobs), 1))()
+        self._keep = []
+        for i, (algo, R, S) in enumerate(jobs):
+            pr, nr = _ptr_len(R, True)
+            ps, ns = _ptr_len(S, True)
+            arr[i].algo, arr[i].R, arr[i].nR, arr[i].S, arr[i].nS = ALGOS[algo], pr, nr, ps, ns
+            self._keep.append((R, S))
+        p = make_params(device=ctx.device, on_device=True, flags=0 if graph else HJ_F_NO_GRAPH)
+        h = ctypes.c_void_p()
+        rc = L.hj_batch_plan(ctx.handle, arr, len(jobs), ctypes.byref(p), ctypes.byref(h))
+        if rc:
+            raise JoinError(rc, "hj_batch_plan")
+        self.handle, self.n = h, len(jobs)
+
+    def run(self):
+        res = (BatchResult * max(self.n, 1))()
+        st = BatchStats()
+        rc = _bind_batch().hj_batch_run(self.handle, res, ctypes.byref(st))
+        if rc:
+            raise JoinError(rc, "hj_batch_run")
+        return list(res)[: self.n], st
+
+    def close(self):
+        if self.handle:
+            _bind_batch().hj_batch_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -10,21 +10,10 @@
 #include <mutex>
 
 #include "hj_common.cuh"
+#include "hj_ctx.h"
 #include "hj_internal.h"
 
 using hj::JoinAccum;
-
-struct hj_ctx {
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev_h2d = nullptr, ev_start = nullptr, ev_mid = nullptr, ev_end = nullptr;
-    cudaEvent_t ev_ph[HJ_PH_COUNT + 1] = {};
-    char *arena = nullptr;
-    size_t arena_bytes = 0;
-    JoinAccum *acc_host = nullptr;  // pinned
-    std::mutex mu;
-};
 
 #define CU_OR(call, code)                                                                   \
     do {                                                                                    \
@@ -177,6 +166,10 @@ int hj_ctx_create(int device, hj_ctx_t **out) {
     CU_OR(cudaEventCreate(&c->ev_end), HJ_E_DEVICE);
     for (int i = 0; i <= HJ_PH_COUNT; i++) CU_OR(cudaEventCreate(&c->ev_ph[i]), HJ_E_DEVICE);
     CU_OR(cudaMallocHost(&c->acc_host, sizeof(JoinAccum)), HJ_E_OOM);
+    c->tuner.nphj_max_table_bytes = 64e6;
+    c->tuner.wave_table_bytes = 64e6;
+    c->tuner.partition_target = 6144;
+    c->tuner.calibrated = 0;
     *out = c;
     return HJ_OK;
 }
@@ -265,11 +258,11 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     if (is_phj(algo)) {
         hj::PhjScratch s;
         hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s);
-        rc = hj::phj_enqueue(geom, algo == HJ_ALGO_PHJ_RADIX_LP, dR, nR, dS, nS, s, acc, st,
+        rc = hj::phj_enqueue(geom, algo == HJ_ALGO_PHJ_RADIX_LP, algo == HJ_ALGO_PHJ_RADIX_LP, dR, nR, dS, nS, s, acc, st,
                              timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
     } else {
         const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
-        rc = hj::nphj_enqueue(algo == HJ_ALGO_NPHJ_LP, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
+        rc = hj::nphj_enqueue(algo == HJ_ALGO_NPHJ_LP, false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
                               timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
     }
     if (rc) {

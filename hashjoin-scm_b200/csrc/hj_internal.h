@@ -52,20 +52,26 @@ struct PhjScratch {
     ulonglong2 *tmp2;        // pass-2 output [nR + nS] (== tmp1 for one pass)
 };
 
+// Kernel attributes (dynamic shared memory limits) for the current device; phj_enqueue calls it too,
+// but callers that capture a stream into a graph call it before the capture.
+int phj_prepare_device();
+
 size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms);
 void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base, PhjScratch *s);
 
+// Result semantics: lp = first match per probe tuple (lowest build position) instead of all matches;
+// skip0 = build tuples with key 0 never match (the phj_radix_lp empty-slot rule, src/algo/phj.c:614).
 // Enqueue a full partitioned join on `st`; matches/checksum accumulate into acc (zeroed by caller).
 // ev_mid, if non-null, is recorded between the partition phase and the join phase.
 // ph, if non-null, holds HJ_PH_COUNT + 1 events recorded at the phase boundaries; *launches receives
 // the number of kernels enqueued.
-int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
+int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                 int num_sms, cudaEvent_t *ph, uint32_t *launches);
 
 // Non-partitioned joins on a global open-addressing table.
 size_t nphj_scratch_bytes(size_t nR, double load);
-int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
+int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                  int num_sms, cudaEvent_t *ph, uint32_t *launches);
 

@@ -80,7 +80,7 @@ extern "C" int hj_nphj_join_noalloc(hj_algo_t algo, const hj_tuple_t *R_dev, siz
     // The result starts at zero; the table and the side record are cleared by the join itself.
     if (cudaMemsetAsync(out_dev, 0, sizeof(hj_device_result_t), st) != cudaSuccess) return HJ_E_DEVICE;
     if (nR == 0 || nS == 0) return HJ_OK;
-    return hj::nphj_enqueue(algo == HJ_ALGO_NPHJ_LP, reinterpret_cast<const ulonglong2 *>(R_dev), nR,
+    return hj::nphj_enqueue(algo == HJ_ALGO_NPHJ_LP, false, reinterpret_cast<const ulonglong2 *>(R_dev), nR,
                             reinterpret_cast<const ulonglong2 *>(S_dev), nS, scratch, kNoallocBytes, kNoallocLoad,
                             reinterpret_cast<hj::JoinAccum *>(out_dev), st, nullptr, sms, nullptr, nullptr);
 }

@@ -40,7 +40,8 @@ struct NphjArgs {
     unsigned long long cap;
     NphjSide *side;
     JoinAccum *acc;
-    int lp;
+    int lp;     // first match per probe tuple instead of all matches
+    int skip0;  // key 0 never matches (the phj_radix_lp rule)
 };
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
@@ -53,6 +54,7 @@ __global__ void nphj_build(NphjArgs a) {
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.nR;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const tuple_v t = ld_stream(a.R + i);
+        if (a.skip0 && t.x == 0) continue;
         if (t.x == kEmpty) {
             if (atomicAdd(&a.side->cnt, 1ull) >= 1ull) seen_dup = true;
             atomicAdd(&a.side->sum, (unsigned long long)t.y);
@@ -95,7 +97,7 @@ __global__ void nphj_lp_dedup_build(NphjArgs a) {
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.nR;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const unsigned long long k = a.R[i].x;
-        if (k == kEmpty) continue;
+        if (k == kEmpty || (a.skip0 && k == 0)) continue;
         unsigned long long h = table_hash(k, a.cap);
         unsigned long long steps = 0;
         for (;;) {
@@ -145,6 +147,7 @@ __global__ void nphj_probe(NphjArgs a) {
         for (int u = 0; u < 2; u++) {
             if (u == 1 && j0 + stride >= a.nS) break;
             const tuple_v s = sv[u];
+            if (a.skip0 && s.x == 0) continue;
             if (s.x == kEmpty) {
                 if (side_cnt) {
                     if (a.lp) {
@@ -198,7 +201,7 @@ size_t nphj_scratch_bytes(size_t nR, double load) {
         }                                                                             \
     } while (0)
 
-int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
+int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                  int num_sms, cudaEvent_t *ph, uint32_t *launches) {
     const unsigned long long cap = nphj_cap(nR, load);
@@ -213,6 +216,7 @@ int nphj_enqueue(bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S, s
     a.side = reinterpret_cast<NphjSide *>(reinterpret_cast<char *>(table) + cap * 16);
     a.acc = acc;
     a.lp = lp ? 1 : 0;
+    a.skip0 = skip0 ? 1 : 0;
     HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
     HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
     HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));

@@ -60,6 +60,8 @@ struct LargePart {
 enum : int {
     kCtrItem1 = 0,       // scatter pass-1 work-item counter
     kCtrItem2 = 1,       // scatter pass-2 work-item counter
+    kCtrNItemsA = 2,     // join items whose build side fits the compact shared-memory table (listed first)
+    kCtrItemA = 3,       // compact join work-item counter
     kCtrNItems = 6,
     kCtrNLarge = 7,
     kCtrItem = 8,        // join work-item counter
@@ -67,8 +69,15 @@ enum : int {
     kCtrLargeS = 11,     // total S tuples in large partitions (lo, hi)
     kCtrLargeWords = 13, // table words used (lo, hi)
     kCtrErr = 15,
-    kNumCounters = 16
+    kCtrMaxKey = 16,     // u64: OR of all R keys (words 16-17)
+    kCtrMaxRid = 18,     // u64: OR of all R row ids (words 18-19)
+    kNumCounters = 20
 };
+
+// Build partitions up to this size whose keys (above the radix bits) and row ids fit 32 bits are
+// joined with a 4-byte-per-field shared-memory table, two CTAs per SM.
+constexpr int kCompactCap = 8192;
+constexpr int kCompactThreads = 512;
 
 // Chunking of the two relations (identical for the histogram and both scatter passes).
 struct ChunkGeom {
@@ -137,7 +146,8 @@ __device__ __forceinline__ void tma_load_1d(void *dst_smem, const void *src, uin
 // ------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) hist_chunk_kernel(const tuple_v *__restrict__ R, size_t nR,
                                                          const tuple_v *__restrict__ S, size_t nS, int bits,
-                                                         ChunkGeom cg, uint32_t *__restrict__ chunk_hist) {
+                                                         ChunkGeom cg, uint32_t *__restrict__ chunk_hist,
+                                                         uint32_t *__restrict__ maxima) {
     extern __shared__ uint32_t sh_hist[];
     const int nbins = 1 << bits;
     const uint64_t mask = (uint64_t)nbins - 1;
@@ -152,49 +162,106 @@ __global__ void __launch_bounds__(512) hist_chunk_kernel(const tuple_v *__restri
     const uint64_t hi = lo + cg.chunk < n ? lo + cg.chunk : n;
     const uint64_t step = blockDim.x;
     uint64_t i = lo + threadIdx.x;
-    for (; i + 3 * step < hi; i += 4 * step) {
-        const tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + step);
-        const tuple_v t2 = ld_stream(in + i + 2 * step), t3 = ld_stream(in + i + 3 * step);
-        atomicAdd(&sh_hist[t0.x & mask], 1u);
-        atomicAdd(&sh_hist[t1.x & mask], 1u);
-        atomicAdd(&sh_hist[t2.x & mask], 1u);
-        atomicAdd(&sh_hist[t3.x & mask], 1u);
+    if (rel == 0) {
+        // Build side: also OR together all keys and row ids; their widths decide whether the compact
+        // join table applies (a value fits 32 bits iff the OR of all values does).
+        unsigned long long kor = 0, ror = 0;
+        for (; i + 3 * step < hi; i += 4 * step) {
+            const tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + step);
+            const tuple_v t2 = ld_stream(in + i + 2 * step), t3 = ld_stream(in + i + 3 * step);
+            atomicAdd(&sh_hist[t0.x & mask], 1u);
+            atomicAdd(&sh_hist[t1.x & mask], 1u);
+            atomicAdd(&sh_hist[t2.x & mask], 1u);
+            atomicAdd(&sh_hist[t3.x & mask], 1u);
+            kor |= t0.x | t1.x | t2.x | t3.x;
+            ror |= t0.y | t1.y | t2.y | t3.y;
+        }
+        for (; i < hi; i += step) {
+            const tuple_v t = ld_stream(in + i);
+            atomicAdd(&sh_hist[t.x & mask], 1u);
+            kor |= t.x;
+            ror |= t.y;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            kor |= __shfl_xor_sync(0xffffffffu, kor, o);
+            ror |= __shfl_xor_sync(0xffffffffu, ror, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicOr(reinterpret_cast<unsigned long long *>(maxima), kor);
+            atomicOr(reinterpret_cast<unsigned long long *>(maxima) + 1, ror);
+        }
+    } else {
+        for (; i + 3 * step < hi; i += 4 * step) {
+            const tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + step);
+            const tuple_v t2 = ld_stream(in + i + 2 * step), t3 = ld_stream(in + i + 3 * step);
+            atomicAdd(&sh_hist[t0.x & mask], 1u);
+            atomicAdd(&sh_hist[t1.x & mask], 1u);
+            atomicAdd(&sh_hist[t2.x & mask], 1u);
+            atomicAdd(&sh_hist[t3.x & mask], 1u);
+        }
+        for (; i < hi; i += step) atomicAdd(&sh_hist[ld_stream(in + i).x & mask], 1u);
     }
-    for (; i < hi; i += step) atomicAdd(&sh_hist[ld_stream(in + i).x & mask], 1u);
     __syncthreads();
     uint32_t *out = chunk_hist + (size_t)c * nbins;
     for (int v = threadIdx.x; v < nbins; v += blockDim.x) out[v] = sh_hist[v];
 }
 
 // ------------------------------------------------------------------------------------------------
-// 2. Per bin, exclusive prefix over the chunks of its relation, and the relation totals.
+// 2. Per bin, exclusive prefix over the chunks of its relation, and the relation totals. Four
+//    consecutive lanes share one bin and split its chunks into four ranges: each lane sums its range,
+//    the four sums are scanned with shuffles, then each lane writes the prefixes of its range.
 // ------------------------------------------------------------------------------------------------
 __global__ void colscan_kernel(const uint32_t *__restrict__ chunk_hist, uint32_t *__restrict__ prefix,
                                uint32_t *__restrict__ total, int nbins, ChunkGeom cg) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= 2u * (uint32_t)nbins) return;
-    const int rel = g >= (uint32_t)nbins;
-    const uint32_t v = rel ? g - nbins : g;
+    const uint32_t col = g >> 2, seg = g & 3u;
+    const bool active = col < 2u * (uint32_t)nbins;
+    const int rel = active && col >= (uint32_t)nbins;
+    const uint32_t v = active ? (rel ? col - nbins : col) : 0u;
     const uint32_t c0 = rel ? cg.cR : 0, c1 = rel ? cg.cR + cg.cS : cg.cR;
-    uint32_t run = 0;
-    uint32_t c = c0;
-    constexpr int U = 16;
-    for (; c + U <= c1; c += U) {
-        uint32_t x[U];
+    const uint32_t per = (c1 - c0 + 3) / 4;
+    const uint32_t r0 = c0 + seg * per < c1 ? c0 + seg * per : c1;
+    const uint32_t r1 = r0 + per < c1 ? r0 + per : c1;
+    uint32_t sum = 0;
+    if (active) {
+        uint32_t c = r0;
+        for (; c + 8 <= r1; c += 8) {
+            uint32_t x[8];
 #pragma unroll
-        for (int u = 0; u < U; u++) x[u] = chunk_hist[(size_t)(c + u) * nbins + v];
+            for (int u = 0; u < 8; u++) x[u] = chunk_hist[(size_t)(c + u) * nbins + v];
 #pragma unroll
-        for (int u = 0; u < U; u++) {
+            for (int u = 0; u < 8; u++) sum += x[u];
+        }
+        for (; c < r1; c++) sum += chunk_hist[(size_t)c * nbins + v];
+    }
+    // Exclusive scan of the four range sums (lanes 4k..4k+3 of the warp).
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o, 4);
+        if (seg >= (uint32_t)o) incl += y;
+    }
+    const uint32_t colsum = __shfl_sync(0xffffffffu, incl, 3, 4);
+    if (!active) return;
+    uint32_t run = incl - sum;
+    uint32_t c = r0;
+    for (; c + 8 <= r1; c += 8) {
+        uint32_t x[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) x[u] = chunk_hist[(size_t)(c + u) * nbins + v];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
             prefix[(size_t)(c + u) * nbins + v] = run;
             run += x[u];
         }
     }
-    for (; c < c1; c++) {
+    for (; c < r1; c++) {
         const uint32_t x = chunk_hist[(size_t)c * nbins + v];
         prefix[(size_t)c * nbins + v] = run;
         run += x;
     }
-    total[(size_t)rel * nbins + v] = run;
+    if (seg == 3) total[(size_t)rel * nbins + v] = colsum;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -222,46 +289,53 @@ __device__ __forceinline__ uint32_t part_to_value(int f, int passes, int b1, int
 
 __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
     __shared__ uint32_t tmp[32];
+    __shared__ uint64_t s_item_run, s_large_run;
     const int tid = threadIdx.x;
     const int nparts = 1 << a.bits;
+    // Each thread owns a contiguous range of partitions.
+    const int per = (nparts + 1023) / 1024;
+    const int f0 = tid * per < nparts ? tid * per : nparts;
+    const int f1 = f0 + per < nparts ? f0 + per : nparts;
     for (int rel = 0; rel < 2; rel++) {
         uint64_t *start = a.start + (size_t)rel * (nparts + 1);
         const uint32_t *tot = a.total + (size_t)rel * nparts;
-        uint64_t running = 0;
-        for (int c = 0; c < nparts; c += 1024) {
-            const int f = c + tid;
-            const uint32_t cnt = f < nparts ? tot[part_to_value(f, a.passes, a.b1, a.F2)] : 0u;
-            uint32_t tsum;
-            const uint32_t ex = block_excl_scan_u32(cnt, tmp, &tsum);
-            if (f < nparts) start[f] = running + ex;
-            running += tsum;
+        uint32_t sum = 0;
+        for (int f = f0; f < f1; f++) sum += tot[part_to_value(f, a.passes, a.b1, a.F2)];
+        uint32_t all;
+        uint64_t run = block_excl_scan_u32(sum, tmp, &all);
+        for (int f = f0; f < f1; f++) {
+            start[f] = run;
+            run += tot[part_to_value(f, a.passes, a.b1, a.F2)];
         }
-        if (tid == 0) start[nparts] = running;
+        if (tid == 0) start[nparts] = all;
     }
     __syncthreads();
 
     // Join work items (partitions with both sides non-empty, src/algo/phj.c:459-491) and large
     // partitions.
     const uint64_t *stR = a.start, *stS = a.start + (nparts + 1);
-    uint64_t item_run = 0, large_run = 0;
-    for (int c = 0; c < nparts; c += 1024) {
-        const int f = c + tid;
-        uint64_t nr = 0, ns = 0;
-        if (f < nparts) {
-            nr = stR[f + 1] - stR[f];
-            ns = stS[f + 1] - stS[f];
+    uint32_t asum = 0, bsum = 0, lsum = 0;  // items with |R_p| <= compact cap, other small items, large
+    for (int f = f0; f < f1; f++) {
+        const uint64_t nr = stR[f + 1] - stR[f], ns = stS[f + 1] - stS[f];
+        if (nr > 0 && ns > 0) {
+            if (nr <= (uint64_t)kCompactCap) asum += ceil_div_u64(ns, kProbeChunk);
+            else if (nr <= (uint64_t)kSmemCap) bsum += ceil_div_u64(ns, kProbeChunk);
+            else lsum++;
         }
-        const bool both = nr > 0 && ns > 0;
-        const bool small = both && nr <= (uint64_t)kSmemCap;
-        const bool large = both && !small;
-        const uint32_t k = small ? ceil_div_u64(ns, kProbeChunk) : 0u;
-        uint32_t ktot, ltot;
-        const uint32_t kex = block_excl_scan_u32(k, tmp, &ktot);
-        const uint32_t lex = block_excl_scan_u32(large ? 1u : 0u, tmp, &ltot);
-        if (small) {
-            for (uint32_t q = 0; q < k; q++) {
-                const uint64_t idx = item_run + kex + q;
-                if (idx < a.max_items) {
+    }
+    uint32_t atot, btot, ltot;
+    uint64_t a_idx = block_excl_scan_u32(asum, tmp, &atot);
+    uint64_t b_idx = block_excl_scan_u32(bsum, tmp, &btot) + atot;
+    uint64_t large_idx = block_excl_scan_u32(lsum, tmp, &ltot);
+    const uint32_t ktot = atot + btot;
+    for (int f = f0; f < f1; f++) {
+        const uint64_t nr = stR[f + 1] - stR[f], ns = stS[f + 1] - stS[f];
+        if (!(nr > 0 && ns > 0)) continue;
+        if (nr <= (uint64_t)kSmemCap) {
+            uint64_t &item_idx = nr <= (uint64_t)kCompactCap ? a_idx : b_idx;
+            const uint32_t k = ceil_div_u64(ns, kProbeChunk);
+            for (uint32_t q = 0; q < k; q++, item_idx++) {
+                if (item_idx < a.max_items) {
                     JoinItem it;
                     it.r_begin = stR[f];
                     it.s_begin = stS[f] + (uint64_t)q * kProbeChunk;
@@ -269,15 +343,13 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
                     const uint64_t rem = ns - (uint64_t)q * kProbeChunk;
                     it.s_len = (uint32_t)(rem < (uint64_t)kProbeChunk ? rem : (uint64_t)kProbeChunk);
                     it.pad[0] = it.pad[1] = 0;
-                    a.items[idx] = it;
+                    a.items[item_idx] = it;
                 } else {
                     atomicOr(&a.counters[kCtrErr], kErrCapacity);
                 }
             }
-        }
-        if (large) {
-            const uint64_t li = large_run + lex;
-            if (li < a.max_large) {
+        } else {
+            if (large_idx < a.max_large) {
                 LargePart lp;
                 lp.r_begin = stR[f];
                 lp.s_begin = stS[f];
@@ -289,15 +361,20 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
                 lp.pad = 0;
                 lp.table_off = 0;
                 lp.r_flat = lp.s_flat = 0;
-                a.large[li] = lp;
+                a.large[large_idx] = lp;
             } else {
                 atomicOr(&a.counters[kCtrErr], kErrCapacity);
             }
+            large_idx++;
         }
-        item_run += ktot;
-        large_run += ltot;
-        __syncthreads();
     }
+    if (tid == 0) a.counters[kCtrNItemsA] = atot < a.max_items ? atot : (uint32_t)a.max_items;
+    if (tid == 0) {
+        s_item_run = ktot;
+        s_large_run = ltot;
+    }
+    __syncthreads();
+    const uint64_t item_run = s_item_run, large_run = s_large_run;
     __syncthreads();
     if (tid == 0) {
         const uint64_t nl = large_run < a.max_large ? large_run : a.max_large;
@@ -329,27 +406,39 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
 __global__ void units_kernel(const uint32_t *__restrict__ chunk_hist, const uint32_t *__restrict__ prefix,
                              const uint64_t *__restrict__ start, int bits, int b1, int F1, int F2,
                              ChunkGeom cg, uint64_t *__restrict__ unit_off, uint32_t *__restrict__ unit_cnt) {
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t nchunks = cg.cR + cg.cS;
-    if (wid >= nchunks * (uint32_t)F1) return;
-    const uint32_t c = wid / F1, d1 = wid % F1;
+    // One CTA per chunk, one thread per pass-1 digit; for a fixed pass-2 digit the threads read
+    // consecutive bins.
+    const uint32_t c = blockIdx.x;
+    const uint32_t d1 = threadIdx.x;
+    if (d1 >= (uint32_t)F1) return;
     const int rel = c < cg.cR ? 0 : 1;
     const int nbins = 1 << bits;
     const uint32_t *h = chunk_hist + (size_t)c * nbins;
     const uint32_t *p = prefix + (size_t)c * nbins;
     uint64_t cnt = 0, pre = 0;
-    for (int d2 = lane; d2 < F2; d2 += 32) {
+    int d2 = 0;
+    for (; d2 + 8 <= F2; d2 += 8) {
+        uint32_t x[8], y[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const uint32_t v = d1 | ((uint32_t)(d2 + u) << b1);
+            x[u] = h[v];
+            y[u] = p[v];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            cnt += x[u];
+            pre += y[u];
+        }
+    }
+    for (; d2 < F2; d2++) {
         const uint32_t v = d1 | ((uint32_t)d2 << b1);
         cnt += h[v];
         pre += p[v];
     }
-    cnt = warp_sum_u64(cnt);
-    pre = warp_sum_u64(pre);
-    if (lane == 0) {
-        unit_cnt[wid] = (uint32_t)cnt;
-        unit_off[wid] = start[(size_t)rel * (nbins + 1) + (size_t)d1 * F2] + pre;
-    }
+    const uint32_t wid = c * (uint32_t)F1 + d1;
+    unit_cnt[wid] = (uint32_t)cnt;
+    unit_off[wid] = start[(size_t)rel * (nbins + 1) + (size_t)d1 * F2] + pre;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -639,12 +728,115 @@ struct JoinArgs {
     const tuple_v *finR, *finS;
     uint32_t *large_table;
     int bits;
-    int lp;
+    int lp;     // first match per probe tuple (lowest build position) instead of all matches
+    int skip0;  // build tuples with key 0 never match (key 0 marks an empty slot in lp_join)
     JoinAccum *acc;
 };
 
 constexpr int kHeadMax = 16384;  // next_pow_2(kSmemCap)
 constexpr size_t kJoinSmem = (size_t)kSmemCap * 16 + kHeadMax * 2 + (size_t)kSmemCap * 2;
+
+// The compact table applies when every build key, shifted right by the radix bits, and every build
+// row id fit in 32 bits (OR of all of them gathered by the histogram pass).
+__device__ __forceinline__ bool compact_applies(const JoinArgs &a) {
+    const unsigned long long *mx = reinterpret_cast<const unsigned long long *>(a.counters + kCtrMaxKey);
+    return (mx[0] >> a.bits) < (1ull << 32) && mx[1] < (1ull << 32);
+}
+
+constexpr size_t kCompactSmem = (size_t)kCompactCap * (4 + 4 + 2 + 2);
+
+// Partition join with 4-byte keys (key >> bits) and 4-byte row ids in shared memory: 96 KiB per CTA,
+// two CTAs per SM, so one CTA's build overlaps the other's probe. Same results as join_small_kernel;
+// within a partition the low `bits` key bits are equal, so comparing key >> bits is comparing keys.
+__global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint32_t *rkey = reinterpret_cast<uint32_t *>(smem);         // [kCompactCap]
+    uint32_t *rrid = rkey + kCompactCap;                           // [kCompactCap]
+    uint16_t *head = reinterpret_cast<uint16_t *>(rrid + kCompactCap);  // [kCompactCap]
+    uint16_t *nxt = head + kCompactCap;                            // [kCompactCap]
+    __shared__ unsigned long long red[64];
+    __shared__ uint32_t s_item;
+    if (!compact_applies(a)) return;
+    const int tid = threadIdx.x;
+    unsigned int *err = &a.counters[kCtrErr];
+    const uint32_t nA = a.counters[kCtrNItemsA];
+    const int B = a.bits;
+    const bool lp = a.lp != 0;
+    const bool skip0 = a.skip0 != 0;
+    unsigned long long cnt = 0, sum = 0;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(&a.counters[kCtrItemA], 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= nA) break;
+        const JoinItem item = a.items[it];
+        const uint32_t nr = item.r_len;
+        const uint32_t nb = next_pow2_u32(nr);
+        const uint64_t hmask = nb - 1;
+        uint32_t *head32 = reinterpret_cast<uint32_t *>(head);
+        for (uint32_t q = tid; q < (nb + 1) / 2; q += kCompactThreads) head32[q] = 0;
+        __syncthreads();
+        // Load and chain the build side; lp_join skips key 0, which reads as an empty slot there.
+        const tuple_v *R = a.finR + item.r_begin;
+        for (uint32_t i0 = tid; i0 < nr; i0 += 4 * kCompactThreads) {
+            tuple_v t[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t i = i0 + u * kCompactThreads;
+                t[u] = i < nr ? ld_stream(R + i) : make_ulonglong2(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t i = i0 + u * kCompactThreads;
+                if (i >= nr) continue;
+                rkey[i] = (uint32_t)(t[u].x >> B);
+                rrid[i] = (uint32_t)t[u].y;
+                if (skip0 && t[u].x == 0) continue;
+                nxt[i] = (uint16_t)atomic_exch_u16(&head[(t[u].x >> B) & hmask], i + 1);
+            }
+        }
+        __syncthreads();
+        const tuple_v *S = a.finS + item.s_begin;
+        const uint32_t ns = item.s_len;
+        for (uint32_t j0 = tid; j0 < ns; j0 += 4 * kCompactThreads) {
+            tuple_v sv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t j = j0 + u * kCompactThreads;
+                sv[u] = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t j = j0 + u * kCompactThreads;
+                if (j >= ns) continue;
+                const uint64_t khi = sv[u].x >> B;
+                uint32_t e = head[khi & hmask];
+                uint32_t best = 0, steps = 0;
+                while (e) {
+                    if ((uint64_t)rkey[e - 1] == khi) {
+                        if (lp) {
+                            if (best == 0 || e < best) best = e;
+                        } else {
+                            cnt++;
+                            sum += (unsigned long long)rrid[e - 1] + sv[u].y;
+                        }
+                    }
+                    e = nxt[e - 1];
+                    if (++steps > nr) {
+                        set_error(err, kErrProbeLimit);
+                        break;
+                    }
+                }
+                if (lp && best) {
+                    cnt++;
+                    sum += (unsigned long long)rrid[best - 1] + sv[u].y;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
+}
 
 __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -665,11 +857,14 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
     const uint32_t nitems = a.counters[kCtrNItems];
     const int B = a.bits;
     const bool lp = a.lp != 0;
+    const bool skip0 = a.skip0 != 0;
+    // Items [0, nA) went to the compact kernel if the build side's keys and row ids fit it.
+    const uint32_t first_item = compact_applies(a) ? a.counters[kCtrNItemsA] : 0u;
     unsigned long long cnt = 0, sum = 0;
     uint32_t phase = 0;
     bool ok = true;
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(&a.counters[kCtrItem], 1u);
+        if (tid == 0) s_item = first_item + atomicAdd(&a.counters[kCtrItem], 1u);
         __syncthreads();
         const uint32_t it = s_item;
         if (it >= nitems) break;
@@ -701,12 +896,11 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
             ok = false;
         }
         phase ^= 1u;
-        __syncthreads();
-        if (!ok) break;
+        if (__syncthreads_or(!ok)) break;
         // Build: chain every R tuple (lp_join skips key 0, which reads as an empty slot there).
         for (uint32_t i = tid; i < nr; i += kJoinThreads) {
             const uint64_t k = rt[i].x;
-            if (lp && k == 0) continue;
+            if (skip0 && k == 0) continue;
             const uint32_t h = (uint32_t)((k >> B) & hmask);
             nxt[i] = (uint16_t)atomic_exch_u16(&head[h], i + 1);
         }
@@ -783,7 +977,7 @@ __global__ void join_large_build(JoinArgs a) {
         const LargePart &L = a.large[l];
         const uint64_t i = g - L.r_flat;
         const uint64_t k = a.finR[L.r_begin + i].x;
-        if (a.lp && k == 0) continue;
+        if (a.skip0 && k == 0) continue;
         uint32_t *head = a.large_table + L.table_off;
         uint32_t *nxt = head + (1ull << L.nb_log);
         const uint64_t h = (k >> a.bits) & ((1ull << L.nb_log) - 1);
@@ -949,7 +1143,23 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
 
 static bool g_attr_done[64] = {};
 
-int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
+int phj_prepare_device() {
+    int cur_dev = 0;
+    HJ_CU(cudaGetDevice(&cur_dev));
+    if (cur_dev < 0 || cur_dev >= 64) return HJ_E_INVAL;
+    if (g_attr_done[cur_dev]) return HJ_OK;
+    const size_t scatter_smem = (size_t)2 * kTile * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
+    HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
+    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
+    HJ_CU(cudaFuncSetAttribute(join_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
+    HJ_CU(cudaFuncSetAttribute(join_compact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kCompactSmem));
+    g_attr_done[cur_dev] = true;
+    return HJ_OK;
+}
+
+int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                 int num_sms, cudaEvent_t *ph, uint32_t *launches) {
     uint32_t nlaunch = 0;
@@ -966,26 +1176,20 @@ int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, con
     cg.cR = s.cR;
     cg.cS = s.cS;
     const uint32_t nchunks = cg.cR + cg.cS;
-    int cur_dev = 0;
-    HJ_CU(cudaGetDevice(&cur_dev));
-    if (cur_dev < 0 || cur_dev >= 64) return HJ_E_INVAL;
-    if (!g_attr_done[cur_dev]) {
-        HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
-        HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
-        HJ_CU(cudaFuncSetAttribute(join_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kJoinSmem));
-        g_attr_done[cur_dev] = true;
+    {
+        const int rc = phj_prepare_device();
+        if (rc) return rc;
     }
     HJ_CU(cudaMemsetAsync(s.counters, 0, kNumCounters * 4, st));
 
     // 1. per-chunk histograms
     HJ_PH(0);
-    hist_chunk_kernel<<<nchunks, 512, hist_smem, st>>>(R, nR, S, nS, g.bits, cg, s.chunk_hist);
+    hist_chunk_kernel<<<nchunks, 512, hist_smem, st>>>(R, nR, S, nS, g.bits, cg, s.chunk_hist,
+                                                       s.counters + kCtrMaxKey);
     HJ_CU(cudaGetLastError());
     HJ_PH(1);
     // 2. prefix over chunks, 3. plan, 4. units
-    colscan_kernel<<<(2 * np + 255) / 256, 256, 0, st>>>(s.chunk_hist, s.prefix, s.total, np, cg);
+    colscan_kernel<<<(8 * np + 255) / 256, 256, 0, st>>>(s.chunk_hist, s.prefix, s.total, np, cg);
     PlanArgs pa;
     pa.bits = g.bits;
     pa.passes = g.passes;
@@ -1004,9 +1208,9 @@ int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, con
     pa.large_table_words = s.large_table_words;
     plan_kernel<<<1, 1024, 0, st>>>(pa);
     {
-        const uint32_t warps = nchunks * (uint32_t)F1;
-        units_kernel<<<(warps * 32 + 255) / 256, 256, 0, st>>>(s.chunk_hist, s.prefix, s.start, g.bits, g.b1, F1,
-                                                               g.passes == 2 ? F2 : 1, cg, s.unit_off, s.unit_cnt);
+        const int ut = F1 < 32 ? 32 : F1;
+        units_kernel<<<nchunks, ut, 0, st>>>(s.chunk_hist, s.prefix, s.start, g.bits, g.b1, F1, g.passes == 2 ? F2 : 1,
+                                             cg, s.unit_off, s.unit_cnt);
     }
     HJ_CU(cudaGetLastError());
     nlaunch += 4;
@@ -1056,7 +1260,9 @@ int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, con
     ja.large_table = s.large_table;
     ja.bits = g.bits;
     ja.lp = lp ? 1 : 0;
+    ja.skip0 = skip0 ? 1 : 0;
     ja.acc = acc;
+    join_compact_kernel<<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
     join_small_kernel<<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
     HJ_CU(cudaGetLastError());
     HJ_PH(5);
@@ -1066,7 +1272,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, const ulonglong2 *R, size_t nR, con
     copy_error<<<1, 32, 0, st>>>(s.counters, acc);
     HJ_CU(cudaGetLastError());
     HJ_PH(6);
-    nlaunch += 5;
+    nlaunch += 6;
     if (launches) *launches = nlaunch;
 #undef HJ_PH
     return HJ_OK;

@@ -177,6 +177,65 @@ int hj_gen_zipf_device(size_t nS, size_t nR, double zipf_factor, uint64_t seed,
 void hj_pkfk_closed_form(size_t nR, size_t nS, uint64_t *matched, uint64_t *checksum);
 
 /* ----------------------------------------------------------------------------------------------
+ * Batched joins: many independent joins of uneven sizes as one captured launch sequence. The
+ * reference runs one join per invocation (src/main.c:429-448); this layer has no counterpart there.
+ * An autotuner decides per join between the non-partitioned join (global table) and the
+ * radix-partitioned pipeline with its own radix bits; results always equal the named algorithm's.
+ * -------------------------------------------------------------------------------------------- */
+#define HJ_F_NO_GRAPH 0x8u /* batches: launch the kernels one by one instead of one captured graph */
+
+typedef struct {
+    double nphj_max_table_bytes; /* joins whose global table (32 B per build tuple) fits run as nphj */
+    double wave_table_bytes;     /* table bytes per wave of non-partitioned joins (a share of L2) */
+    int partition_target;        /* partitioned joins: radix bits so build partitions hold ~this many */
+    int calibrated;              /* 1 after hj_tuner_calibrate */
+} hj_tuner_t;
+
+typedef struct {
+    hj_algo_t algo;              /* result semantics: the reference algorithm the join stands for */
+    const hj_tuple_t *R;         /* device pointers */
+    size_t nR;
+    const hj_tuple_t *S;
+    size_t nS;
+} hj_batch_job_t;
+
+typedef struct {
+    uint64_t matched_cnt;
+    uint64_t checksum;
+    int status;                  /* HJ_OK or an HJ_E_* code for this join */
+    int impl;                    /* what ran: 0 = non-partitioned table, 1 = radix-partitioned */
+    int num_radix_bits;          /* radix-partitioned joins: bits and passes chosen */
+    int num_passes;
+} hj_batch_result_t;
+
+typedef struct {
+    double seconds;              /* device time of the whole batch (CUDA events) */
+    uint32_t kernel_launches;    /* kernels the batch launches */
+    int waves;                   /* waves of non-partitioned joins */
+    int nphj_jobs, phj_jobs;
+} hj_batch_stats_t;
+
+typedef struct hj_batch hj_batch_t;
+
+int hj_tuner_get(hj_ctx_t *ctx, hj_tuner_t *out);
+int hj_tuner_set(hj_ctx_t *ctx, const hj_tuner_t *in);
+/* Decision for one join of the given sizes (impl 0/1 as in hj_batch_result_t). */
+int hj_tuner_decide(hj_ctx_t *ctx, size_t nR, size_t nS, int *impl, int *bits, int *passes);
+/* Time both implementations on PK-FK joins with |S| = 8|R|, |R| = 2^16..2^24, and set the table budget
+ * to the largest build where the non-partitioned join won. report (optional) receives triples
+ * (|R|, seconds non-partitioned, seconds partitioned). Allocates temporary device memory. */
+int hj_tuner_calibrate(hj_ctx_t *ctx, double *report, int report_len);
+/* Plan a batch: decisions, device memory for all of it, and (unless HJ_F_NO_GRAPH) the captured
+ * graph. The relations must stay valid and unchanged in place until hj_batch_destroy. */
+int hj_batch_plan(hj_ctx_t *ctx, const hj_batch_job_t *jobs, int njobs, const hj_params_t *p, hj_batch_t **out);
+/* Run a planned batch (one graph launch), wait, and fill one result per job. */
+int hj_batch_run(hj_batch_t *b, hj_batch_result_t *results, hj_batch_stats_t *stats);
+int hj_batch_destroy(hj_batch_t *b);
+/* plan + run + destroy */
+int hj_join_batch(hj_ctx_t *ctx, const hj_batch_job_t *jobs, int njobs, const hj_params_t *p,
+                  hj_batch_result_t *results, hj_batch_stats_t *stats);
+
+/* ----------------------------------------------------------------------------------------------
  * Allocation-free join. This entry point has no counterpart in the reference, whose joins allocate
  * their tables per call (src/algo/nphj.c:745-757).
  *

@@ -190,3 +190,29 @@ def test_context_reuse_is_deterministic(hj, oracle, cuda):
             for a in ALGOS:
                 r = hj.join(a, R, S, ctx=ctx)
                 assert (r.matched_cnt, r.checksum) == want[a]
+
+
+@pytest.mark.parametrize("wide_fields", [False, True])
+@pytest.mark.parametrize("algo", ["phj_radix_bc", "phj_radix_lp"])
+def test_mixed_partition_sizes(hj, oracle, cuda, algo, wide_fields):
+    """Partitions below the compact table's capacity, between it and the shared-memory capacity, and
+    above it (global-memory path) in one join; with 32-bit-fitting keys/row ids (compact table used)
+    and with 64-bit ones (compact table not applicable)."""
+    rng = np.random.default_rng(31 + wide_fields)
+    sizes = {0: 5000, 1: 9000, 2: 9800, 3: 20000}  # partition (key & 3) -> |R_p|
+    parts = []
+    for p, n in sizes.items():
+        hi = rng.permutation(4 * n)[:n].astype(np.uint64) + np.uint64(1)
+        parts.append((hi << np.uint64(2)) | np.uint64(p))
+    keys = np.concatenate(parts)
+    if wide_fields:
+        keys = keys | np.uint64(1 << 62)
+    R = np.empty((keys.shape[0], 2), dtype=np.uint64)
+    R[:, 0] = rng.permutation(keys)
+    R[:, 1] = rng.integers(0, 2**63 if wide_fields else 2**31, R.shape[0], dtype=np.uint64)
+    R[::50, 0] = R[1::50, 0]  # some duplicate build keys
+    S = R[rng.integers(0, R.shape[0], 200_000)].copy()
+    S[:, 1] = rng.integers(0, 2**31, S.shape[0], dtype=np.uint64)
+    S[::9, 0] += np.uint64(4)  # misses in the same partition
+    got = run(hj, algo, R, S, cuda, bits=2, passes=1)
+    assert got == oracle.join(algo, R, S)
