@@ -25,6 +25,7 @@
 #include "hj_common.cuh"
 #include "hj_ctx.h"
 #include "hj_internal.h"
+#include "hj_nphj.cuh"
 
 namespace hj {
 
@@ -70,47 +71,54 @@ __device__ __forceinline__ void mj_range(unsigned long long total, unsigned long
     *hi = *lo + chunk < total ? *lo + chunk : total;
 }
 
-__global__ void mj_build(const MJob *__restrict__ jobs, int njobs, const unsigned long long *__restrict__ r_flat,
-                         unsigned long long total) {
-    extern __shared__ unsigned long long sflat[];
-    mj_load_flat(sflat, r_flat, njobs);
-    unsigned long long lo, hi;
-    mj_range(total, &lo, &hi);
-    int j = -1;
-    unsigned long long jbeg = 0, jend = 0;
-    MJob J;
-    for (unsigned long long g = lo + threadIdx.x; g < hi; g += blockDim.x) {
-        if (j < 0 || g >= jend || g < jbeg) {
-            j = mj_find(sflat, njobs, g);
-            J = jobs[j];
-            jbeg = sflat[j];
-            jend = sflat[j + 1];
+// A piece of one job's build or probe side: the multi-join kernels take these as work items, so a
+// block always works on a single job.
+struct MChunk {
+    unsigned int job;
+    unsigned int len;
+    unsigned long long begin;
+};
+
+__device__ __forceinline__ void mj_insert(const MJob &J, const tuple_v t, unsigned long long i) {
+    if (J.skip0 && t.x == 0) return;
+    if (t.x == kMjEmpty) {
+        if (atomicAdd(&J.side->cnt, 1ull) >= 1ull) atomicOr(&J.side->dup, 1u);
+        atomicAdd(&J.side->sum, (unsigned long long)t.y);
+        atomicMax(&J.side->notpos, ~i);
+        return;
+    }
+    unsigned long long h = table_hash(t.x, J.cap);
+    for (unsigned long long steps = 0;; steps++) {
+        const unsigned long long cur = atomicCAS(&J.table[h].x, kMjEmpty, (unsigned long long)t.x);
+        if (cur == kMjEmpty) {
+            J.table[h].y = t.y;
+            return;
         }
-        const unsigned long long i = g - jbeg;
-        const tuple_v t = ld_stream(J.R + i);
-        if (J.skip0 && t.x == 0) continue;
-        if (t.x == kMjEmpty) {
-            if (atomicAdd(&J.side->cnt, 1ull) >= 1ull) atomicOr(&J.side->dup, 1u);
-            atomicAdd(&J.side->sum, (unsigned long long)t.y);
-            atomicMax(&J.side->notpos, ~i);
-            continue;
+        if (cur == t.x && !J.side->dup) atomicOr(&J.side->dup, 1u);
+        if (++h == J.cap) h = 0;
+        if (steps + 1 >= J.cap) {
+            set_error(&J.acc->error, kErrProbeLimit);
+            return;
         }
-        unsigned long long h = table_hash(t.x, J.cap);
-        for (unsigned long long steps = 0;; steps++) {
-            unsigned long long *kp = &J.table[h].x;
-            unsigned long long cur = *reinterpret_cast<volatile unsigned long long *>(kp);
-            if (cur == kMjEmpty) {
-                cur = atomicCAS(kp, kMjEmpty, (unsigned long long)t.x);
-                if (cur == kMjEmpty) {
-                    J.table[h].y = t.y;
-                    break;
-                }
+    }
+}
+
+__global__ void mj_build(const MJob *__restrict__ jobs, const MChunk *__restrict__ chunks, int nchunks) {
+    constexpr int U = 4;
+    for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const MChunk ch = chunks[c];
+        const MJob J = jobs[ch.job];
+        for (unsigned e0 = threadIdx.x; e0 < ch.len; e0 += U * blockDim.x) {
+            tuple_v t[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const unsigned e = e0 + u * blockDim.x;
+                t[u] = e < ch.len ? ld_stream(J.R + ch.begin + e) : make_ulonglong2(0, 0);
             }
-            if (cur == t.x && !J.side->dup) atomicOr(&J.side->dup, 1u);
-            if (++h == J.cap) h = 0;
-            if (steps + 1 >= J.cap) {
-                set_error(&J.acc->error, kErrProbeLimit);
-                break;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const unsigned e = e0 + u * blockDim.x;
+                if (e < ch.len) mj_insert(J, t[u], ch.begin + e);
             }
         }
     }
@@ -209,66 +217,37 @@ __global__ void mj_lp_resolve(const MJob *__restrict__ jobs, int njobs, const un
     }
 }
 
-__device__ __forceinline__ void mj_flush(JoinAccum *acc, unsigned long long &cnt, unsigned long long &sum) {
-    if (cnt) atomicAdd(&acc->matched, cnt);
-    if (sum) atomicAdd(&acc->checksum, sum);
-    cnt = 0;
-    sum = 0;
-}
-
-__global__ void mj_probe(const MJob *__restrict__ jobs, int njobs, const unsigned long long *__restrict__ s_flat,
-                         unsigned long long total) {
-    extern __shared__ unsigned long long sflat[];
-    mj_load_flat(sflat, s_flat, njobs);
-    unsigned long long lo, hi;
-    mj_range(total, &lo, &hi);
-    int j = -1;
-    unsigned long long jbeg = 0, jend = 0;
-    MJob J;
-    bool first_only = true;
-    unsigned long long side_cnt = 0;
-    unsigned long long cnt = 0, sum = 0;
-    for (unsigned long long g = lo + threadIdx.x; g < hi; g += blockDim.x) {
-        if (j < 0 || g >= jend || g < jbeg) {
-            if (j >= 0) mj_flush(J.acc, cnt, sum);
-            j = mj_find(sflat, njobs, g);
-            J = jobs[j];
-            jbeg = sflat[j];
-            jend = sflat[j + 1];
-            first_only = J.lp || !*reinterpret_cast<volatile unsigned int *>(&J.side->dup);
-            side_cnt = J.side->cnt;
-        }
-        const tuple_v s = ld_stream(J.S + (g - jbeg));
-        if (J.skip0 && s.x == 0) continue;
-        if (s.x == kMjEmpty) {
-            if (side_cnt) {
-                if (J.lp) {
-                    cnt++;
-                    sum += J.R[~J.side->notpos].y + s.y;
-                } else {
-                    cnt += side_cnt;
-                    sum += J.side->sum + side_cnt * s.y;
-                }
+__global__ void __launch_bounds__(256, 8) mj_probe(const MJob *__restrict__ jobs, const MChunk *__restrict__ chunks,
+                                                  int nchunks) {
+    __shared__ unsigned long long red[64];
+    constexpr int U = 2;
+    for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const MChunk ch = chunks[c];
+        const MJob J = jobs[ch.job];
+        ProbeArgs P;
+        P.table = J.table;
+        P.cap = J.cap;
+        P.lp = J.lp != 0;
+        P.skip0 = J.skip0 != 0;
+        P.first_only = P.lp || *reinterpret_cast<volatile unsigned int *>(&J.side->dup) == 0;
+        P.side_cnt = J.side->cnt;
+        P.side_sum = J.side->sum;
+        P.side_first_rid = P.side_cnt ? J.R[~J.side->notpos].y : 0;
+        P.err = &J.acc->error;
+        unsigned long long cnt = 0, sum = 0;
+        for (unsigned e0 = threadIdx.x; e0 < ch.len; e0 += U * blockDim.x) {
+            tuple_v sv[U];
+            bool valid[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const unsigned e = e0 + u * blockDim.x;
+                valid[u] = e < ch.len;
+                sv[u] = valid[u] ? ld_stream(J.S + ch.begin + e) : make_ulonglong2(0, 0);
             }
-            continue;
+            probe_group<U>(P, sv, valid, cnt, sum);
         }
-        unsigned long long h = table_hash(s.x, J.cap);
-        for (unsigned long long steps = 0;; steps++) {
-            const tuple_v e = J.table[h];
-            if (e.x == kMjEmpty) break;
-            if (e.x == s.x) {
-                cnt++;
-                sum += e.y + s.y;
-                if (first_only) break;
-            }
-            if (++h == J.cap) h = 0;
-            if (steps + 1 >= J.cap) {
-                set_error(&J.acc->error, kErrProbeLimit);
-                break;
-            }
-        }
+        block_sum2_to(cnt, sum, red, &J.acc->matched, &J.acc->checksum);
     }
-    if (j >= 0) mj_flush(J.acc, cnt, sum);
 }
 
 }  // namespace hj
@@ -289,8 +268,22 @@ struct Wave {
     unsigned long long total_r, total_s, total_t;
     hj::MJob *jobs_dev;
     unsigned long long *r_flat, *s_flat, *t_flat;  // device, count + 1 each
+    hj::MChunk *r_chunks, *s_chunks;                // device work items of the build and probe kernels
+    int n_r_chunks, n_s_chunks;
     bool any_lp;
 };
+
+constexpr unsigned kBuildChunk = 8192, kProbeChunkMJ = 16384;
+
+void make_chunks(std::vector<hj::MChunk> &out, unsigned job, unsigned long long n, unsigned piece) {
+    for (unsigned long long b = 0; b < n; b += piece) {
+        hj::MChunk c;
+        c.job = job;
+        c.begin = b;
+        c.len = (unsigned)(n - b < piece ? n - b : piece);
+        out.push_back(c);
+    }
+}
 
 size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -359,8 +352,8 @@ int enqueue_batch(hj_batch *b) {
         BCU(cudaMemsetAsync(w.sides, 0, sizeof(hj::MSide) * w.count, st));
         const size_t sm = sizeof(unsigned long long) * (w.count + 1);
         const int grid = sms * 8;
-        if (w.total_r) {
-            hj::mj_build<<<grid, 256, sm, st>>>(w.jobs_dev, w.count, w.r_flat, w.total_r);
+        if (w.n_r_chunks) {
+            hj::mj_build<<<std::min(grid, w.n_r_chunks), 256, 0, st>>>(w.jobs_dev, w.r_chunks, w.n_r_chunks);
             launches++;
         }
         if (w.any_lp && w.total_r) {
@@ -369,8 +362,8 @@ int enqueue_batch(hj_batch *b) {
             hj::mj_lp_resolve<<<grid, 256, sm, st>>>(w.jobs_dev, w.count, w.t_flat, w.total_t);
             launches += 3;
         }
-        if (w.total_s) {
-            hj::mj_probe<<<grid, 256, sm, st>>>(w.jobs_dev, w.count, w.s_flat, w.total_s);
+        if (w.n_s_chunks) {
+            hj::mj_probe<<<std::min(grid, w.n_s_chunks), 256, 0, st>>>(w.jobs_dev, w.s_chunks, w.n_s_chunks);
             launches++;
         }
         BCU(cudaGetLastError());
@@ -463,7 +456,13 @@ int hj_batch_plan(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_p
         for (int q = 0; q < wr.second; q++) t += nphj_slots(jobs[order[wr.first + q]].nR) * 16;
         t += sizeof(hj::MSide) * wr.second;
         max_wave_tables = std::max(max_wave_tables, a256(t));
-        desc_bytes += a256(sizeof(hj::MJob) * wr.second) + 3 * a256(8 * (wr.second + 1));
+        size_t nrc = 0, nsc = 0;
+        for (int q = 0; q < wr.second; q++) {
+            nrc += (jobs[order[wr.first + q]].nR + kBuildChunk - 1) / kBuildChunk;
+            nsc += (jobs[order[wr.first + q]].nS + kProbeChunkMJ - 1) / kProbeChunkMJ;
+        }
+        desc_bytes += a256(sizeof(hj::MJob) * wr.second) + 3 * a256(8 * (wr.second + 1)) +
+                      a256(sizeof(hj::MChunk) * (nrc + 1)) + a256(sizeof(hj::MChunk) * (nsc + 1));
     }
     size_t phj_bytes = 0;
     for (int j : b->phj_jobs) {
@@ -504,6 +503,7 @@ int hj_batch_plan(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_p
         w.count = wr.second;
         std::vector<hj::MJob> mj(w.count);
         std::vector<unsigned long long> rf(w.count + 1, 0), sf(w.count + 1, 0), tf(w.count + 1, 0);
+        std::vector<hj::MChunk> rch, sch;
         char *tp = tables;
         size_t slots_total = 0;
         for (int q = 0; q < w.count; q++) slots_total += nphj_slots(jobs[order[w.first + q]].nR);
@@ -526,6 +526,8 @@ int hj_batch_plan(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_p
             m.skip0 = sem_skip0(J.algo) ? 1u : 0u;
             w.any_lp = w.any_lp || m.lp;
             mj[q] = m;
+            make_chunks(rch, (unsigned)q, J.nR, kBuildChunk);
+            make_chunks(sch, (unsigned)q, J.nS, kProbeChunkMJ);
             rf[q + 1] = rf[q] + J.nR;
             sf[q + 1] = sf[q] + J.nS;
             tf[q + 1] = tf[q] + m.cap;
@@ -543,6 +545,15 @@ int hj_batch_plan(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_p
         cur += a256(8 * (w.count + 1));
         w.t_flat = reinterpret_cast<unsigned long long *>(cur);
         cur += a256(8 * (w.count + 1));
+        w.n_r_chunks = (int)rch.size();
+        w.n_s_chunks = (int)sch.size();
+        w.r_chunks = reinterpret_cast<hj::MChunk *>(cur);
+        cur += a256(sizeof(hj::MChunk) * (rch.size() + 1));
+        w.s_chunks = reinterpret_cast<hj::MChunk *>(cur);
+        cur += a256(sizeof(hj::MChunk) * (sch.size() + 1));
+        if ((rch.size() && cudaMemcpy(w.r_chunks, rch.data(), sizeof(hj::MChunk) * rch.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
+            (sch.size() && cudaMemcpy(w.s_chunks, sch.data(), sizeof(hj::MChunk) * sch.size(), cudaMemcpyHostToDevice) != cudaSuccess))
+            return fail(HJ_E_DEVICE);
         if (cudaMemcpy(w.jobs_dev, mj.data(), sizeof(hj::MJob) * w.count, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(w.r_flat, rf.data(), 8 * (w.count + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(w.s_flat, sf.data(), 8 * (w.count + 1), cudaMemcpyHostToDevice) != cudaSuccess ||

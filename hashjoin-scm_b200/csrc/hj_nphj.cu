@@ -20,10 +20,11 @@
 
 #include "hj_common.cuh"
 #include "hj_internal.h"
+#include "hj_nphj.cuh"
 
 namespace hj {
 
-constexpr unsigned long long kEmpty = ~0ull;
+constexpr unsigned long long kEmpty = kTableEmpty;
 
 struct NphjSide {
     unsigned long long cnt;      // R tuples with key == kEmpty
@@ -48,37 +49,48 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
     return *reinterpret_cast<const volatile unsigned long long *>(p);
 }
 
-// Insert R tuple (k, rid) at its own slot; records duplicates.
-__global__ void nphj_build(NphjArgs a) {
-    bool seen_dup = false;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.nR;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        const tuple_v t = ld_stream(a.R + i);
-        if (a.skip0 && t.x == 0) continue;
-        if (t.x == kEmpty) {
-            if (atomicAdd(&a.side->cnt, 1ull) >= 1ull) seen_dup = true;
-            atomicAdd(&a.side->sum, (unsigned long long)t.y);
-            atomicMin(&a.side->minpos, i);
-            continue;
+// Insert R tuple i at its own slot; records duplicates.
+__device__ __forceinline__ void nphj_insert(const NphjArgs &a, const tuple_v t, unsigned long long i, bool &seen_dup) {
+    if (a.skip0 && t.x == 0) return;
+    if (t.x == kEmpty) {
+        if (atomicAdd(&a.side->cnt, 1ull) >= 1ull) seen_dup = true;
+        atomicAdd(&a.side->sum, (unsigned long long)t.y);
+        atomicMin(&a.side->minpos, i);
+        return;
+    }
+    unsigned long long h = table_hash(t.x, a.cap);
+    for (unsigned long long steps = 0;;) {
+        // Claim with a CAS straight away: at load <= 0.5 most first slots are empty.
+        const unsigned long long cur = atomicCAS(&a.table[h].x, kEmpty, (unsigned long long)t.x);
+        if (cur == kEmpty) {
+            a.table[h].y = t.y;
+            return;
         }
-        unsigned long long h = table_hash(t.x, a.cap);
-        unsigned long long steps = 0;
-        for (;;) {
-            unsigned long long *kp = &a.table[h].x;
-            unsigned long long cur = ld_volatile_u64(kp);
-            if (cur == kEmpty) {
-                cur = atomicCAS(kp, kEmpty, (unsigned long long)t.x);
-                if (cur == kEmpty) {
-                    a.table[h].y = t.y;
-                    break;
-                }
-            }
-            if (cur == t.x) seen_dup = true;
-            if (++h == a.cap) h = 0;
-            if (++steps >= a.cap) {
-                set_error(&a.acc->error, kErrProbeLimit);
-                break;
-            }
+        if (cur == t.x) seen_dup = true;
+        if (++h == a.cap) h = 0;
+        if (++steps >= a.cap) {
+            set_error(&a.acc->error, kErrProbeLimit);
+            return;
+        }
+    }
+}
+
+__global__ void nphj_build(NphjArgs a) {
+    constexpr int U = 4;
+    bool seen_dup = false;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < a.nR;
+         i0 += U * stride) {
+        tuple_v t[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned long long i = i0 + u * stride;
+            t[u] = i < a.nR ? ld_stream(a.R + i) : make_ulonglong2(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned long long i = i0 + u * stride;
+            if (i < a.nR) nphj_insert(a, t[u], i, seen_dup);
         }
     }
     if (__syncthreads_or(seen_dup) && threadIdx.x == 0) atomicOr(&a.side->dup, 1u);
@@ -131,52 +143,34 @@ __global__ void nphj_lp_resolve(NphjArgs a) {
     }
 }
 
-__global__ void nphj_probe(NphjArgs a) {
+// Two probes per thread at eight 256-thread blocks per SM measured best for tables that sit in L2
+// (more probes per thread cost occupancy through registers).
+__global__ void __launch_bounds__(256, 8) nphj_probe(NphjArgs a) {
     __shared__ unsigned long long red[64];
-    const bool dup = *reinterpret_cast<volatile unsigned int *>(&a.side->dup) != 0;
-    const bool first_only = a.lp || !dup;
-    const unsigned long long side_cnt = a.side->cnt;
+    constexpr int U = 2;
+    ProbeArgs P;
+    P.table = a.table;
+    P.cap = a.cap;
+    P.lp = a.lp != 0;
+    P.skip0 = a.skip0 != 0;
+    P.first_only = P.lp || *reinterpret_cast<volatile unsigned int *>(&a.side->dup) == 0;
+    P.side_cnt = a.side->cnt;
+    P.side_sum = a.side->sum;
+    P.side_first_rid = P.side_cnt ? a.R[a.side->minpos].y : 0;
+    P.err = &a.acc->error;
     unsigned long long cnt = 0, sum = 0;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     for (unsigned long long j0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j0 < a.nS;
-         j0 += 2 * stride) {
-        tuple_v sv[2];
-        sv[0] = ld_stream(a.S + j0);
-        sv[1] = j0 + stride < a.nS ? ld_stream(a.S + j0 + stride) : make_ulonglong2(0, 0);
+         j0 += U * stride) {
+        tuple_v sv[U];
+        bool valid[U];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-            if (u == 1 && j0 + stride >= a.nS) break;
-            const tuple_v s = sv[u];
-            if (a.skip0 && s.x == 0) continue;
-            if (s.x == kEmpty) {
-                if (side_cnt) {
-                    if (a.lp) {
-                        cnt++;
-                        sum += a.R[a.side->minpos].y + s.y;
-                    } else {
-                        cnt += side_cnt;
-                        sum += a.side->sum + side_cnt * s.y;
-                    }
-                }
-                continue;
-            }
-            unsigned long long h = table_hash(s.x, a.cap);
-            unsigned long long steps = 0;
-            for (;;) {
-                const tuple_v e = a.table[h];
-                if (e.x == kEmpty) break;
-                if (e.x == s.x) {
-                    cnt++;
-                    sum += e.y + s.y;
-                    if (first_only) break;
-                }
-                if (++h == a.cap) h = 0;
-                if (++steps >= a.cap) {
-                    set_error(&a.acc->error, kErrProbeLimit);
-                    break;
-                }
-            }
+        for (int u = 0; u < U; u++) {
+            const unsigned long long j = j0 + u * stride;
+            valid[u] = j < a.nS;
+            sv[u] = valid[u] ? ld_stream(a.S + j) : make_ulonglong2(0, 0);
         }
+        probe_group<U>(P, sv, valid, cnt, sum);
     }
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
 }
