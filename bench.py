@@ -50,8 +50,14 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["join", "batch"], default="join",
-                    help="join: the headline 2^27 x 2^29 join; batch: 512 independent joins (config 4)")
+    ap.add_argument("--mode", choices=["join", "batch", "serve"], default="join",
+                    help="join: the headline 2^27 x 2^29 join; batch: 512 independent joins; "
+                         "serve: a Poisson stream of join requests through the join server")
+    ap.add_argument("--rates", default="250,500,1000,1500,2000",
+                    help="serve mode: offered request rates (requests/s) to sweep")
+    ap.add_argument("--requests", type=int, default=1000, help="serve mode: requests per rate")
+    ap.add_argument("--slots", type=int, default=8, help="serve mode: concurrent requests on the GPU")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve mode: HBM pool budget")
     ap.add_argument("--batch-jobs", type=int, default=512)
     ap.add_argument("--calibrate", action="store_true", help="batch mode: calibrate the autotuner first")
     ap.add_argument("--algo", default="phj_radix_bc")
@@ -467,6 +473,152 @@ def run_batch_mode(a, rank, world, local_rank):
     return 0
 
 
+def serve_workload(hj, torch, dev, n_small, seed):
+    """Device-resident relations for served requests: n_small PK-FK pairs sized like the batched joins
+    (|R| log-uniform in [2^10, 2^22], multiple of 256; |S| = k|R|, k uniform in 1..16) and one large pair
+    of 2^26 x 2^28; every pair generated on the device with its own seed."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    sizes = []
+    for i in range(n_small):
+        nR = (int(2 ** rng.uniform(10, 22)) + 255) // 256 * 256
+        k = int(rng.integers(1, 17))
+        sizes.append((nR, k * nR))
+    sizes.append((1 << 26, 1 << 28))
+    total = sum(r + s for r, s in sizes)
+    buf = torch.empty((total, 2), dtype=torch.int64, device=dev)
+    pairs, off = [], 0
+    for i, (nR, nS) in enumerate(sizes):
+        R = buf[off:off + nR]
+        S = buf[off + nR:off + nR + nS]
+        off += nR + nS
+        hj.gen_fast_device(nR, nS, R.data_ptr(), S.data_ptr(), seed=seed + i)
+        pairs.append((R, S, hj.pkfk_closed_form(nR, nS)))
+    torch.cuda.synchronize(dev)
+    return pairs[:-1], pairs[-1], buf
+
+
+def run_serve_mode(a, rank, world, local_rank):
+    """Poisson arrivals at each offered rate; 5% of requests are the 2^26 x 2^28 join. The join server
+    (slots, HBM pool budget, per-request autotuned implementation) is compared with a sequential
+    per-join loop (hj_join with the same per-request decision) serving the same arrival times."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    hj = load_module("hashjoin_scm_b200", PKG_DIR / "__init__.py")
+    hj.lib()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    small, big, buf = serve_workload(hj, torch, dev, 64, 12345 + 1000 * rank)
+    rates = [float(x) for x in a.rates.split(",") if x]
+    rng = np.random.default_rng(777 + rank)
+    streams = []
+    for lam in rates:
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, a.requests))
+        picks = [big if rng.random() < 0.05 else small[int(rng.integers(len(small)))] for _ in range(a.requests)]
+        streams.append((lam, arrivals, picks))
+
+    def pace(t_arr):
+        while True:
+            d = t_arr - hj.now()
+            if d <= 0:
+                return
+            if d > 4e-4:
+                time.sleep(d - 3e-4)
+
+    def summarize(lat, t0, t_last, n):
+        lat = np.sort(np.asarray(lat))
+        return {"joins_per_s": n / (t_last - t0), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat[-1] * 1e3)}
+
+    # 1. the join server
+    srv_out, peak, budget = [], 0.0, 0.0
+    impl_counts = {0: 0, 1: 0}
+    with hj.Server(local_rank, slots=a.slots, hbm_budget_bytes=a.budget_gb * 1e9) as srv:
+        for R, S, _ in small[:8] + [big]:  # warm-up: kernel attributes, first launches
+            srv.wait_all([srv.submit("phj_radix_bc", R, S, on_device=True)])
+        for lam, arrivals, picks in streams:
+            t0 = hj.now() + 0.02
+            ids = []
+            for (R, S, _), t in zip(picks, arrivals):
+                pace(t0 + t)
+                ids.append(srv.submit("phj_radix_bc", R, S, on_device=True))
+            got = srv.wait_all(ids, timeout_s=600.0)
+            lat, t_last = [], t0
+            for rid, (R, S, want), t in zip(ids, picks, arrivals):
+                c = got[rid]
+                if c.status or (c.matched_cnt, c.checksum) != want:
+                    raise RuntimeError("served join result differs from the closed form")
+                lat.append(c.done_s - (t0 + t))
+                t_last = max(t_last, c.done_s)
+                impl_counts[c.impl] += 1
+            srv_out.append(summarize(lat, t0, t_last, len(ids)))
+        st = srv.stats()
+        peak, budget = st.peak_in_use_bytes, st.budget_bytes
+
+    # 2. sequential per-join loop on the same arrivals
+    loop_out = []
+    with hj.Context(local_rank) as ctx:
+        def decided(R, S):
+            impl, bits, passes = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            hj._bind_batch().hj_tuner_decide(ctx.handle, R.shape[0], S.shape[0], ctypes.byref(impl),
+                                             ctypes.byref(bits), ctypes.byref(passes))
+            return ("nphj_sc", {}) if impl.value == 0 else ("phj_radix_bc", {"bits": bits.value, "passes": passes.value})
+
+        plans = {id(p[0]): decided(p[0], p[1]) for p in small + [big]}
+        for R, S, _ in small[:8] + [big]:
+            algo, kw = plans[id(R)]
+            hj.join(algo, R, S, on_device=True, device=local_rank, ctx=ctx, flags=hj.HJ_F_NO_TIMING, **kw)
+        for lam, arrivals, picks in streams:
+            t0 = hj.now() + 0.02
+            lat, t_last = [], t0
+            for (R, S, want), t in zip(picks, arrivals):
+                pace(t0 + t)
+                algo, kw = plans[id(R)]
+                r = hj.join(algo, R, S, on_device=True, device=local_rank, ctx=ctx, flags=hj.HJ_F_NO_TIMING, **kw)
+                done = hj.now()
+                if (r.matched_cnt, r.checksum) != want:
+                    raise RuntimeError("looped join result differs from the closed form")
+                lat.append(done - (t0 + t))
+                t_last = done
+            loop_out.append(summarize(lat, t0, t_last, len(picks)))
+
+    # sustained rate: the highest offered rate the server kept up with (completion rate >= 95% offered)
+    best = 0
+    for i, (lam, _, _) in enumerate(streams):
+        if srv_out[i]["joins_per_s"] >= 0.95 * lam:
+            best = i
+    joins_s = srv_out[best]["joins_per_s"]
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([joins_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        joins_s = float(t.item()) * world
+    if rank == 0:
+        line = {
+            "metric": "served joins/s at p99 latency", "value": joins_s, "unit": "joins/s", "n_gpus": world,
+            "steps": a.requests, "warmup": 9, "ms_per_step": 1e3 / srv_out[best]["joins_per_s"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic",
+            "config": {"workload": "Poisson stream of PK-FK join requests (phj_radix_bc semantics): 95% sized "
+                                   "|R| log-uniform in [2^10, 2^22], |S| = k|R| with k in 1..16, 5% 2^26 x 2^28; "
+                                   "relations device-resident", "requests_per_rate": a.requests,
+                       "slots": a.slots, "hbm_budget_bytes": budget, "peak_pool_bytes": peak},
+            "p50_ms": srv_out[best]["p50_ms"], "p99_ms": srv_out[best]["p99_ms"],
+            "offered_rate": streams[best][0],
+            "sweep": [{"offered_rate": lam, "server": s, "loop": l}
+                      for (lam, _, _), s, l in zip(streams, srv_out, loop_out)],
+            "impl_counts": {"nphj": impl_counts[0], "phj": impl_counts[1]},
+        }
+        print(json.dumps(line), flush=True)
+    del buf
+    return 0
+
+
 def main():
     a = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -486,6 +638,8 @@ def main():
     try:
         if a.mode == "batch":
             return run_batch_mode(a, rank, world, local_rank)
+        if a.mode == "serve":
+            return run_serve_mode(a, rank, world, local_rank)
         return run_ours(a, rank, world, local_rank)
     finally:
         if world > 1:

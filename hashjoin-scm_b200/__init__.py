@@ -417,3 +417,122 @@ class Batch:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ---------------------------------------------------------------------------------------------
+# Join server (include/hjscm.h, "Join server")
+# ---------------------------------------------------------------------------------------------
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double),
+                ("autotune", ctypes.c_int), ("tuner", Tuner)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("matched_cnt", ctypes.c_uint64), ("checksum", ctypes.c_uint64),
+                ("status", ctypes.c_int), ("impl", ctypes.c_int), ("submit_s", ctypes.c_double),
+                ("start_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("admitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("budget_bytes", ctypes.c_double), ("in_use_bytes", ctypes.c_double),
+                ("peak_in_use_bytes", ctypes.c_double), ("queued", ctypes.c_int), ("inflight", ctypes.c_int)]
+
+
+def _bind_server():
+    L = _bind_batch()
+    if getattr(L, "_server_bound", False):
+        return L
+    vp, i32, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    L.hj_now.argtypes = []
+    L.hj_now.restype = ctypes.c_double
+    L.hj_server_config_init.argtypes = [ctypes.POINTER(ServerConfig)]
+    L.hj_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+    L.hj_server_submit.argtypes = [vp, i32, vp, sz, vp, sz, i32, ctypes.POINTER(ctypes.c_uint64)]
+    L.hj_server_poll.argtypes = [vp, ctypes.POINTER(Completion), i32, ctypes.POINTER(i32), i32]
+    L.hj_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.hj_server_destroy.argtypes = [vp]
+    for f in ("hj_server_config_init", "hj_server_create", "hj_server_submit", "hj_server_poll",
+              "hj_server_stats", "hj_server_destroy"):
+        getattr(L, f).restype = i32
+    L._server_bound = True
+    return L
+
+
+def now() -> float:
+    """The library's monotonic clock (seconds), the one server completions are stamped with."""
+    return _bind_server().hj_now()
+
+
+class Server:
+    """A join server (hj_server_t): submit() queues a join and returns its id at once; poll() returns
+    completions. Relations are numpy (n, 2) uint64 arrays (host) or CUDA tensors (on_device=True); the
+    server keeps a reference to them until their completion has been polled."""
+
+    def __init__(self, device: int = 0, slots: int = 8, hbm_budget_bytes: float = 150e9, autotune: bool = True,
+                 tuner: dict | None = None):
+        L = _bind_server()
+        cfg = ServerConfig()
+        L.hj_server_config_init(ctypes.byref(cfg))
+        cfg.device, cfg.slots, cfg.hbm_budget_bytes, cfg.autotune = device, slots, hbm_budget_bytes, int(autotune)
+        for k, v in (tuner or {}).items():
+            setattr(cfg.tuner, k, v)
+        h = ctypes.c_void_p()
+        rc = L.hj_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc:
+            raise JoinError(rc, "hj_server_create")
+        self.handle = h
+        self._keep = {}
+
+    def submit(self, algo: str, R, S, on_device: bool = False) -> int:
+        if not on_device:
+            R = np.ascontiguousarray(R)
+            S = np.ascontiguousarray(S)
+        pr, nr = _ptr_len(R, on_device)
+        ps, ns = _ptr_len(S, on_device)
+        rid = ctypes.c_uint64()
+        rc = _bind_server().hj_server_submit(self.handle, ALGOS[algo], pr, nr, ps, ns, int(on_device),
+                                             ctypes.byref(rid))
+        if rc:
+            raise JoinError(rc, "hj_server_submit")
+        self._keep[rid.value] = (R, S)
+        return rid.value
+
+    def poll(self, max_n: int = 256, wait_ms: int = 0) -> list:
+        buf = (Completion * max_n)()
+        n = ctypes.c_int()
+        rc = _bind_server().hj_server_poll(self.handle, buf, max_n, ctypes.byref(n), wait_ms)
+        if rc:
+            raise JoinError(rc, "hj_server_poll")
+        out = list(buf)[: n.value]
+        for c in out:
+            self._keep.pop(c.id, None)
+        return out
+
+    def wait_all(self, ids, timeout_s: float = 120.0) -> dict:
+        """Poll until every id in ids has completed; returns {id: Completion}."""
+        want, got = set(ids), {}
+        t_end = now() + timeout_s
+        while want - set(got):
+            if now() > t_end:
+                raise JoinError(HJ_E_TIMEOUT, "hj_server_poll")
+            for c in self.poll(wait_ms=50):
+                got[c.id] = c
+        return got
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        _bind_server().hj_server_stats(self.handle, ctypes.byref(st))
+        return st
+
+    def close(self):
+        if self.handle:
+            _bind_server().hj_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -266,6 +266,59 @@ typedef struct {
 int hj_nphj_join_noalloc(hj_algo_t algo, const hj_tuple_t *R_dev, size_t nR, const hj_tuple_t *S_dev,
                          size_t nS, hj_device_result_t *out_dev, void *stream);
 
+/* ----------------------------------------------------------------------------------------------
+ * Join server: requests arrive at any time and are served concurrently under an HBM budget. The
+ * reference runs one join per process (src/main.c:429-448); this layer has no counterpart there.
+ *   - hj_server_create allocates one device pool of hbm_budget_bytes (capped at 92% of the free device
+ *     memory) and `slots` CUDA streams; serving then calls no CUDA allocator.
+ *   - hj_server_submit queues a join and returns at once. Each admitted request takes its scratch (and
+ *     the device copies of host relations) from the pool and returns it on completion; a request is
+ *     admitted when a slot and its memory are free, first come first served, except that later requests
+ *     may pass a head that does not fit yet while the head has waited less than 50 ms. A request that
+ *     can never fit the pool is refused at submission with HJ_E_BUDGET.
+ *   - The relations (host or device, as inputs_on_device says) must stay valid and unchanged until the
+ *     request's completion has been polled.
+ *   - Each request runs the implementation the autotuner picks for its sizes (or, with autotune = 0,
+ *     the named algorithm at 14 radix bits / 2 passes) with the named algorithm's result semantics, so
+ *     its result is the same as hj_join's, alone or in any mix.
+ * -------------------------------------------------------------------------------------------- */
+typedef struct {
+    int device;
+    int slots;                   /* requests on the GPU at once (1..256), one stream each */
+    double hbm_budget_bytes;     /* device pool size */
+    int autotune;                /* 1: per-request implementation from the tuner (default) */
+    hj_tuner_t tuner;            /* used when tuner.partition_target > 0, else the context defaults */
+} hj_server_config_t;
+
+typedef struct {
+    uint64_t id;
+    uint64_t matched_cnt;
+    uint64_t checksum;
+    int status;                  /* HJ_OK or an HJ_E_* code */
+    int impl;                    /* 0 = non-partitioned table, 1 = radix-partitioned */
+    double submit_s, start_s, done_s; /* hj_now() clock: submission, admission, completion seen */
+} hj_server_completion_t;
+
+typedef struct {
+    uint64_t submitted, admitted, completed;
+    double budget_bytes, in_use_bytes, peak_in_use_bytes;
+    int queued, inflight;
+} hj_server_stats_t;
+
+typedef struct hj_server hj_server_t;
+
+/* Monotonic clock in seconds, the one completions are stamped with. */
+double hj_now(void);
+int hj_server_config_init(hj_server_config_t *cfg); /* device 0, 8 slots, 150e9 bytes, autotune */
+int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out);
+int hj_server_submit(hj_server_t *srv, hj_algo_t algo, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,
+                     size_t nS, int inputs_on_device, uint64_t *id);
+/* Up to max completions into out (*n of them); waits up to wait_ms for the first when none is ready. */
+int hj_server_poll(hj_server_t *srv, hj_server_completion_t *out, int max, int *n, int wait_ms);
+int hj_server_stats(hj_server_t *srv, hj_server_stats_t *out);
+/* Serves what is queued, waits for it, and frees everything; completions not polled are dropped. */
+int hj_server_destroy(hj_server_t *srv);
+
 #ifdef __cplusplus
 }
 #endif

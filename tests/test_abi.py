@@ -113,3 +113,21 @@ def test_join_without_gpu_reports_device_error(hj):
     R = np.array([[1, 1]], dtype=np.uint64)
     r = hj.join("phj_radix_bc", R, R, check=False)
     assert r.status == hj.HJ_E_DEVICE
+
+
+def test_server_without_gpu_reports_device_error(hj):
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(hj.JoinError) as e:
+        hj.Server(0, slots=2, hbm_budget_bytes=1e6)
+    assert e.value.status == hj.HJ_E_DEVICE
+
+
+def test_server_config_defaults(hj):
+    L = hj._bind_server()
+    cfg = hj.ServerConfig()
+    assert L.hj_server_config_init(cfg) == 0
+    assert (cfg.device, cfg.slots, cfg.hbm_budget_bytes, cfg.autotune) == (0, 8, 150e9, 1)
+    assert L.hj_server_config_init(None) == hj.HJ_E_INVAL
+    assert 0 < hj.now()
