@@ -529,10 +529,13 @@ def run_serve_mode(a, rank, world, local_rank):
             if d > 4e-4:
                 time.sleep(d - 3e-4)
 
-    def summarize(lat, t0, t_last, n):
-        lat = np.sort(np.asarray(lat))
+    def summarize(lat, picks, t0, t_last, n):
+        lat = np.asarray(lat)
+        small_lat = np.asarray([x for x, p in zip(lat, picks) if p is not big])
         return {"joins_per_s": n / (t_last - t0), "p50_ms": float(np.percentile(lat, 50) * 1e3),
-                "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat[-1] * 1e3)}
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3),
+                "small_p50_ms": float(np.percentile(small_lat, 50) * 1e3),
+                "small_p99_ms": float(np.percentile(small_lat, 99) * 1e3)}
 
     # 1. the join server
     srv_out, peak, budget = [], 0.0, 0.0
@@ -555,7 +558,7 @@ def run_serve_mode(a, rank, world, local_rank):
                 lat.append(c.done_s - (t0 + t))
                 t_last = max(t_last, c.done_s)
                 impl_counts[c.impl] += 1
-            srv_out.append(summarize(lat, t0, t_last, len(ids)))
+            srv_out.append(summarize(lat, picks, t0, t_last, len(ids)))
         st = srv.stats()
         peak, budget = st.peak_in_use_bytes, st.budget_bytes
 
@@ -584,7 +587,7 @@ def run_serve_mode(a, rank, world, local_rank):
                     raise RuntimeError("looped join result differs from the closed form")
                 lat.append(done - (t0 + t))
                 t_last = done
-            loop_out.append(summarize(lat, t0, t_last, len(picks)))
+            loop_out.append(summarize(lat, picks, t0, t_last, len(picks)))
 
     # sustained rate: the highest offered rate the server kept up with (completion rate >= 95% offered)
     best = 0

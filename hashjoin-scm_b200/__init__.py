@@ -424,7 +424,7 @@ class Batch:
 # ---------------------------------------------------------------------------------------------
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double),
-                ("autotune", ctypes.c_int), ("tuner", Tuner)]
+                ("autotune", ctypes.c_int), ("tuner", Tuner), ("small_request_tuples", ctypes.c_double)]
 
 
 class Completion(ctypes.Structure):

@@ -8,11 +8,15 @@
 //     while serving;
 //   - `slots` requests run at once, each on its own CUDA stream, so a request that arrives while others
 //     are on the GPU is admitted as soon as a slot and its memory are free and its kernels overlap with
-//     theirs;
+//     theirs; small requests run on high-priority streams, so their thread blocks are scheduled ahead of
+//     the waiting blocks of a large join and their latency stays near their own run time;
+//   - the dispatcher thread polls the slots' completion events without sleeping while any request is
+//     on the GPU (a sleep of a few microseconds costs tens of microseconds of timer slack per request);
 //   - admission is first come, first served, except that requests behind a head that does not fit yet
 //     may go first while the head has waited less than a bound;
 //   - each request runs the implementation the context's autotuner picks for its sizes (or the named
 //     one) with the named algorithm's result semantics, so its result is the same alone and in the mix.
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -96,7 +100,9 @@ class Pool {
 };
 
 struct Slot {
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // low priority: large requests
+    cudaStream_t stream_hi = nullptr;  // high priority: small requests
+    cudaStream_t cur = nullptr;        // the one the slot's request runs on
     cudaEvent_t done = nullptr;
     hj::JoinAccum *acc_host = nullptr;  // pinned
     bool busy = false;
@@ -118,6 +124,7 @@ struct hj_server {
     std::mutex mu;
     std::condition_variable cv_submit, cv_done;
     std::deque<Request> queue;
+    std::atomic<int> pending{0};  // queued requests, readable without the lock
     std::deque<hj_server_completion_t> done;
     uint64_t next_id = 1, n_submitted = 0, n_admitted = 0, n_completed = 0;
     bool stop = false;
@@ -153,7 +160,8 @@ int request_need(hj_server *s, Request &r) {
 // Enqueue one admitted request on a slot's stream; nothing here waits for the device.
 int launch(hj_server *s, Slot &sl) {
     Request &r = sl.req;
-    cudaStream_t st = sl.stream;
+    const bool small = (double)(r.nR + r.nS) <= s->cfg.small_request_tuples;
+    cudaStream_t st = sl.cur = small ? sl.stream_hi : sl.stream;
     char *base = s->pool_mem + r.off;
     hj::JoinAccum *acc = reinterpret_cast<hj::JoinAccum *>(base);
     char *cur = base + 256;
@@ -253,6 +261,7 @@ void worker_main(hj_server *s) {
                     free_slot->busy = true;
                     to_launch.push_back(free_slot);
                     it = s->queue.erase(it);
+                    s->pending.fetch_sub(1, std::memory_order_release);
                     s->n_admitted++;
                     continue;
                 }
@@ -265,18 +274,26 @@ void worker_main(hj_server *s) {
                 bool any_busy = false;
                 for (Slot &sl : s->slots) any_busy = any_busy || sl.busy;
                 if (s->stop && s->queue.empty() && !any_busy) return;
-                if (!any_busy)
-                    s->cv_submit.wait_for(lk, std::chrono::milliseconds(2));
+                if (!any_busy && s->queue.empty()) {
+                    // Idle: spin briefly for the next submission, then block until one arrives.
+                    lk.unlock();
+                    const double t_spin = now_s() + 2e-4;
+                    while (now_s() < t_spin && s->pending.load(std::memory_order_acquire) == 0)
+                        std::this_thread::yield();
+                    lk.lock();
+                    if (s->queue.empty() && !s->stop)
+                        s->cv_submit.wait_for(lk, std::chrono::milliseconds(2));
+                }
             }
         }
         for (Slot *sl : to_launch) {
             const int rc = launch(s, *sl);
             if (rc) {
-                cudaStreamSynchronize(sl->stream);
+                cudaStreamSynchronize(sl->cur);
                 complete(s, *sl, rc, nullptr);
             }
         }
-        if (to_launch.empty() && !progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        if (to_launch.empty() && !progressed) std::this_thread::yield();
     }
 }
 
@@ -293,6 +310,7 @@ int hj_server_config_init(hj_server_config_t *c) {
     c->slots = 8;
     c->hbm_budget_bytes = 150e9;
     c->autotune = 1;
+    c->small_request_tuples = (double)(1u << 25);
     return HJ_OK;
 }
 
@@ -325,9 +343,12 @@ int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out) {
     s->pool_bytes = want;
     s->pool.init(want);
     hj::phj_prepare_device();
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     s->slots.resize(cfg->slots);
     for (Slot &sl : s->slots) {
-        if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        if (cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&sl.stream_hi, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
             cudaMallocHost(&sl.acc_host, sizeof(hj::JoinAccum)) != cudaSuccess) {
             if (prev >= 0) cudaSetDevice(prev);
@@ -360,6 +381,7 @@ int hj_server_submit(hj_server_t *s, hj_algo_t algo, const hj_tuple_t *R, size_t
     std::lock_guard<std::mutex> lk(s->mu);
     r.id = s->next_id++;
     s->queue.push_back(r);
+    s->pending.fetch_add(1, std::memory_order_release);
     s->n_submitted++;
     if (id) *id = r.id;
     s->cv_submit.notify_all();
@@ -408,9 +430,11 @@ int hj_server_destroy(hj_server_t *s) {
     cudaSetDevice(s->cfg.device);
     for (Slot &sl : s->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
+        if (sl.stream_hi) cudaStreamSynchronize(sl.stream_hi);
         if (sl.done) cudaEventDestroy(sl.done);
         if (sl.acc_host) cudaFreeHost(sl.acc_host);
         if (sl.stream) cudaStreamDestroy(sl.stream);
+        if (sl.stream_hi) cudaStreamDestroy(sl.stream_hi);
     }
     if (s->pool_mem) cudaFree(s->pool_mem);
     if (s->ctx) hj_ctx_destroy(s->ctx);
