@@ -537,7 +537,11 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
     return s;
 }
 
-template <int THREADS, int ITEMS>
+// STABLE: tuples of equal digit keep their input order (needed for the build side of joins that report
+// the first match in input order). Otherwise the rank of a tuple within its digit is taken with one
+// shared-memory atomic, in whatever order the warps reach it: the partitions hold the same tuples,
+// and the joins that count every match do not depend on their order.
+template <int THREADS, int ITEMS, bool STABLE>
 __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
     constexpr int T = THREADS * ITEMS;
     constexpr int NW = THREADS / 32;
@@ -546,7 +550,8 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
     long long *gbase = reinterpret_cast<long long *>(inbuf + 2 * T);     // [256]
     long long *running = gbase + 256;                                   // [256]
     uint32_t *tdstart = reinterpret_cast<uint32_t *>(running + 256);    // [256]
-    uint16_t *whist = reinterpret_cast<uint16_t *>(tdstart + 256);      // [NW][F]
+    uint16_t *whist = reinterpret_cast<uint16_t *>(tdstart + 256);      // STABLE: [NW][F]
+    uint32_t *thist = reinterpret_cast<uint32_t *>(tdstart + 256);      // !STABLE: [F] tile histogram
     __shared__ __align__(8) unsigned long long bars[2];
     __shared__ uint32_t scan_tmp[32];
     __shared__ TileSlot slots[2];
@@ -562,6 +567,8 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
     const int nbins = 1 << a.bits;
     ItemIter it;  // used by thread 0 only
 
+    if (!STABLE)
+        for (int j = tid; j < 256; j += THREADS) thist[j] = 0;
     if (tid == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
@@ -619,55 +626,70 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
                 d[i] = (uint32_t)F;
             }
         }
-        uint16_t *wh = whist + w * F;
-        for (int j = lane; j < F; j += 32) wh[j] = 0;
-        __syncwarp();
-        // Stable rank within the warp: items in order, lanes in order. The lanes holding the same
-        // digit are found with one ballot per digit bit (plus the bit that marks padding lanes of a
-        // partial tile), which is cheaper here than match.any.
-        const int nbits = a.logF + (cnt < (uint32_t)T ? 1 : 0);
         uint32_t rk[ITEMS];
+        if constexpr (STABLE) {
+            uint16_t *wh = whist + w * F;
+            for (int j = lane; j < F; j += 32) wh[j] = 0;
+            __syncwarp();
+            // Stable rank within the warp: items in order, lanes in order. The lanes holding the same
+            // digit are found with one ballot per digit bit (plus the bit that marks padding lanes of
+            // a partial tile), which is cheaper here than match.any.
+            const int nbits = a.logF + (cnt < (uint32_t)T ? 1 : 0);
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            unsigned peers = 0xffffffffu;
+            for (int i = 0; i < ITEMS; i++) {
+                unsigned peers = 0xffffffffu;
 #pragma unroll
-            for (int b = 0; b < 9; b++) {
-                if (b < nbits) {
-                    const unsigned bit = (d[i] >> b) & 1u;
-                    const unsigned bal = __ballot_sync(0xffffffffu, bit);
-                    peers &= bit ? bal : ~bal;
+                for (int b = 0; b < 9; b++) {
+                    if (b < nbits) {
+                        const unsigned bit = (d[i] >> b) & 1u;
+                        const unsigned bal = __ballot_sync(0xffffffffu, bit);
+                        peers &= bit ? bal : ~bal;
+                    }
+                }
+                const bool valid = d[i] < (uint32_t)F;
+                uint32_t pre = 0;
+                if (valid) pre = wh[d[i]];
+                rk[i] = pre + __popc(peers & ltmask);
+                __syncwarp();
+                if (valid && (peers & ltmask) == 0) wh[d[i]] = (uint16_t)(pre + __popc(peers));
+                __syncwarp();
+            }
+            __syncthreads();
+            // Tile histogram per digit and exclusive prefix over warps.
+            uint32_t h = 0;
+            if (tid < F) {
+                for (int q = 0; q < NW; q++) {
+                    const uint32_t c = whist[q * F + tid];
+                    whist[q * F + tid] = (uint16_t)h;
+                    h += c;
                 }
             }
-            const bool valid = d[i] < (uint32_t)F;
-            uint32_t pre = 0;
-            if (valid) pre = wh[d[i]];
-            rk[i] = pre + __popc(peers & ltmask);
-            __syncwarp();
-            if (valid && (peers & ltmask) == 0) wh[d[i]] = (uint16_t)(pre + __popc(peers));
-            __syncwarp();
-        }
-        __syncthreads();
-        // Tile histogram per digit and exclusive prefix over warps.
-        uint32_t h = 0;
-        if (tid < F) {
-            for (int q = 0; q < NW; q++) {
-                const uint32_t c = whist[q * F + tid];
-                whist[q * F + tid] = (uint16_t)h;
-                h += c;
+            const uint32_t ex = block_excl_scan_u32(tid < F ? h : 0u, scan_tmp, nullptr);
+            if (tid < F) {
+                tdstart[tid] = ex;
+                gbase[tid] = running[tid] - (long long)ex;
+                running[tid] += h;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++)
+                if (d[i] < (uint32_t)F) rk[i] = atomicAdd(&thist[d[i]], 1u);
+            __syncthreads();
+            const uint32_t h = tid < F ? thist[tid] : 0u;
+            const uint32_t ex = block_excl_scan_u32(h, scan_tmp, nullptr);
+            if (tid < F) {
+                thist[tid] = 0;
+                tdstart[tid] = ex;
+                gbase[tid] = running[tid] - (long long)ex;
+                running[tid] += h;
             }
         }
-        const uint32_t ex = block_excl_scan_u32(tid < F ? h : 0u, scan_tmp, nullptr);
-        if (tid < F) {
-            tdstart[tid] = ex;
-            gbase[tid] = running[tid] - (long long)ex;
-            running[tid] += h;
-        }
         __syncthreads();
-        // Stage the tile sorted by digit (stable), in place.
+        // Stage the tile sorted by digit, in place.
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             if (d[i] < (uint32_t)F) {
-                const uint32_t pos = tdstart[d[i]] + wh[d[i]] + rk[i];
+                const uint32_t pos = tdstart[d[i]] + (STABLE ? whist[w * F + d[i]] : 0u) + rk[i];
                 buf[pos] = v[i];
             }
         }
@@ -1150,7 +1172,9 @@ int phj_prepare_device() {
     if (g_attr_done[cur_dev]) return HJ_OK;
     const size_t scatter_smem = (size_t)2 * kTile * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
     HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
-    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems>,
+    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
+    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_compact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1242,7 +1266,10 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.unit_cnt = s.unit_cnt;
         sa.counters = s.counters;
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
-        scatter_kernel<kScatterThreads, kScatterItems><<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+        if (lp)
+            scatter_kernel<kScatterThreads, kScatterItems, true><<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+        else
+            scatter_kernel<kScatterThreads, kScatterItems, false><<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
         HJ_CU(cudaGetLastError());
         nlaunch++;
         HJ_PH(3 + pass);
