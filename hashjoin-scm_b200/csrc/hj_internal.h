@@ -35,12 +35,16 @@ constexpr int kProbeChunk = 1 << 16;   // S tuples per join work item
 struct PhjScratch {
     uint64_t chunk;          // tuples per input chunk
     uint32_t cR, cS;         // chunks of R and of S
+    uint64_t sub;            // tuples per sub-chunk (pass-1 work item)
+    uint32_t spc;            // sub-chunks per chunk
     uint32_t *chunk_hist;    // [chunk][2^B] joint digit histogram of each chunk
     uint32_t *prefix;        // [chunk][2^B] exclusive prefix over the chunks of the same relation
     uint32_t *total;         // [2][2^B]
     uint64_t *start;         // [2][2^B + 1] final partition starts
     uint64_t *unit_off;      // [chunk][F1] start of (chunk, d1) in the pass-1 output
     uint32_t *unit_cnt;      // [chunk][F1] its size
+    uint32_t *subhist;       // [chunk][spc][F1] pass-1 digit histogram of each sub-chunk, then its start
+                             // within (chunk, d1)
     uint32_t *counters;      // work-item counters, totals, error word (memset per join)
     void *items;             // join work items
     size_t max_items;

@@ -83,6 +83,9 @@ constexpr int kCompactThreads = 512;
 struct ChunkGeom {
     uint64_t chunk;  // tuples per chunk (a multiple of the tile)
     uint32_t cR, cS; // chunks of R, chunks of S (R's come first)
+    uint64_t sub;    // tuples per sub-chunk (a multiple of the tile): the pass-1 work item
+    uint32_t spc;    // sub-chunks per chunk
+    uint32_t pad;
 };
 
 __device__ __forceinline__ uint64_t ld_u64_pair(const uint32_t *p) {
@@ -141,66 +144,94 @@ __device__ __forceinline__ void tma_load_1d(void *dst_smem, const void *src, uin
     }
 }
 
+// Count the tuples [lo, hi) of `in`, read by one warp (four 512-byte loads in flight), into the joint
+// histogram and into the warp's histogram of the pass-1 digit. BUILD: also OR together all keys and row
+// ids; their widths decide whether the compact join table applies (a value fits 32 bits iff the OR of
+// all values does).
+template <bool BUILD>
+__device__ __forceinline__ void hist_range_warp(const tuple_v *__restrict__ in, uint64_t lo, uint64_t hi,
+                                                uint32_t *sh_hist, uint32_t *wsub, uint64_t mask, uint32_t m1,
+                                                unsigned long long &kor, unsigned long long &ror) {
+    uint64_t i = lo + (threadIdx.x & 31u);
+    for (; i + 96 < hi; i += 128) {
+        const tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + 32);
+        const tuple_v t2 = ld_stream(in + i + 64), t3 = ld_stream(in + i + 96);
+        atomicAdd(&sh_hist[t0.x & mask], 1u);
+        atomicAdd(&sh_hist[t1.x & mask], 1u);
+        atomicAdd(&sh_hist[t2.x & mask], 1u);
+        atomicAdd(&sh_hist[t3.x & mask], 1u);
+        atomicAdd(&wsub[(uint32_t)t0.x & m1], 1u);
+        atomicAdd(&wsub[(uint32_t)t1.x & m1], 1u);
+        atomicAdd(&wsub[(uint32_t)t2.x & m1], 1u);
+        atomicAdd(&wsub[(uint32_t)t3.x & m1], 1u);
+        if (BUILD) {
+            kor |= t0.x | t1.x | t2.x | t3.x;
+            ror |= t0.y | t1.y | t2.y | t3.y;
+        }
+    }
+    for (; i < hi; i += 32) {
+        const tuple_v t = ld_stream(in + i);
+        atomicAdd(&sh_hist[t.x & mask], 1u);
+        atomicAdd(&wsub[(uint32_t)t.x & m1], 1u);
+        if (BUILD) {
+            kor |= t.x;
+            ror |= t.y;
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
-// 1. Per-chunk joint histogram of the low `bits` key bits. One CTA per chunk; every bin is written.
+// 1. Per-chunk joint histogram of the low `bits` key bits, and per sub-chunk the histogram of the
+//    pass-1 digit (the low log2(F1) bits). One CTA per chunk; each warp takes whole sub-chunks, so a
+//    sub-chunk's digit histogram is complete after a warp barrier and no CTA barrier interrupts the
+//    stream of loads. Every bin is written.
 // ------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) hist_chunk_kernel(const tuple_v *__restrict__ R, size_t nR,
                                                          const tuple_v *__restrict__ S, size_t nS, int bits,
-                                                         ChunkGeom cg, uint32_t *__restrict__ chunk_hist,
+                                                         int F1, ChunkGeom cg, uint32_t *__restrict__ chunk_hist,
+                                                         uint32_t *__restrict__ subhist,
                                                          uint32_t *__restrict__ maxima) {
     extern __shared__ uint32_t sh_hist[];
     const int nbins = 1 << bits;
+    const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+    uint32_t *wsub = sh_hist + nbins + (size_t)w * F1;  // [warps][F1] per-warp pass-1 digit histogram
     const uint64_t mask = (uint64_t)nbins - 1;
+    const uint32_t m1 = (uint32_t)F1 - 1u;
     const uint32_t c = blockIdx.x;
     const int rel = c < cg.cR ? 0 : 1;
     const uint64_t lc = rel ? c - cg.cR : c;
     const tuple_v *in = rel ? S : R;
     const uint64_t n = rel ? nS : nR;
-    for (int v = threadIdx.x; v < nbins; v += blockDim.x) sh_hist[v] = 0;
+    for (int v = threadIdx.x; v < nbins + (int)nw * F1; v += blockDim.x) sh_hist[v] = 0;
     __syncthreads();
-    const uint64_t lo = lc * cg.chunk;
-    const uint64_t hi = lo + cg.chunk < n ? lo + cg.chunk : n;
-    const uint64_t step = blockDim.x;
-    uint64_t i = lo + threadIdx.x;
+    const uint64_t clo = lc * cg.chunk;
+    const uint64_t chi = clo + cg.chunk < n ? clo + cg.chunk : n;
+    unsigned long long kor = 0, ror = 0;
+    for (uint32_t j = w; j < cg.spc; j += nw) {
+        const uint64_t lo = clo + (uint64_t)j * cg.sub < chi ? clo + (uint64_t)j * cg.sub : chi;
+        const uint64_t hi = lo + cg.sub < chi ? lo + cg.sub : chi;
+        if (rel == 0)
+            hist_range_warp<true>(in, lo, hi, sh_hist, wsub, mask, m1, kor, ror);
+        else
+            hist_range_warp<false>(in, lo, hi, sh_hist, wsub, mask, m1, kor, ror);
+        __syncwarp();
+        uint32_t *so = subhist + ((size_t)c * cg.spc + j) * F1;
+        for (int v = lane; v < F1; v += 32) {
+            so[v] = wsub[v];
+            wsub[v] = 0;
+        }
+        __syncwarp();
+    }
     if (rel == 0) {
-        // Build side: also OR together all keys and row ids; their widths decide whether the compact
-        // join table applies (a value fits 32 bits iff the OR of all values does).
-        unsigned long long kor = 0, ror = 0;
-        for (; i + 3 * step < hi; i += 4 * step) {
-            const tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + step);
-            const tuple_v t2 = ld_stream(in + i + 2 * step), t3 = ld_stream(in + i + 3 * step);
-            atomicAdd(&sh_hist[t0.x & mask], 1u);
-            atomicAdd(&sh_hist[t1.x & mask], 1u);
-            atomicAdd(&sh_hist[t2.x & mask], 1u);
-            atomicAdd(&sh_hist[t3.x & mask], 1u);
-            kor |= t0.x | t1.x | t2.x | t3.x;
-            ror |= t0.y | t1.y | t2.y | t3.y;
-        }
-        for (; i < hi; i += step) {
-            const tuple_v t = ld_stream(in + i);
-            atomicAdd(&sh_hist[t.x & mask], 1u);
-            kor |= t.x;
-            ror |= t.y;
-        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             kor |= __shfl_xor_sync(0xffffffffu, kor, o);
             ror |= __shfl_xor_sync(0xffffffffu, ror, o);
         }
-        if ((threadIdx.x & 31) == 0) {
+        if (lane == 0) {
             atomicOr(reinterpret_cast<unsigned long long *>(maxima), kor);
             atomicOr(reinterpret_cast<unsigned long long *>(maxima) + 1, ror);
         }
-    } else {
-        for (; i + 3 * step < hi; i += 4 * step) {
-            const tuple_v t0 = ld_stream(in + i), t1 = ld_stream(in + i + step);
-            const tuple_v t2 = ld_stream(in + i + 2 * step), t3 = ld_stream(in + i + 3 * step);
-            atomicAdd(&sh_hist[t0.x & mask], 1u);
-            atomicAdd(&sh_hist[t1.x & mask], 1u);
-            atomicAdd(&sh_hist[t2.x & mask], 1u);
-            atomicAdd(&sh_hist[t3.x & mask], 1u);
-        }
-        for (; i < hi; i += step) atomicAdd(&sh_hist[ld_stream(in + i).x & mask], 1u);
     }
     __syncthreads();
     uint32_t *out = chunk_hist + (size_t)c * nbins;
@@ -401,11 +432,12 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
 // ------------------------------------------------------------------------------------------------
 // 4. Units: for every chunk c and pass-1 digit d1, the number of the chunk's tuples with that digit
 //    and where they start in the pass-1 output: start[d1 * F2] + sum over d2 of prefix[c][(d1, d2)].
-//    One warp per (c, d1).
+//    The sub-chunk histograms of the chunk become, in place, each sub-chunk's start within (c, d1).
 // ------------------------------------------------------------------------------------------------
 __global__ void units_kernel(const uint32_t *__restrict__ chunk_hist, const uint32_t *__restrict__ prefix,
                              const uint64_t *__restrict__ start, int bits, int b1, int F1, int F2,
-                             ChunkGeom cg, uint64_t *__restrict__ unit_off, uint32_t *__restrict__ unit_cnt) {
+                             ChunkGeom cg, uint64_t *__restrict__ unit_off, uint32_t *__restrict__ unit_cnt,
+                             uint32_t *__restrict__ subhist, uint32_t *__restrict__ err) {
     // One CTA per chunk, one thread per pass-1 digit; for a fixed pass-2 digit the threads read
     // consecutive bins.
     const uint32_t c = blockIdx.x;
@@ -439,6 +471,25 @@ __global__ void units_kernel(const uint32_t *__restrict__ chunk_hist, const uint
     const uint32_t wid = c * (uint32_t)F1 + d1;
     unit_cnt[wid] = (uint32_t)cnt;
     unit_off[wid] = start[(size_t)rel * (nbins + 1) + (size_t)d1 * F2] + pre;
+    uint32_t *sh = subhist + (size_t)c * cg.spc * F1 + d1;
+    uint32_t run = 0;
+    uint32_t j = 0;
+    for (; j + 8 <= cg.spc; j += 8) {
+        uint32_t x[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) x[u] = sh[(size_t)(j + u) * F1];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            sh[(size_t)(j + u) * F1] = run;
+            run += x[u];
+        }
+    }
+    for (; j < cg.spc; j++) {
+        const uint32_t x = sh[(size_t)j * F1];
+        sh[(size_t)j * F1] = run;
+        run += x;
+    }
+    if (run != (uint32_t)cnt) set_error(err, kErrCapacity);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -457,6 +508,7 @@ struct ScatterArgs {
     const uint64_t *start;      // [2][2^B + 1]
     const uint64_t *unit_off;   // [chunk][F1]
     const uint32_t *unit_cnt;   // [chunk][F1]
+    const uint32_t *subpre;     // [chunk][spc][F1] start of (sub-chunk, d1) within (chunk, d1)
     uint32_t *counters;
     int ctr_item;
 };
@@ -485,12 +537,15 @@ __device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item,
     it.item = item;
     it.done = 0;
     if (a.pass == 0) {
-        const uint32_t c = item;
+        // Pass 1 work item: sub-chunk j of chunk c.
+        const uint32_t c = item / cg.spc, j = item % cg.spc;
         const int rel = c < cg.cR ? 0 : 1;
         const uint64_t lc = rel ? c - cg.cR : c;
         const uint64_t n = rel ? a.nS : a.nR;
-        const uint64_t lo = lc * cg.chunk;
-        it.len = lo < n ? (n - lo < cg.chunk ? n - lo : cg.chunk) : 0;
+        const uint64_t clo = lc * cg.chunk;
+        const uint64_t chi = clo + cg.chunk < n ? clo + cg.chunk : n;
+        const uint64_t lo = clo + (uint64_t)j * cg.sub;
+        it.len = lo < chi ? (chi - lo < cg.sub ? chi - lo : cg.sub) : 0;
         it.in = (rel ? a.inS : a.inR) + lo;
         it.out = rel ? a.outS : a.outR;
         it.out_len = n;
@@ -560,16 +615,17 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
     const int F = a.F;
     const uint64_t dmask = (uint64_t)F - 1;
     const uint32_t nchunks = a.cg.cR + a.cg.cS;
-    const uint32_t nitems = a.pass == 0 ? nchunks : nchunks * (uint32_t)a.F1;
+    const uint32_t nitems = a.pass == 0 ? nchunks * a.cg.spc : nchunks * (uint32_t)a.F1;
     unsigned int *err = &a.counters[kCtrErr];
     const unsigned ltmask = lanemask_lt();
     const uint32_t bar0 = smem_addr(&bars[0]);
     const int nbins = 1 << a.bits;
-    ItemIter it;  // used by thread 0 only
+    __shared__ ItemIter it;  // used by thread 0 only
 
     if (!STABLE)
         for (int j = tid; j < 256; j += THREADS) thist[j] = 0;
     if (tid == 0) {
+        it = ItemIter();
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -584,8 +640,8 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
         const TileSlot sl = slots[cur];
         if (sl.item == ~0u) break;
         tuple_v *buf = inbuf + (size_t)cur * T;
-        // Prefetch the next tile into the other buffer; its previous contents were consumed before
-        // the barrier that ended the previous iteration.
+        // Prefetch the next tile into the other buffer; the barrier that ended the previous iteration
+        // ordered every read of it before this copy.
         if (tid == 0) {
             const TileSlot sn = next_tile<T>(a, it, nitems);
             slots[cur ^ 1u] = sn;
@@ -595,7 +651,8 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
         if (sl.first && tid < F) {
             long long off;
             if (a.pass == 0) {
-                off = (long long)a.unit_off[(size_t)sl.item * a.F1 + tid];
+                const uint32_t c = sl.item / a.cg.spc;
+                off = (long long)(a.unit_off[(size_t)c * a.F1 + tid] + a.subpre[(size_t)sl.item * a.F1 + tid]);
             } else {
                 const uint32_t c = sl.item / a.F1, d1 = sl.item % a.F1;
                 const int rel = c < a.cg.cR ? 0 : 1;
@@ -675,41 +732,70 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
             for (int i = 0; i < ITEMS; i++)
                 if (d[i] < (uint32_t)F) rk[i] = atomicAdd(&thist[d[i]], 1u);
             __syncthreads();
-            const uint32_t h = tid < F ? thist[tid] : 0u;
-            const uint32_t ex = block_excl_scan_u32(h, scan_tmp, nullptr);
-            if (tid < F) {
-                thist[tid] = 0;
-                tdstart[tid] = ex;
-                gbase[tid] = running[tid] - (long long)ex;
-                running[tid] += h;
+            // Warp 0 scans the tile histogram: lane l owns digits [l*K, l*K + K).
+            if (w == 0) {
+                const int K = (F + 31) >> 5;
+                const int d0 = lane * K;
+                uint32_t hv[8];
+                uint32_t sum = 0;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    hv[j] = (j < K && d0 + j < F) ? thist[d0 + j] : 0u;
+                    sum += hv[j];
+                }
+                uint32_t incl = sum;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                uint32_t ex = incl - sum;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    if (j < K && d0 + j < F) {
+                        const int dd = d0 + j;
+                        thist[dd] = 0;
+                        tdstart[dd] = ex;
+                        const long long r0 = running[dd];
+                        gbase[dd] = r0 - (long long)ex;
+                        running[dd] = r0 + hv[j];
+                        ex += hv[j];
+                    }
+                }
             }
         }
         __syncthreads();
-        // Stage the tile sorted by digit, in place.
+        // Stage the tile sorted by digit, in place (the digit is recomputed: fewer live registers).
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
-            if (d[i] < (uint32_t)F) {
-                const uint32_t pos = tdstart[d[i]] + (STABLE ? whist[w * F + d[i]] : 0u) + rk[i];
+            const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
+            if (idx < cnt) {
+                const uint32_t di = (uint32_t)((v[i].x >> a.shift) & dmask);
+                const uint32_t pos = tdstart[di] + (STABLE ? whist[w * F + di] : 0u) + rk[i];
                 buf[pos] = v[i];
             }
         }
         __syncthreads();
         // Write each digit run: consecutive threads write consecutive 16-byte tuples. Full tiles load
-        // all their staged tuples first so that the stores issue back to back.
+        // their staged tuples in two halves so that the stores issue back to back.
         if (cnt == (uint32_t)T) {
-            tuple_v t[ITEMS];
-            long long dst[ITEMS];
 #pragma unroll
-            for (int i = 0; i < ITEMS; i++) t[i] = buf[tid + i * THREADS];
+            for (int hh = 0; hh < 2; hh++) {
+                tuple_v t[ITEMS / 2];
+                long long dst[ITEMS / 2];
 #pragma unroll
-            for (int i = 0; i < ITEMS; i++)
-                dst[i] = gbase[(uint32_t)((t[i].x >> a.shift) & dmask)] + (long long)(tid + i * THREADS);
+                for (int i = 0; i < ITEMS / 2; i++) t[i] = buf[tid + (hh * ITEMS / 2 + i) * THREADS];
 #pragma unroll
-            for (int i = 0; i < ITEMS; i++) {
-                if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len)
-                    st_stream(sl.out + dst[i], t[i]);
-                else
-                    set_error(err, kErrBounds);
+                for (int i = 0; i < ITEMS / 2; i++)
+                    dst[i] = gbase[(uint32_t)((t[i].x >> a.shift) & dmask)] +
+                             (long long)(tid + (hh * ITEMS / 2 + i) * THREADS);
+#pragma unroll
+                for (int i = 0; i < ITEMS / 2; i++) {
+                    if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len)
+                        st_stream(sl.out + dst[i], t[i]);
+                    else
+                        set_error(err, kErrBounds);
+                }
             }
         } else
         for (uint32_t j = tid; j < cnt; j += THREADS) {
@@ -1075,21 +1161,31 @@ int radix_geom(int bits, int passes, RadixGeom *g) {
 
 static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Pass-1 work items: about kSubPerChunk sub-chunks per chunk (two per warp of the histogram kernel).
+constexpr int kSubPerChunk = 32;
+
 static ChunkGeom chunk_geom(size_t nR, size_t nS, int num_sms) {
     // About three chunks per SM (the scatter kernel's residency), each a whole number of tiles.
     const uint64_t tiles = (uint64_t)ceil_div_u64(nR, kTile) + ceil_div_u64(nS, kTile);
     const uint64_t target = (uint64_t)(num_sms > 0 ? num_sms : 148) * 3;
     uint64_t ct = (tiles + target - 1) / target;
     if (ct < 1) ct = 1;
+    // Pass 1 takes sub-chunks as work items, so that CTAs that run ahead take more of them instead of
+    // idling while the slowest chunk finishes.
+    const uint64_t st = (ct + kSubPerChunk - 1) / kSubPerChunk;
     ChunkGeom cg;
     cg.chunk = ct * kTile;
     cg.cR = ceil_div_u64(nR, cg.chunk);
     cg.cS = ceil_div_u64(nS, cg.chunk);
+    cg.sub = st * kTile;
+    cg.spc = (uint32_t)((ct + st - 1) / st);
+    cg.pad = 0;
     return cg;
 }
 
 struct PhjSizes {
-    size_t chunk_hist, prefix, total, start, units_off, units_cnt, counters, items, large, large_table, tmp1, tmp2;
+    size_t chunk_hist, prefix, total, start, units_off, units_cnt, subhist, counters, items, large, large_table,
+        tmp1, tmp2;
     size_t max_items, max_large, large_table_words;
     ChunkGeom cg;
 };
@@ -1105,6 +1201,7 @@ static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms)
     z.start = align_up(2 * (np + 1) * 8, 256);
     z.units_off = align_up(nchunks * (size_t)g.F1 * 8, 256);
     z.units_cnt = align_up(nchunks * (size_t)g.F1 * 4, 256);
+    z.subhist = align_up(nchunks * (size_t)z.cg.spc * g.F1 * 4, 256);
     z.counters = 256;
     z.max_items = np + nS / kProbeChunk + 2;
     z.items = align_up(z.max_items * sizeof(JoinItem), 256);
@@ -1121,7 +1218,7 @@ static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms)
 
 size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms) {
     PhjSizes z = phj_sizes(g, nR, nS, num_sms);
-    return z.chunk_hist + z.prefix + z.total + z.start + z.units_off + z.units_cnt + z.counters + z.items +
+    return z.chunk_hist + z.prefix + z.total + z.start + z.units_off + z.units_cnt + z.subhist + z.counters + z.items +
            z.large + z.large_table + z.tmp1 + z.tmp2;
 }
 
@@ -1131,12 +1228,15 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
     s->chunk = z.cg.chunk;
     s->cR = z.cg.cR;
     s->cS = z.cg.cS;
+    s->sub = z.cg.sub;
+    s->spc = z.cg.spc;
     s->chunk_hist = reinterpret_cast<uint32_t *>(p); p += z.chunk_hist;
     s->prefix = reinterpret_cast<uint32_t *>(p); p += z.prefix;
     s->total = reinterpret_cast<uint32_t *>(p); p += z.total;
     s->start = reinterpret_cast<uint64_t *>(p); p += z.start;
     s->unit_off = reinterpret_cast<uint64_t *>(p); p += z.units_off;
     s->unit_cnt = reinterpret_cast<uint32_t *>(p); p += z.units_cnt;
+    s->subhist = reinterpret_cast<uint32_t *>(p); p += z.subhist;
     s->counters = reinterpret_cast<uint32_t *>(p); p += z.counters;
     s->items = p; p += z.items;
     s->max_items = z.max_items;
@@ -1171,7 +1271,7 @@ int phj_prepare_device() {
     if (cur_dev < 0 || cur_dev >= 64) return HJ_E_INVAL;
     if (g_attr_done[cur_dev]) return HJ_OK;
     const size_t scatter_smem = (size_t)2 * kTile * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
-    HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
+    HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 136 * 1024));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, true>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false>,
@@ -1194,11 +1294,14 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     const int F1 = g.F1, F2 = g.F2;
     constexpr int T = kTile;
     const size_t scatter_smem = (size_t)2 * T * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
-    const size_t hist_smem = (size_t)np * 4;
+    const size_t hist_smem = (size_t)np * 4 + (size_t)16 * F1 * 4;  // 16 warps
     ChunkGeom cg;
     cg.chunk = s.chunk;
     cg.cR = s.cR;
     cg.cS = s.cS;
+    cg.sub = s.sub;
+    cg.spc = s.spc;
+    cg.pad = 0;
     const uint32_t nchunks = cg.cR + cg.cS;
     {
         const int rc = phj_prepare_device();
@@ -1208,7 +1311,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
 
     // 1. per-chunk histograms
     HJ_PH(0);
-    hist_chunk_kernel<<<nchunks, 512, hist_smem, st>>>(R, nR, S, nS, g.bits, cg, s.chunk_hist,
+    hist_chunk_kernel<<<nchunks, 512, hist_smem, st>>>(R, nR, S, nS, g.bits, F1, cg, s.chunk_hist, s.subhist,
                                                        s.counters + kCtrMaxKey);
     HJ_CU(cudaGetLastError());
     HJ_PH(1);
@@ -1234,7 +1337,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     {
         const int ut = F1 < 32 ? 32 : F1;
         units_kernel<<<nchunks, ut, 0, st>>>(s.chunk_hist, s.prefix, s.start, g.bits, g.b1, F1, g.passes == 2 ? F2 : 1,
-                                             cg, s.unit_off, s.unit_cnt);
+                                             cg, s.unit_off, s.unit_cnt, s.subhist, s.counters + kCtrErr);
     }
     HJ_CU(cudaGetLastError());
     nlaunch += 4;
@@ -1264,6 +1367,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.start = s.start;
         sa.unit_off = s.unit_off;
         sa.unit_cnt = s.unit_cnt;
+        sa.subpre = s.subhist;
         sa.counters = s.counters;
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
         if (lp)

@@ -216,3 +216,20 @@ def test_mixed_partition_sizes(hj, oracle, cuda, algo, wide_fields):
     S[::9, 0] += np.uint64(4)  # misses in the same partition
     got = run(hj, algo, R, S, cuda, bits=2, passes=1)
     assert got == oracle.join(algo, R, S)
+
+
+@pytest.mark.parametrize("algo", ["phj_radix_bc", "phj_radix_lp"])
+def test_many_subchunks_with_duplicates(hj, oracle, cuda, algo):
+    # 2^22 + 2^24 tuples make chunks of 24 tiles, i.e. two pass-1 work items per chunk (16 tiles and a
+    # partial 8), plus a ragged last chunk; duplicate build keys make the lp result depend on order.
+    rng = np.random.default_rng(31)
+    nR, nS = (1 << 22) + 777, (1 << 24) - 1234
+    R = np.empty((nR, 2), dtype=np.uint64)
+    S = np.empty((nS, 2), dtype=np.uint64)
+    R[:, 0] = rng.integers(0, 1 << 20, nR, dtype=np.uint64)
+    R[:, 1] = rng.integers(0, 2**48, nR, dtype=np.uint64)
+    S[:, 0] = rng.integers(0, (1 << 20) + 4096, nS, dtype=np.uint64)
+    S[:, 1] = rng.integers(0, 2**48, nS, dtype=np.uint64)
+    want = oracle.join(algo, R, S)
+    assert run(hj, algo, R, S, cuda) == want
+    assert run(hj, algo, R, S, cuda, bits=11, passes=2) == want
