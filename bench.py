@@ -150,6 +150,29 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def reduce_over_ranks(value: float, dist, device, op: str = "max") -> float:
+    """The max (or min) of a per-rank number over all ranks; the number itself without a process group.
+    Every rank must call it at the same point (it is a collective)."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.MIN)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world: int, seconds: float) -> float:
+    """Weak scaling: every rank processed units_per_rank; seconds is the slowest rank's time."""
+    return world * units_per_rank / seconds
+
+
+def emit(rank: int, line: dict) -> None:
+    """Rank 0 prints the one JSON line of the run."""
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -288,12 +311,8 @@ def run_ours(a, rank, world, local_rank):
     clocks = sampler.stop()
     if dist:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * (nR + nS) * a.steps / (ms / 1e3)
+    ms = reduce_over_ranks(e0.elapsed_time(e1), dist, dev)
+    value = whole_job_rate((nR + nS) * a.steps, world, ms / 1e3)
     phases = {name: statistics.mean(r.phase[i] for r in results) for i, name in enumerate(hj.PHASES)}
     launches = sum(r.kernel_launches for r in results)
 
@@ -338,12 +357,8 @@ def run_ours(a, rank, world, local_rank):
         t0 = time.perf_counter()
         for _ in range(a.e2e_steps):
             e2e_step()
-        el = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([el], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": world * (nR + nS) * a.e2e_steps / el, "unit": UNIT,
+        el = reduce_over_ranks(time.perf_counter() - t0, dist, dev)
+        e2e = {"value": whole_job_rate((nR + nS) * a.e2e_steps, world, el), "unit": UNIT,
                "h2d_bytes_per_step": (nR + nS) * 16, "d2h_bytes_per_step": 64,
                "steps": a.e2e_steps, "ms_per_step": el / a.e2e_steps * 1e3}
         host_ctx.close()
@@ -453,9 +468,15 @@ def run_batch_mode(a, rank, world, local_rank):
         t_batch, (res, st) = timed(b.run, a.steps)
         check(res)
     n = len(jobs)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    t_loop = reduce_over_ranks(t_loop, dist, dev)
+    t_loop_tuned = reduce_over_ranks(t_loop_tuned, dist, dev)
+    t_batch = reduce_over_ranks(t_batch, dist, dev)
     if rank == 0:
         line = {
-            "metric": "batched joins/s", "value": world * n / t_batch, "unit": "joins/s", "n_gpus": world,
+            "metric": "batched joins/s", "value": whole_job_rate(n, world, t_batch), "unit": "joins/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
             "config": {"workload": f"{n} PK-FK joins, |R| log-uniform in [2^10, 2^22] (multiple of 256), "
@@ -594,13 +615,11 @@ def run_serve_mode(a, rank, world, local_rank):
     for i, (lam, _, _) in enumerate(streams):
         if srv_out[i]["joins_per_s"] >= 0.95 * lam:
             best = i
-    joins_s = srv_out[best]["joins_per_s"]
+    dist = None
     if world > 1:
         import torch.distributed as dist
-
-        t = torch.tensor([joins_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MIN)
-        joins_s = float(t.item()) * world
+    # the slowest rank's sustained rate, times the ranks (each serves its own stream)
+    joins_s = world * reduce_over_ranks(srv_out[best]["joins_per_s"], dist, dev, op="min")
     if rank == 0:
         line = {
             "metric": "served joins/s at p99 latency", "value": joins_s, "unit": "joins/s", "n_gpus": world,
