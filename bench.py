@@ -50,9 +50,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["join", "batch", "serve"], default="join",
+    ap.add_argument("--mode", choices=["join", "batch", "serve", "skew"], default="join",
                     help="join: the headline 2^27 x 2^29 join; batch: 512 independent joins; "
-                         "serve: a Poisson stream of join requests through the join server")
+                         "serve: a Poisson stream of join requests through the join server; "
+                         "skew: 2^26 x 2^28 lp joins on Zipf and duplicate-key data")
     ap.add_argument("--rates", default="250,500,1000,1500,2000",
                     help="serve mode: offered request rates (requests/s) to sweep")
     ap.add_argument("--requests", type=int, default=1000, help="serve mode: requests per rate")
@@ -641,6 +642,101 @@ def run_serve_mode(a, rank, world, local_rank):
     return 0
 
 
+def dense_expected(torch, R, S, lp: bool):
+    """Result of a join whose keys are dense in [0, K] computed by direct addressing on the device (an
+    independent check, not the library): per key the build count, the wrapping sum of build row ids and
+    the row id of the first build tuple in input order."""
+    M = (1 << 64) - 1
+    rk, rr = R[:, 0], R[:, 1]
+    sk, sr = S[:, 0], S[:, 1]
+    K = int(max(int(rk.max()), int(sk.max()))) + 1
+    cnt = torch.bincount(rk, minlength=K)
+    if lp:
+        pos = torch.full((K,), R.shape[0], dtype=torch.int64, device=R.device)
+        pos.scatter_reduce_(0, rk, torch.arange(R.shape[0], device=R.device), reduce="amin", include_self=True)
+        hit = cnt[sk] > 0
+        first = rr[pos.clamp(max=R.shape[0] - 1)]
+        matched = int(hit.sum())
+        checksum = int((torch.where(hit, first[sk] + sr, torch.zeros_like(sr))).sum()) & M
+        return matched, checksum
+    sumr = torch.zeros(K, dtype=torch.int64, device=R.device).index_add_(0, rk, rr)
+    c = cnt[sk]
+    matched = int(c.sum())
+    checksum = int((sumr[sk] + c * sr).sum()) & M
+    return matched, checksum
+
+
+def run_skew_mode(a, rank, world, local_rank):
+    """Config 3: R = 2^26 unique keys (a seeded permutation, row_id = key), S = 2^28 Zipf FK keys for
+    theta in {0.5, 1.0, 1.5}; and the duplicate variant, R = 2^26 rows holding 2^24 distinct keys 4 times
+    each, S = 2^28 uniform over those keys. phj_radix_lp (14 bits, 2 passes) and nphj_lp, inputs resident
+    in HBM, every join checked against a direct-address count on the device."""
+    import torch
+
+    hj = load_module("hashjoin_scm_b200", PKG_DIR / "__init__.py")
+    hj.lib()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    nR, nS = 1 << 26, 1 << 28
+    R = torch.empty((nR, 2), dtype=torch.int64, device=dev)
+    S = torch.empty((nS, 2), dtype=torch.int64, device=dev)
+    ctx = hj.Context(local_rank)
+    cases = []
+    total_tuples, total_s = 0, 0.0
+    data = [("zipf 0.5", 0.5, 1), ("zipf 1.0", 1.0, 1), ("zipf 1.5", 1.5, 1), ("dup x4", None, 4)]
+    for name, theta, dup in data:
+        seed = 12345 + 1000 * rank
+        if theta is None:
+            hj.gen_fast_device(nR, nS, R.data_ptr(), S.data_ptr(), seed=seed, dup=dup, stream=stream.cuda_stream)
+        else:
+            hj.gen_fast_device(nR, 0, R.data_ptr(), S.data_ptr(), seed=seed, stream=stream.cuda_stream)
+            hj.gen_zipf_device(nS, nR, theta, S.data_ptr(), seed=seed, stream=stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        for algo in ("phj_radix_lp", "nphj_lp"):
+            want = dense_expected(torch, R, S, lp=True)
+            torch.cuda.synchronize(dev)
+
+            def step():
+                r = hj.join(algo, R, S, on_device=True, device=local_rank, stream=stream.cuda_stream,
+                            flags=hj.HJ_F_PHASE_TIMES, ctx=ctx)
+                if (r.matched_cnt, r.checksum) != want:
+                    raise RuntimeError(f"{name} {algo}: {(r.matched_cnt, r.checksum)} != {want}")
+                return r
+
+            for _ in range(a.warmup):
+                step()
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = [step() for _ in range(a.steps)]
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            sec = e0.elapsed_time(e1) / 1e3 / a.steps
+            phases = {n: round(statistics.mean(r.phase[i] for r in res) * 1e3, 3) for i, n in enumerate(hj.PHASES)}
+            cases.append({"data": name, "algo": algo, "ms": sec * 1e3, "tuples_per_s": (nR + nS) / sec,
+                          "matched_cnt": want[0], "phase_ms": phases,
+                          "large_partitions": int(res[-1].large_partitions)})
+            total_tuples += nR + nS
+            total_s += sec
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    total_s = reduce_over_ranks(total_s, dist, dev)
+    emit(rank, {
+        "metric": "skew/duplicate lp joins (|R|+|S|)/s", "value": whole_job_rate(total_tuples, world, total_s),
+        "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": total_s / len(cases) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": "R=2^26, S=2^28 16-B tuples: Zipf FK theta 0.5/1.0/1.5 over unique R keys, and "
+                               "R of 2^24 keys x4 with uniform S; phj_radix_lp (14 bits, 2 passes) and nphj_lp",
+                   "value": "all cases' tuples over all cases' time"},
+        "cases": cases,
+    })
+    ctx.close()
+    return 0
+
+
 def main():
     a = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -662,6 +758,8 @@ def main():
             return run_batch_mode(a, rank, world, local_rank)
         if a.mode == "serve":
             return run_serve_mode(a, rank, world, local_rank)
+        if a.mode == "skew":
+            return run_skew_mode(a, rank, world, local_rank)
         return run_ours(a, rank, world, local_rank)
     finally:
         if world > 1:
