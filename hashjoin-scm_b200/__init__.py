@@ -27,10 +27,19 @@ ALGOS = {
     "nphj_lp": 1,
     "phj_radix_bc": 2,
     "phj_radix_lp": 3,
-    # bandwidth-regulated aliases compute the same results (src/algo/phj_bw_reg.c:2874-2893)
-    "phj_radix_bw_reg_bc": 2,
-    "phj_radix_bw_reg_lp": 3,
+    # every match counted, as phj_radix_bc (src/algo/phj.c:683, 784, 881)
+    "phj_radix_sc": 4,
+    "phj_radix_hr": 5,
+    "phj_radix_hro": 6,
 }
+# bandwidth-regulated aliases compute the same results (src/algo/phj_bw_reg.c:2874-2893); the
+# asymmetric-radix names run with radix_bits_pass1 (src/algo/phj_asymm_radix.c)
+for _s, _a in (("bc", 2), ("lp", 3), ("sc", 4), ("hr", 5), ("hro", 6)):
+    ALGOS["phj_radix_bw_reg_" + _s] = _a
+    if _s != "lp":
+        ALGOS["phj_asymm_radix_" + _s] = _a
+        ALGOS["phj_asymm_radix_bw_reg_" + _s] = _a
+ASYMM_DEFAULT_BITS_PASS1 = 11
 
 STATUS = {
     0: "HJ_OK",
@@ -62,6 +71,8 @@ class Params(ctypes.Structure):
         ("stream", ctypes.c_void_p),
         ("flags", ctypes.c_uint32),
         ("table_load", ctypes.c_double),
+        ("radix_bits_pass1", ctypes.c_int),
+        ("reserved", ctypes.c_int),
     ]
 
 
@@ -170,7 +181,7 @@ def _ptr_len(rel, on_device: bool):
 
 
 def make_params(bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
-                stream: int | None = None, flags: int = 0, load: float = 0.5) -> Params:
+                stream: int | None = None, flags: int = 0, load: float = 0.5, bits_pass1: int = 0) -> Params:
     p = Params()
     lib().hj_params_init(ctypes.byref(p))
     p.num_radix_bits, p.num_passes, p.device = bits, passes, device
@@ -178,16 +189,21 @@ def make_params(bits: int = 14, passes: int = 2, device: int = 0, on_device: boo
     p.stream = stream or None
     p.flags = flags
     p.table_load = load
+    p.radix_bits_pass1 = bits_pass1
     return p
 
 
 def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
          stream: int | None = None, flags: int = 0, load: float = 0.5, ctx: "Context | None" = None,
-         check: bool = True) -> Result:
-    """Run one join (synchronous). Raises JoinError on a non-zero status when check is set."""
+         check: bool = True, bits_pass1: int | None = None) -> Result:
+    """Run one join (synchronous). Raises JoinError on a non-zero status when check is set.
+    bits_pass1: pass-1 radix bits of a two-pass join (None: 11 for phj_asymm_radix_* names, as the
+    reference's NUM_RADIX_BITS_PASS1 default, else an even split)."""
     L = lib()
     a = ALGOS[algo]
-    p = make_params(bits, passes, device, on_device, stream, flags, load)
+    if bits_pass1 is None:
+        bits_pass1 = ASYMM_DEFAULT_BITS_PASS1 if algo.startswith("phj_asymm_radix") else 0
+    p = make_params(bits, passes, device, on_device, stream, flags, load, bits_pass1)
     pr, nr = _ptr_len(R, on_device)
     ps, ns = _ptr_len(S, on_device)
     res = Result()

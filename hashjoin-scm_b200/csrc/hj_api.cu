@@ -54,7 +54,7 @@ void resolve_params(const hj_params_t *p, hj_params_t *out) {
     if (!(out->table_load > 0.0)) out->table_load = 0.5;
 }
 
-bool is_phj(hj_algo_t a) { return a == HJ_ALGO_PHJ_RADIX_BC || a == HJ_ALGO_PHJ_RADIX_LP; }
+bool is_phj(hj_algo_t a) { return hj::algo_is_phj(a); }
 
 int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, bool host_inputs, int num_sms,
                  size_t *bytes) {
@@ -62,7 +62,7 @@ int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, boo
     if (host_inputs) need += align256(nR * 16) + align256(nS * 16);
     if (is_phj(algo)) {
         hj::RadixGeom g;
-        int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &g);
+        int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &g, p.radix_bits_pass1);
         if (rc) return rc;
         need += hj::phj_scratch_bytes(g, nR, nS, num_sms);
     } else {
@@ -122,7 +122,8 @@ const char *hj_status_str(int s) {
     }
 }
 
-static const char *const k_algo_names[HJ_ALGO_COUNT] = {"nphj_sc", "nphj_lp", "phj_radix_bc", "phj_radix_lp"};
+static const char *const k_algo_names[HJ_ALGO_COUNT] = {"nphj_sc",      "nphj_lp",      "phj_radix_bc", "phj_radix_lp",
+                                                        "phj_radix_sc", "phj_radix_hr", "phj_radix_hro"};
 
 const char *hj_algo_name(hj_algo_t a) {
     return ((int)a >= 0 && a < HJ_ALGO_COUNT) ? k_algo_names[a] : "?";
@@ -135,14 +136,23 @@ int hj_algo_from_name(const char *name, hj_algo_t *algo) {
             *algo = (hj_algo_t)i;
             return HJ_OK;
         }
-    // Bandwidth-regulated variants compute identical results (src/algo/phj_bw_reg.c:2874-2893).
-    if (strcmp(name, "phj_radix_bw_reg_bc") == 0) {
-        *algo = HJ_ALGO_PHJ_RADIX_BC;
-        return HJ_OK;
-    }
-    if (strcmp(name, "phj_radix_bw_reg_lp") == 0) {
-        *algo = HJ_ALGO_PHJ_RADIX_LP;
-        return HJ_OK;
+    // Bandwidth-regulated variants compute identical results (src/algo/phj_bw_reg.c:2874-2893); the
+    // asymmetric-radix variants too (the bit split is hj_params_t.radix_bits_pass1).
+    static const char *const prefixes[] = {"phj_radix_bw_reg_", "phj_asymm_radix_bw_reg_", "phj_asymm_radix_"};
+    for (const char *pre : prefixes) {
+        const size_t n = strlen(pre);
+        if (strncmp(name, pre, n) != 0) continue;
+        const char *suf = name + n;
+        static const char *const sufs[] = {"bc", "lp", "sc", "hr", "hro"};
+        static const hj_algo_t algs[] = {HJ_ALGO_PHJ_RADIX_BC, HJ_ALGO_PHJ_RADIX_LP, HJ_ALGO_PHJ_RADIX_SC,
+                                         HJ_ALGO_PHJ_RADIX_HR, HJ_ALGO_PHJ_RADIX_HRO};
+        for (int i = 0; i < 5; i++)
+            if (strcmp(suf, sufs[i]) == 0) {
+                // The reference has no phj_asymm_radix_lp (src/main.c:80-82, 114-116, 128, 138).
+                if (i == 1 && pre[4] == 'a') return HJ_E_NOT_FOUND;
+                *algo = algs[i];
+                return HJ_OK;
+            }
     }
     return HJ_E_NOT_FOUND;
 }
@@ -217,7 +227,7 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     if (p.device != c->device) return out->status = HJ_E_INVAL;
     hj::RadixGeom geom = {};
     if (is_phj(algo)) {
-        int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &geom);
+        int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &geom, p.radix_bits_pass1);
         if (rc) return out->status = rc;
         out->physical_passes = geom.passes;
     }
@@ -258,11 +268,11 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     if (is_phj(algo)) {
         hj::PhjScratch s;
         hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s);
-        rc = hj::phj_enqueue(geom, algo == HJ_ALGO_PHJ_RADIX_LP, algo == HJ_ALGO_PHJ_RADIX_LP, dR, nR, dS, nS, s, acc, st,
+        rc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
                              timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
     } else {
         const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
-        rc = hj::nphj_enqueue(algo == HJ_ALGO_NPHJ_LP, false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
+        rc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
                               timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
     }
     if (rc) {

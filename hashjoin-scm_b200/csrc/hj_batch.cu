@@ -287,8 +287,8 @@ void make_chunks(std::vector<hj::MChunk> &out, unsigned job, unsigned long long 
 
 size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-bool sem_lp(hj_algo_t a) { return a == HJ_ALGO_NPHJ_LP || a == HJ_ALGO_PHJ_RADIX_LP; }
-bool sem_skip0(hj_algo_t a) { return a == HJ_ALGO_PHJ_RADIX_LP; }
+bool sem_lp(hj_algo_t a) { return hj::algo_lp(a); }
+bool sem_skip0(hj_algo_t a) { return hj::algo_skip0(a); }
 
 unsigned long long nphj_slots(size_t nR) { return (unsigned long long)((double)nR / 0.5) + 2; }
 

@@ -21,7 +21,14 @@ struct RadixGeom {
     int nparts() const { return 1 << bits; }
 };
 
-int radix_geom(int bits, int passes, RadixGeom *g);
+// b1_req > 0 asks for that many pass-1 bits (clamped so that both passes have 1..8 bits).
+int radix_geom(int bits, int passes, RadixGeom *g, int b1_req = 0);
+
+// Result semantics of an algorithm: radix-partitioned or not; first match per probe tuple (lp) or
+// every match; build key 0 never matches (the phj_radix_lp empty-slot rule, src/algo/phj.c:614).
+inline bool algo_is_phj(hj_algo_t a) { return a >= HJ_ALGO_PHJ_RADIX_BC && a < HJ_ALGO_COUNT; }
+inline bool algo_lp(hj_algo_t a) { return a == HJ_ALGO_NPHJ_LP || a == HJ_ALGO_PHJ_RADIX_LP; }
+inline bool algo_skip0(hj_algo_t a) { return a == HJ_ALGO_PHJ_RADIX_LP; }
 
 // Tile and work-item constants shared by the plan and the kernels.
 constexpr int kScatterThreads = 256;

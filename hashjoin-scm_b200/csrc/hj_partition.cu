@@ -1141,7 +1141,7 @@ __global__ void copy_error(const uint32_t *counters, JoinAccum *acc) {
 // ------------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------------
-int radix_geom(int bits, int passes, RadixGeom *g) {
+int radix_geom(int bits, int passes, RadixGeom *g, int b1_req) {
     if (bits < 1 || bits > 15) return HJ_E_INVAL;
     if (passes != 1 && passes != 2) return HJ_E_INVAL;
     // Partition contents do not depend on how the bits are split across passes; a single pass runs
@@ -1151,7 +1151,15 @@ int radix_geom(int bits, int passes, RadixGeom *g) {
     if (P == 2 && bits < 2) P = 1;
     g->bits = bits;
     g->passes = P;
-    g->b1 = P == 2 ? bits / 2 : bits;
+    int b1 = bits / 2;
+    if (b1_req > 0) {
+        b1 = b1_req;
+        if (b1 > 8) b1 = 8;
+        if (b1 > bits - 1) b1 = bits - 1;
+        if (b1 < bits - 8) b1 = bits - 8;
+        if (b1 < 1) b1 = 1;
+    }
+    g->b1 = P == 2 ? b1 : bits;
     g->b2 = bits - g->b1;
     if (g->b1 > 8 || g->b2 > 8) return HJ_E_INVAL;
     g->F1 = 1 << g->b1;

@@ -136,7 +136,7 @@ namespace {
 int request_need(hj_server *s, Request &r) {
     hj_params_t p;
     hj_params_init(&p);
-    const bool phj_named = r.algo == HJ_ALGO_PHJ_RADIX_BC || r.algo == HJ_ALGO_PHJ_RADIX_LP;
+    const bool phj_named = hj::algo_is_phj(r.algo);
     if (s->cfg.autotune) {
         hj_tuner_decide(s->ctx, r.nR, r.nS, &r.impl, &r.bits, &r.passes);
     } else {
@@ -177,8 +177,8 @@ int launch(hj_server *s, Slot &sl) {
         R = dr;
         S = ds;
     }
-    const bool lp = r.algo == HJ_ALGO_NPHJ_LP || r.algo == HJ_ALGO_PHJ_RADIX_LP;
-    const bool skip0 = r.algo == HJ_ALGO_PHJ_RADIX_LP;
+    const bool lp = hj::algo_lp(r.algo);
+    const bool skip0 = hj::algo_skip0(r.algo);
     int rc = HJ_OK;
     if (r.nR && r.nS) {
         if (r.impl == 0) {

@@ -18,7 +18,7 @@
 
 static pthread_mutex_t g_cfg_mu = PTHREAD_MUTEX_INITIALIZER;
 static char g_prefix[4096] = "";
-static int g_bits = -1, g_passes = -1, g_device = -1;
+static int g_bits = -1, g_passes = -1, g_device = -1, g_bits_pass1 = -1;
 static __thread hj_result_t t_last;
 static __thread int t_have_last;
 
@@ -47,6 +47,21 @@ static void current_config(char *prefix, size_t plen, hj_params_t *p) {
     pthread_mutex_unlock(&g_cfg_mu);
 }
 
+void hj_ref_configure_asymm(int num_radix_bits_pass1) {
+    pthread_mutex_lock(&g_cfg_mu);
+    g_bits_pass1 = num_radix_bits_pass1;
+    pthread_mutex_unlock(&g_cfg_mu);
+}
+
+/* Pass-1 bits of the phj_asymm_radix_* entry points: NUM_RADIX_BITS_PASS1, 11 unless configured
+ * (src/algo/phj_asymm_radix.h:10-17). */
+static int asymm_bits_pass1(void) {
+    pthread_mutex_lock(&g_cfg_mu);
+    const int b = g_bits_pass1 >= 0 ? g_bits_pass1 : env_int("HJ_NUM_RADIX_BITS_PASS1", 11);
+    pthread_mutex_unlock(&g_cfg_mu);
+    return b;
+}
+
 int hj_load_bin(const char *path, size_t n, hj_tuple_t *buf) {
     if (!path || (n && !buf)) return HJ_E_INVAL;
     FILE *f = fopen(path, "rb");
@@ -72,10 +87,11 @@ int hj_ref_last_result(hj_result_t *out) {
 }
 
 /* Shared body of the entry points: the part of join_init_run / nphj_sc outside the thread pools. */
-static void run_ref(hj_algo_t algo, const datameta_t datameta, timekeeper_t *const tk) {
+static void run_ref_p1(hj_algo_t algo, int bits_pass1, const datameta_t datameta, timekeeper_t *const tk) {
     char prefix[4096], rpath[8192], spath[8192];
     hj_params_t p;
     current_config(prefix, sizeof(prefix), &p);
+    p.radix_bits_pass1 = bits_pass1;
     hj_result_t res;
     memset(&res, 0, sizeof(res));
     tk->buildpart = tk->probejoin = 0.0;
@@ -104,12 +120,31 @@ static void run_ref(hj_algo_t algo, const datameta_t datameta, timekeeper_t *con
     tk->total = res.total;
 }
 
+static void run_ref(hj_algo_t algo, const datameta_t d, timekeeper_t *const tk) { run_ref_p1(algo, 0, d, tk); }
+static void run_asymm(hj_algo_t algo, const datameta_t d, timekeeper_t *const tk) {
+    run_ref_p1(algo, asymm_bits_pass1(), d, tk);
+}
+
 void nphj_sc(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_NPHJ_SC, d, tk); }
 void nphj_lp(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_NPHJ_LP, d, tk); }
 void phj_radix_bc(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_BC, d, tk); }
 void phj_radix_lp(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_LP, d, tk); }
 void phj_radix_bw_reg_bc(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_BC, d, tk); }
 void phj_radix_bw_reg_lp(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_LP, d, tk); }
+void phj_radix_sc(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_SC, d, tk); }
+void phj_radix_hr(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_HR, d, tk); }
+void phj_radix_hro(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_HRO, d, tk); }
+void phj_radix_bw_reg_sc(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_SC, d, tk); }
+void phj_radix_bw_reg_hr(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_HR, d, tk); }
+void phj_radix_bw_reg_hro(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_PHJ_RADIX_HRO, d, tk); }
+void phj_asymm_radix_bc(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_BC, d, tk); }
+void phj_asymm_radix_sc(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_SC, d, tk); }
+void phj_asymm_radix_hr(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_HR, d, tk); }
+void phj_asymm_radix_hro(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_HRO, d, tk); }
+void phj_asymm_radix_bw_reg_bc(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_BC, d, tk); }
+void phj_asymm_radix_bw_reg_sc(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_SC, d, tk); }
+void phj_asymm_radix_bw_reg_hr(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_HR, d, tk); }
+void phj_asymm_radix_bw_reg_hro(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_HRO, d, tk); }
 
 const algo_t hj_ref_algos[] = {
     {"nphj_sc", nphj_sc},
@@ -118,6 +153,20 @@ const algo_t hj_ref_algos[] = {
     {"phj_radix_lp", phj_radix_lp},
     {"phj_radix_bw_reg_bc", phj_radix_bw_reg_bc},
     {"phj_radix_bw_reg_lp", phj_radix_bw_reg_lp},
+    {"phj_radix_sc", phj_radix_sc},
+    {"phj_radix_hr", phj_radix_hr},
+    {"phj_radix_hro", phj_radix_hro},
+    {"phj_radix_bw_reg_sc", phj_radix_bw_reg_sc},
+    {"phj_radix_bw_reg_hr", phj_radix_bw_reg_hr},
+    {"phj_radix_bw_reg_hro", phj_radix_bw_reg_hro},
+    {"phj_asymm_radix_bc", phj_asymm_radix_bc},
+    {"phj_asymm_radix_sc", phj_asymm_radix_sc},
+    {"phj_asymm_radix_hr", phj_asymm_radix_hr},
+    {"phj_asymm_radix_hro", phj_asymm_radix_hro},
+    {"phj_asymm_radix_bw_reg_bc", phj_asymm_radix_bw_reg_bc},
+    {"phj_asymm_radix_bw_reg_sc", phj_asymm_radix_bw_reg_sc},
+    {"phj_asymm_radix_bw_reg_hr", phj_asymm_radix_bw_reg_hr},
+    {"phj_asymm_radix_bw_reg_hro", phj_asymm_radix_bw_reg_hro},
 };
 const int hj_ref_algo_count = (int)(sizeof(hj_ref_algos) / sizeof(hj_ref_algos[0]));
 

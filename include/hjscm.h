@@ -15,8 +15,14 @@
  *   phj_radix_lp   radix-partitioned join, linear-probing partition tables, first match per probe
  *                  (replaces src/algo/phj.c phj_radix_lp -> join_init_run(..., lp_join))
  *
- * plus the bandwidth-regulated aliases phj_radix_bw_reg_bc / phj_radix_bw_reg_lp, which compute the
- * same results (src/algo/phj_bw_reg.c:2874-2893).
+ * phj_radix_sc, phj_radix_hr and phj_radix_hro differ from phj_radix_bc only in the layout of the
+ * in-partition table on the CPU (separate-chaining buckets, src/algo/phj.c:683; a histogram-sorted copy
+ * of R_p scanned per bucket, phj.c:784; the same scanned with AVX-512, phj.c:881). All three count every
+ * match, so their results equal phj_radix_bc's and they run its partition join here.
+ * The phj_asymm_radix_* names (src/algo/phj_asymm_radix.c) split the radix bits unevenly between the
+ * two passes (hj_params_t.radix_bits_pass1); the partitions, hence the results, do not depend on the
+ * split. The bandwidth-regulated names phj_radix_bw_reg_* / phj_asymm_radix_bw_reg_* compute the same
+ * results as their unregulated counterparts (src/algo/phj_bw_reg.c:2874-2893).
  *
  * All entry points return an int status (HJ_OK or an HJ_E_* code) instead of exiting, and no entry
  * point frees memory it does not own.
@@ -49,7 +55,10 @@ typedef enum {
     HJ_ALGO_NPHJ_LP = 1,
     HJ_ALGO_PHJ_RADIX_BC = 2,
     HJ_ALGO_PHJ_RADIX_LP = 3,
-    HJ_ALGO_COUNT = 4
+    HJ_ALGO_PHJ_RADIX_SC = 4,  /* src/algo/phj.c:2523 phj_radix_sc -> sc_join (phj.c:683) */
+    HJ_ALGO_PHJ_RADIX_HR = 5,  /* src/algo/phj.c:2527 phj_radix_hr -> hr_join (phj.c:784) */
+    HJ_ALGO_PHJ_RADIX_HRO = 6, /* src/algo/phj.c:2532 phj_radix_hro -> hro_join (phj.c:881) */
+    HJ_ALGO_COUNT = 7
 } hj_algo_t;
 
 /* Status codes. The reference exit()s on every failure (src/main.c:215-218, src/inc/utils.c:501-518). */
@@ -76,6 +85,10 @@ typedef struct {
     void *stream;         /* cudaStream_t to run on; NULL selects the context's own stream */
     uint32_t flags;       /* HJ_F_* bits */
     double table_load;    /* NPHJ global table load factor (0 selects 0.5) */
+    int radix_bits_pass1; /* two passes: bits of pass 1 (NUM_RADIX_BITS_PASS1 of phj_asymm_radix,
+                             src/algo/phj_asymm_radix.h:10-19); 0 selects bits / 2. Clamped to the
+                             split where each pass has 1..8 bits. */
+    int reserved;
 } hj_params_t;
 
 #define HJ_F_NO_TIMING   0x1u /* skip the per-phase CUDA events (buildpart/probejoin stay 0) */

@@ -61,13 +61,31 @@ typedef struct algo_t {
     void (*joinalgo)(const datameta_t, timekeeper_t *const);
 } algo_t;
 
-/* Entry points under the reference's names (src/main.c:73-77, 109-110). */
+/* Entry points under the reference's names (src/main.c:73-82, 109-116, 126-138). */
 void nphj_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
 void nphj_lp(const datameta_t datameta, timekeeper_t *const timekeeper);
 void phj_radix_bc(const datameta_t datameta, timekeeper_t *const timekeeper);
 void phj_radix_lp(const datameta_t datameta, timekeeper_t *const timekeeper);
 void phj_radix_bw_reg_bc(const datameta_t datameta, timekeeper_t *const timekeeper);
 void phj_radix_bw_reg_lp(const datameta_t datameta, timekeeper_t *const timekeeper);
+/* Same results as phj_radix_bc (every match counted; src/algo/phj.c:2523-2535). */
+void phj_radix_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_radix_hr(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_radix_hro(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_radix_bw_reg_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_radix_bw_reg_hr(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_radix_bw_reg_hro(const datameta_t datameta, timekeeper_t *const timekeeper);
+/* Two passes with NUM_RADIX_BITS_PASS1 bits in pass 1 (src/algo/phj_asymm_radix.c,
+ * phj_asymm_radix.h:10-19; 11 unless hj_ref_configure_asymm or HJ_NUM_RADIX_BITS_PASS1 says otherwise,
+ * clamped so that each pass has at most 8 bits). */
+void phj_asymm_radix_bc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_asymm_radix_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_asymm_radix_hr(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_asymm_radix_hro(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_asymm_radix_bw_reg_bc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_asymm_radix_bw_reg_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_asymm_radix_bw_reg_hr(const datameta_t datameta, timekeeper_t *const timekeeper);
+void phj_asymm_radix_bw_reg_hro(const datameta_t datameta, timekeeper_t *const timekeeper);
 
 /* The dispatch table (src/main.c:72-143 restricted to the names above) and its length. */
 extern const algo_t hj_ref_algos[];
@@ -78,6 +96,8 @@ const algo_t *hj_ref_find_algo(const char *name);
 /* Run-time replacements for the reference's compile-time knobs. prefix may be NULL (keep),
  * num_radix_bits / num_passes / device < 0 keep the current value. */
 void hj_ref_configure(const char *data_path_prefix, int num_radix_bits, int num_passes, int device);
+/* NUM_RADIX_BITS_PASS1 of the phj_asymm_radix_* entry points (< 0: back to the environment / 11). */
+void hj_ref_configure_asymm(int num_radix_bits_pass1);
 
 /* Result of the last call of one of the functions above on this thread (the reference only prints
  * it). */

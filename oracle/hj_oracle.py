@@ -29,8 +29,14 @@ LIB_PATH = HERE / "liboracle.so"
 REF_DIR = HERE / "_ref"
 
 ALL, FIRST, FIRST_NP = 0, 1, 2  # hj_oracle.c modes: bc/sc, phj lp, nphj lp
+# sc_join, hr_join and hro_join count every match (src/algo/phj.c:683-1037), as bc_join does.
 MODE_OF_ALGO = {"nphj_sc": ALL, "phj_radix_bc": ALL, "nphj_lp": FIRST_NP, "phj_radix_lp": FIRST,
-                "phj_radix_bw_reg_bc": ALL, "phj_radix_bw_reg_lp": FIRST}
+                "phj_radix_sc": ALL, "phj_radix_hr": ALL, "phj_radix_hro": ALL}
+for _s, _m in (("bc", ALL), ("lp", FIRST), ("sc", ALL), ("hr", ALL), ("hro", ALL)):
+    MODE_OF_ALGO["phj_radix_bw_reg_" + _s] = _m
+    if _s != "lp":
+        MODE_OF_ALGO["phj_asymm_radix_" + _s] = _m
+        MODE_OF_ALGO["phj_asymm_radix_bw_reg_" + _s] = _m
 RAND_MAX = 2147483647
 MASK64 = (1 << 64) - 1
 
@@ -263,12 +269,14 @@ _TRIAL_LINE = re.compile(r"hjref_trial: (\d+) buildpart: ([\d.eE+-]+) probejoin:
 
 
 def ref_run_files(algo: str, prefix: str, rfile: str, sfile: str, nR: int, nS: int, bits: int = 14,
-                  passes: int = 2, threads: int | None = None, trials: int = 1, timeout: float = 900):
-    """Run the reference's join on .bin files; returns [(cnt, sum, buildpart, probejoin, total)]."""
+                  passes: int = 2, threads: int | None = None, trials: int = 1, timeout: float = 900,
+                  bits1: int = 11):
+    """Run the reference's join on .bin files; returns [(cnt, sum, buildpart, probejoin, total)].
+    bits1 is NUM_RADIX_BITS_PASS1 of the phj_asymm_radix_* joins."""
     threads = threads or os.cpu_count() or 1
     cmd = [str(REF_DIR / f"hjref_p{passes}"), f"--algo={algo}", f"--prefix={prefix}", f"--r={rfile}",
            f"--s={sfile}", f"--nr={nR}", f"--ns={nS}", f"--bits={bits}", f"--threads={threads}",
-           f"--trials={trials}"]
+           f"--trials={trials}", f"--bits1={bits1}"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
     if out.returncode != 0:
         raise RuntimeError(f"reference run failed ({out.returncode}): {out.stderr[-2000:]}")
@@ -278,10 +286,11 @@ def ref_run_files(algo: str, prefix: str, rfile: str, sfile: str, nR: int, nS: i
 
 
 def ref_join(algo: str, R: np.ndarray, S: np.ndarray, bits: int = 14, passes: int = 2,
-             threads: int | None = None) -> tuple[int, int]:
+             threads: int | None = None, bits1: int = 11) -> tuple[int, int]:
     """(matched_cnt, check_sum) printed by the reference's own join on these relations."""
     with tempfile.TemporaryDirectory() as d:
         _arr(R).tofile(os.path.join(d, "r.bin"))
         _arr(S).tofile(os.path.join(d, "s.bin"))
-        runs = ref_run_files(algo, d, "r.bin", "s.bin", R.shape[0], S.shape[0], bits, passes, threads)
+        runs = ref_run_files(algo, d, "r.bin", "s.bin", R.shape[0], S.shape[0], bits, passes, threads,
+                             bits1=bits1)
         return runs[0][0], runs[0][1]

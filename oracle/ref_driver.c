@@ -4,8 +4,11 @@
  *
  * It replaces src/main.c's libconfig-driven setup (src/main.c:147-255) with flags and calls the
  * reference functions unmodified:
- *   hjref_pN --algo=<nphj_sc|nphj_lp|phj_radix_bc|phj_radix_lp> --prefix=DIR --r=REL --s=REL
- *            --nr=N --ns=M [--bits=14] [--threads=T] [--trials=K]
+ *   hjref_pN --algo=NAME --prefix=DIR --r=REL --s=REL --nr=N --ns=M [--bits=14] [--bits1=11]
+ *            [--threads=T] [--trials=K]
+ *       NAME: nphj_sc, nphj_lp, phj_radix_{bc,lp,sc,hr,hro}, and with N = 2 phj_asymm_radix_{bc,sc,hr,hro}
+ *       (pass-1 bits --bits1, NUM_RADIX_BITS_PASS1, default 11 and at most --bits as
+ *       src/algo/phj_asymm_radix.h:10-17 rules).
  *       Each trial prints the reference's "matched_cnt: ..\tcheck_sum: .." line, then
  *       "hjref_trial: <k> buildpart: <s> probejoin: <s> total: <s>".
  *   hjref_pN --gen=<pkfk|payload|dup|zipf> --prefix=DIR --nr=N --ns=M [--factor=F] [--seed=12345]
@@ -22,6 +25,7 @@
 
 int hjref_threads = 1;
 int hjref_radix_bits = 14;
+int hjref_radix_bits_pass1 = 11;
 const char *hjref_data_prefix = ".";
 const char *hjref_work_prefix = "/tmp";
 
@@ -32,6 +36,15 @@ void nphj_sc(const datameta_t, timekeeper_t *const);
 void nphj_lp(const datameta_t, timekeeper_t *const);
 void phj_radix_bc(const datameta_t, timekeeper_t *const);
 void phj_radix_lp(const datameta_t, timekeeper_t *const);
+void phj_radix_sc(const datameta_t, timekeeper_t *const);
+void phj_radix_hr(const datameta_t, timekeeper_t *const);
+void phj_radix_hro(const datameta_t, timekeeper_t *const);
+#if NUM_PASSES == 2
+void phj_asymm_radix_bc(const datameta_t, timekeeper_t *const);
+void phj_asymm_radix_sc(const datameta_t, timekeeper_t *const);
+void phj_asymm_radix_hr(const datameta_t, timekeeper_t *const);
+void phj_asymm_radix_hro(const datameta_t, timekeeper_t *const);
+#endif
 void gen_pkfk_uniform(const size_t, const size_t, const char *, const char *, const char *);
 void payload_gen_pkfk_uniform(const size_t, const size_t, const char *, const char *, const char *);
 void gen_dup_uniform(const size_t, const size_t, const char *, const char *, const char *);
@@ -53,6 +66,8 @@ int main(int argc, char **argv) {
     hjref_threads = (v = arg(argc, argv, "threads")) ? atoi(v) : (int)nproc;
     if (hjref_threads < 1) hjref_threads = 1;
     hjref_radix_bits = (v = arg(argc, argv, "bits")) ? atoi(v) : 14;
+    hjref_radix_bits_pass1 = (v = arg(argc, argv, "bits1")) ? atoi(v) : 11;
+    if (hjref_radix_bits_pass1 > hjref_radix_bits) hjref_radix_bits_pass1 = hjref_radix_bits;
     hjref_data_prefix = (v = arg(argc, argv, "prefix")) ? v : ".";
     const size_t nR = (v = arg(argc, argv, "nr")) ? strtoull(v, NULL, 10) : 0;
     const size_t nS = (v = arg(argc, argv, "ns")) ? strtoull(v, NULL, 10) : 0;
@@ -80,6 +95,15 @@ int main(int argc, char **argv) {
     else if (algo && !strcmp(algo, "nphj_lp")) fn = nphj_lp;
     else if (algo && !strcmp(algo, "phj_radix_bc")) fn = phj_radix_bc;
     else if (algo && !strcmp(algo, "phj_radix_lp")) fn = phj_radix_lp;
+    else if (algo && !strcmp(algo, "phj_radix_sc")) fn = phj_radix_sc;
+    else if (algo && !strcmp(algo, "phj_radix_hr")) fn = phj_radix_hr;
+    else if (algo && !strcmp(algo, "phj_radix_hro")) fn = phj_radix_hro;
+#if NUM_PASSES == 2
+    else if (algo && !strcmp(algo, "phj_asymm_radix_bc")) fn = phj_asymm_radix_bc;
+    else if (algo && !strcmp(algo, "phj_asymm_radix_sc")) fn = phj_asymm_radix_sc;
+    else if (algo && !strcmp(algo, "phj_asymm_radix_hr")) fn = phj_asymm_radix_hr;
+    else if (algo && !strcmp(algo, "phj_asymm_radix_hro")) fn = phj_asymm_radix_hro;
+#endif
     if (!fn) {
         fprintf(stderr, "unknown or missing --algo\n");
         return 2;

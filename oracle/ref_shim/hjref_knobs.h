@@ -8,6 +8,7 @@
 #define HJREF_KNOBS_H
 extern int hjref_threads;
 extern int hjref_radix_bits;
+extern int hjref_radix_bits_pass1;
 extern const char *hjref_data_prefix;
 extern const char *hjref_work_prefix;
 #define THREAD_NUM hjref_threads
@@ -20,6 +21,9 @@ extern const char *hjref_work_prefix;
 #define CORE_NUM 1024
 #define SINGLE_SOCKET_CORE_NUM 1024
 #define NUM_RADIX_BITS hjref_radix_bits
+/* phj_asymm_radix.h compares this with NUM_RADIX_BITS in an #if; as identifiers both read 0 there, so
+ * the header keeps this definition, and the driver applies the header's clamp (pass 1 <= all bits). */
+#define NUM_RADIX_BITS_PASS1 hjref_radix_bits_pass1
 #define DATA_PATH_PREFIX hjref_data_prefix
 #define WORK_PATH_PREFIX hjref_work_prefix
 #define DUMP_PATH_PREFIX hjref_work_prefix

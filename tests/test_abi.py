@@ -17,8 +17,13 @@ def test_every_declared_function_is_exported(hj):
     assert not missing, missing
 
 
-@pytest.mark.parametrize("name,code", [("nphj_sc", 0), ("nphj_lp", 1), ("phj_radix_bc", 2), ("phj_radix_lp", 3),
-                                       ("phj_radix_bw_reg_bc", 2), ("phj_radix_bw_reg_lp", 3)])
+@pytest.mark.parametrize("name,code", [
+    ("nphj_sc", 0), ("nphj_lp", 1), ("phj_radix_bc", 2), ("phj_radix_lp", 3), ("phj_radix_sc", 4),
+    ("phj_radix_hr", 5), ("phj_radix_hro", 6), ("phj_radix_bw_reg_bc", 2), ("phj_radix_bw_reg_lp", 3),
+    ("phj_radix_bw_reg_sc", 4), ("phj_radix_bw_reg_hr", 5), ("phj_radix_bw_reg_hro", 6),
+    ("phj_asymm_radix_bc", 2), ("phj_asymm_radix_sc", 4), ("phj_asymm_radix_hr", 5), ("phj_asymm_radix_hro", 6),
+    ("phj_asymm_radix_bw_reg_bc", 2), ("phj_asymm_radix_bw_reg_sc", 4), ("phj_asymm_radix_bw_reg_hr", 5),
+    ("phj_asymm_radix_bw_reg_hro", 6)])
 def test_algo_lookup(hj, name, code):
     out = ctypes.c_int(-1)
     assert hj.lib().hj_algo_from_name(name.encode(), ctypes.byref(out)) == 0
@@ -28,9 +33,12 @@ def test_algo_lookup(hj, name, code):
 def test_algo_lookup_unknown_and_names(hj):
     out = ctypes.c_int(-1)
     L = hj.lib()
-    assert L.hj_algo_from_name(b"phj_radix_hr", ctypes.byref(out)) == hj.HJ_E_NOT_FOUND
+    # names the reference does not have (src/main.c:72-143), or that this library does not implement
+    for bad in (b"phj_asymm_radix_lp", b"phj_radix_bw_reg_", b"phj_radix_xx", b"ptr_phj_radix_hro", b"phj_ind_sc"):
+        assert L.hj_algo_from_name(bad, ctypes.byref(out)) == hj.HJ_E_NOT_FOUND, bad
     assert L.hj_algo_from_name(None, ctypes.byref(out)) == hj.HJ_E_INVAL
-    assert [L.hj_algo_name(i).decode() for i in range(4)] == ["nphj_sc", "nphj_lp", "phj_radix_bc", "phj_radix_lp"]
+    assert [L.hj_algo_name(i).decode() for i in range(7)] == ["nphj_sc", "nphj_lp", "phj_radix_bc", "phj_radix_lp",
+                                                             "phj_radix_sc", "phj_radix_hr", "phj_radix_hro"]
     for code in range(10):
         assert L.hj_status_str(code)
 
@@ -100,7 +108,7 @@ def test_cli_gen_matches_library_generator(hj, tmp_path):
 
 
 def test_cli_unknown_algo(hj):
-    out = subprocess.run([str(hj.MAIN_PATH), "--algo=phj_radix_hro", "--r=x", "--s=y", "--nr=1", "--ns=1"],
+    out = subprocess.run([str(hj.MAIN_PATH), "--algo=ptr_phj_radix_hro", "--r=x", "--s=y", "--nr=1", "--ns=1"],
                          capture_output=True, text=True)
     assert out.returncode == 1
     assert "does not exist" in out.stdout  # the reference's message (src/main.c:215)
@@ -131,3 +139,23 @@ def test_server_config_defaults(hj):
     assert (cfg.device, cfg.slots, cfg.hbm_budget_bytes, cfg.autotune) == (0, 8, 150e9, 1)
     assert L.hj_server_config_init(None) == hj.HJ_E_INVAL
     assert 0 < hj.now()
+
+
+def test_reference_table_names_resolve(hj):
+    # Every name of the reference-facing dispatch table is also a library algorithm, and both agree
+    # with the Python table.
+    L = hj.lib()
+    import ctypes as C
+
+    class AlgoT(C.Structure):
+        _fields_ = [("name", C.c_char * 128), ("fn", C.c_void_p)]
+
+    n = C.c_int.in_dll(L, "hj_ref_algo_count").value
+    table = (AlgoT * n).in_dll(L, "hj_ref_algos")
+    names = [t.name.decode() for t in table]
+    assert len(names) == len(set(names)) == 20
+    for name in names:
+        out = C.c_int(-1)
+        assert L.hj_algo_from_name(name.encode(), C.byref(out)) == 0, name
+        assert hj.ALGOS[name] == out.value, name
+        assert getattr(L, name)  # exported under the reference's name

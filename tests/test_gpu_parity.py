@@ -233,3 +233,42 @@ def test_many_subchunks_with_duplicates(hj, oracle, cuda, algo):
     want = oracle.join(algo, R, S)
     assert run(hj, algo, R, S, cuda) == want
     assert run(hj, algo, R, S, cuda, bits=11, passes=2) == want
+
+
+@pytest.mark.parametrize("algo", ["phj_radix_sc", "phj_radix_hr", "phj_radix_hro", "phj_radix_bw_reg_hro",
+                                  "phj_asymm_radix_bc", "phj_asymm_radix_sc", "phj_asymm_radix_hr",
+                                  "phj_asymm_radix_bw_reg_hro"])
+def test_every_match_family(hj, oracle, cuda, algo):
+    # sc / hr / hro and the asymmetric names count every match, as bc does; every bit split (requested
+    # pass-1 bits are clamped to the split where each pass has 1..8 bits) gives the same partitions.
+    rng = np.random.default_rng(41)
+    nR, nS = 30_000, 90_000
+    R = np.empty((nR, 2), dtype=np.uint64)
+    S = np.empty((nS, 2), dtype=np.uint64)
+    R[:, 0] = rng.integers(0, 6000, nR, dtype=np.uint64)
+    S[:, 0] = rng.integers(0, 7000, nS, dtype=np.uint64)
+    R[:, 1] = rng.integers(0, 2**64 - 1, nR, dtype=np.uint64)
+    S[:, 1] = rng.integers(0, 2**64 - 1, nS, dtype=np.uint64)
+    R[::97, 0] = U64MAX
+    S[::89, 0] = U64MAX
+    want = oracle.join("phj_radix_bc", R, S)
+    for bits, passes, b1 in ((14, 2, None), (14, 2, 8), (14, 2, 3), (10, 2, 11), (9, 2, 1), (6, 1, None)):
+        assert run(hj, algo, R, S, cuda, bits=bits, passes=passes, bits_pass1=b1) == want, (bits, passes, b1)
+
+
+def test_asymm_cli_entry_point(hj, tmp_path):
+    # The reference-named entry point phj_asymm_radix_hr through the bin/main-style driver, with the
+    # pass-1 bits from the environment as the reference's NUM_RADIX_BITS_PASS1.
+    import os
+    import subprocess
+
+    R, S = hj.gen_dup_uniform(1 << 12, 1 << 14)
+    R.tofile(tmp_path / "r.bin")
+    S.tofile(tmp_path / "s.bin")
+    env = dict(os.environ, HJ_NUM_RADIX_BITS_PASS1="7", HJ_NUM_RADIX_BITS="12")
+    out = subprocess.run([str(hj.MAIN_PATH), "--algo=phj_asymm_radix_hr", f"--r={tmp_path / 'r.bin'}",
+                          f"--s={tmp_path / 's.bin'}",
+                          f"--nr={1 << 12}", f"--ns={1 << 14}"], capture_output=True, text=True, env=env)
+    assert out.returncode == 0, out.stderr
+    want = hj.join("phj_radix_bc", R, S)
+    assert f"matched_cnt: {want.matched_cnt}\tcheck_sum: {want.checksum}" in out.stdout

@@ -166,6 +166,35 @@ def test_oracle_matches_reference_binary_random(oracle):
     assert oracle.ref_join("nphj_lp", R, S, threads=1) == oracle.join("nphj_lp", R, S)
 
 
+@pytest.mark.skipif(not pathlib.Path("/root/reference/src").exists(), reason="reference sources absent")
+def test_reference_sc_hr_hro_and_asymm_equal_bc(oracle):
+    """The reference's separate-chaining, histogram-sorted and AVX-512 partition joins, and its
+    asymmetric-radix joins, return bc_join's count and checksum: the claim the library's phj_radix_sc /
+    _hr / _hro and phj_asymm_radix_* names rest on. Random keys (>= 1) with heavy duplication, probe
+    keys partly absent."""
+    if not (oracle.ref_available(1) and oracle.ref_available(2)):
+        pytest.skip("reference not built")
+    rng = np.random.default_rng(12)
+    R, S = _random_relations(rng, 4096, 16384, 900)
+    R[:, 0] = np.maximum(R[:, 0], 1)
+    S[:, 0] = np.maximum(S[:, 0], 1)
+    want = oracle.join("phj_radix_bc", R, S)
+    assert want[0] > S.shape[0]  # duplicates: more matches than probe tuples
+    for algo in ("phj_radix_sc", "phj_radix_hr", "phj_radix_hro"):
+        assert oracle.join(algo, R, S) == want
+        for bits, passes in ((6, 1), (10, 2)):
+            assert oracle.ref_join(algo, R, S, bits=bits, passes=passes, threads=4) == want, (algo, bits)
+    # The reference's asymmetric sc and hro joins crash (SIGSEGV) or miscount on some geometries (for
+    # example 12 bits over 4096 build tuples), so only its asymmetric bc and hr joins pin the split.
+    R2 = R.copy()
+    R2[:, 0] = rng.permutation(R.shape[0]).astype(np.uint64) + 1  # unique build keys, absent probe keys
+    want2 = oracle.join("phj_radix_bc", R2, S)
+    for algo in ("phj_asymm_radix_bc", "phj_asymm_radix_hr"):
+        for bits, bits1 in ((10, 7), (12, 11), (8, 11), (12, 6)):
+            assert oracle.ref_join(algo, R, S, bits=bits, passes=2, threads=4, bits1=bits1) == want, (algo, bits)
+            assert oracle.ref_join(algo, R2, S, bits=bits, passes=2, threads=4, bits1=bits1) == want2, (algo, bits)
+
+
 @pytest.mark.skipif(os.environ.get("HJ_SLOW") != "1", reason="minutes of CPU; set HJ_SLOW=1")
 def test_generator_reproduces_published_skew_and_dup_logs(hj, oracle):
     """Full-size replays of the reference's published skew/dup datasets (2^24 x 2^28)."""
