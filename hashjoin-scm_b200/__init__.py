@@ -52,9 +52,11 @@ STATUS = {
     7: "HJ_E_IO",
     8: "HJ_E_OVERFLOW",
     9: "HJ_E_BUDGET",
+    10: "HJ_E_CAPACITY",
+    11: "HJ_E_ROWID",
 }
 HJ_OK, HJ_E_INVAL, HJ_E_OOM, HJ_E_DEVICE, HJ_E_PROBE_LIMIT, HJ_E_TIMEOUT = 0, 1, 2, 3, 4, 5
-HJ_E_NOT_FOUND, HJ_E_IO, HJ_E_OVERFLOW, HJ_E_BUDGET = 6, 7, 8, 9
+HJ_E_NOT_FOUND, HJ_E_IO, HJ_E_OVERFLOW, HJ_E_BUDGET, HJ_E_CAPACITY, HJ_E_ROWID = 6, 7, 8, 9, 10, 11
 
 HJ_F_NO_TIMING = 0x1
 HJ_F_PINNED_HOST = 0x2
@@ -90,6 +92,7 @@ class Result(ctypes.Structure):
         ("phase", ctypes.c_double * 6),
         ("kernel_launches", ctypes.c_uint32),
         ("pad", ctypes.c_uint32),
+        ("retrieve", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -145,6 +148,10 @@ def lib() -> ctypes.CDLL:
     L.hj_join_ctx.restype = i32
     L.hj_join.argtypes = [i32, ctypes.POINTER(Params), vp, sz, vp, sz, ctypes.POINTER(Result)]
     L.hj_join.restype = i32
+    L.hj_join_mat_ctx.argtypes = [vp, i32, ctypes.POINTER(Params), vp, sz, vp, sz, vp, sz, ctypes.POINTER(Result)]
+    L.hj_join_mat_ctx.restype = i32
+    L.hj_join_mat.argtypes = [i32, ctypes.POINTER(Params), vp, sz, vp, sz, vp, sz, ctypes.POINTER(Result)]
+    L.hj_join_mat.restype = i32
     L.hj_gen_pkfk_uniform.argtypes = [sz, sz, ctypes.c_uint, i32, vp, vp]
     L.hj_gen_pkfk_uniform.restype = i32
     L.hj_gen_dup_uniform.argtypes = [sz, sz, ctypes.c_uint, vp, vp]
@@ -211,6 +218,37 @@ def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, o
         rc = L.hj_join_ctx(ctx.handle, a, ctypes.byref(p), pr, nr, ps, ns, ctypes.byref(res))
     else:
         rc = L.hj_join(a, ctypes.byref(p), pr, nr, ps, ns, ctypes.byref(res))
+    if check and rc != 0:
+        raise JoinError(rc, algo)
+    res.status = rc
+    return res
+
+
+def join_mat(algo: str, R, S, *, pairs=None, pair_cap: int | None = None, bits: int = 14, passes: int = 2,
+             device: int = 0, on_device: bool = False, stream: int | None = None, flags: int = 0,
+             load: float = 0.5, ctx: "Context | None" = None, check: bool = True,
+             bits_pass1: int | None = None) -> Result:
+    """Materialising join (the reference's ptr_* joins; a "ptr_" prefix on algo is accepted): one
+    (r.row_id, s.row_id) pair per match, checksum recomputed by the retrieve phase. pairs: None (kept
+    in library scratch), a CUDA tensor (n, 2) int64 when on_device, or a numpy (n, 2) uint64 array."""
+    L = lib()
+    name = algo[4:] if algo.startswith("ptr_") else algo
+    a = ALGOS[name]
+    if bits_pass1 is None:
+        bits_pass1 = ASYMM_DEFAULT_BITS_PASS1 if name.startswith("phj_asymm_radix") else 0
+    p = make_params(bits, passes, device, on_device, stream, flags, load, bits_pass1)
+    pr, nr = _ptr_len(R, on_device)
+    ps, ns = _ptr_len(S, on_device)
+    pp, cap = (None, 0)
+    if pairs is not None:
+        pp, cap = _ptr_len(pairs, on_device)
+        if pair_cap is not None:
+            cap = min(cap, pair_cap)
+    res = Result()
+    if ctx is not None:
+        rc = L.hj_join_mat_ctx(ctx.handle, a, ctypes.byref(p), pr, nr, ps, ns, pp, cap, ctypes.byref(res))
+    else:
+        rc = L.hj_join_mat(a, ctypes.byref(p), pr, nr, ps, ns, pp, cap, ctypes.byref(res))
     if check and rc != 0:
         raise JoinError(rc, algo)
     res.status = rc

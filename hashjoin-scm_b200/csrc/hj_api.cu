@@ -91,6 +91,8 @@ int map_error_bits(unsigned bits) {
     if (!bits) return HJ_OK;
     if (bits & hj::kErrSpinLimit) return HJ_E_TIMEOUT;
     if (bits & hj::kErrProbeLimit) return HJ_E_PROBE_LIMIT;
+    if (bits & hj::kErrOutput) return HJ_E_CAPACITY;
+    if (bits & hj::kErrRowId) return HJ_E_ROWID;
     return HJ_E_OVERFLOW;
 }
 
@@ -118,6 +120,8 @@ const char *hj_status_str(int s) {
         case HJ_E_IO: return "i/o error";
         case HJ_E_OVERFLOW: return "device bound check fired";
         case HJ_E_BUDGET: return "over the HBM budget";
+        case HJ_E_CAPACITY: return "the pair buffer is too small (matched_cnt = pairs needed)";
+        case HJ_E_ROWID: return "a matched row id is not a 1-based position of its relation";
         default: return "unknown status";
     }
 }
@@ -174,6 +178,7 @@ int hj_ctx_create(int device, hj_ctx_t **out) {
     CU_OR(cudaEventCreate(&c->ev_start), HJ_E_DEVICE);
     CU_OR(cudaEventCreate(&c->ev_mid), HJ_E_DEVICE);
     CU_OR(cudaEventCreate(&c->ev_end), HJ_E_DEVICE);
+    CU_OR(cudaEventCreate(&c->ev_ret), HJ_E_DEVICE);
     for (int i = 0; i <= HJ_PH_COUNT; i++) CU_OR(cudaEventCreate(&c->ev_ph[i]), HJ_E_DEVICE);
     CU_OR(cudaMallocHost(&c->acc_host, sizeof(JoinAccum)), HJ_E_OOM);
     c->tuner.nphj_max_table_bytes = 64e6;
@@ -195,6 +200,7 @@ int hj_ctx_destroy(hj_ctx_t *c) {
         cudaEventDestroy(c->ev_h2d);
         cudaEventDestroy(c->ev_start);
         cudaEventDestroy(c->ev_mid);
+        if (c->ev_ret) cudaEventDestroy(c->ev_ret);
         cudaEventDestroy(c->ev_end);
         for (int i = 0; i <= HJ_PH_COUNT; i++) cudaEventDestroy(c->ev_ph[i]);
         if (c->stream) cudaStreamDestroy(c->stream);
@@ -306,6 +312,150 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     out->kernel_launches = launches;
     out->status = map_error_bits(c->acc_host->error);
     return out->status;
+}
+
+// Materialising joins (the reference's ptr_* joins, src/algo/ptr_phj.c, ptr_nphj.c): the join writes
+// one (r.row_id, s.row_id) pair per match, and a retrieve phase recomputes the checksum by gathering
+// R[r_row_id - 1].row_id + S[s_row_id - 1].row_id (src/inc/utils.c:712-724).
+static int join_mat(hj_ctx *c, hj_algo_t algo, const hj_params_t &p, const hj_tuple_t *R, size_t nR,
+                    const hj_tuple_t *S, size_t nS, hj_pair_t *user_pairs, size_t user_cap,
+                    unsigned long long cap_guess, hj_result_t *out) {
+    hj::RadixGeom geom = {};
+    if (is_phj(algo)) {
+        int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &geom, p.radix_bits_pass1);
+        if (rc) return out->status = rc;
+        out->physical_passes = geom.passes;
+    }
+    if (nR == 0 || nS == 0) return out->status = HJ_OK;
+    const bool host_in = !p.inputs_on_device;
+    // Pairs land in the caller's device buffer, or in the arena (library-owned, or staged for a host
+    // buffer).
+    const bool pairs_in_arena = !user_pairs || host_in;
+    const unsigned long long cap = user_pairs ? (unsigned long long)user_cap : cap_guess;
+    size_t need = kAccBytes;
+    if (host_in) need += align256(nR * 16) + align256(nS * 16);
+    if (is_phj(algo))
+        need += hj::phj_scratch_bytes(geom, nR, nS, c->num_sms);
+    else
+        need += align256(hj::nphj_scratch_bytes(nR, p.table_load, true));
+    if (pairs_in_arena) need += align256(cap * 16);
+    int rc = ensure_arena(c, need);
+    if (rc) return out->status = rc;
+    cudaStream_t st = p.stream ? (cudaStream_t)p.stream : c->stream;
+    const bool timing = !(p.flags & HJ_F_NO_TIMING);
+    uint32_t launches = 0;
+
+    char *cur = c->arena;
+    JoinAccum *acc = reinterpret_cast<JoinAccum *>(cur);
+    cur += kAccBytes;
+    const ulonglong2 *dR = reinterpret_cast<const ulonglong2 *>(R);
+    const ulonglong2 *dS = reinterpret_cast<const ulonglong2 *>(S);
+    if (host_in) {
+        ulonglong2 *r = reinterpret_cast<ulonglong2 *>(cur);
+        cur += align256(nR * 16);
+        ulonglong2 *s = reinterpret_cast<ulonglong2 *>(cur);
+        cur += align256(nS * 16);
+        if (timing) CU_OR(cudaEventRecord(c->ev_h2d, st), out->status = HJ_E_DEVICE);
+        CU_OR(cudaMemcpyAsync(r, R, nR * 16, cudaMemcpyHostToDevice, st), out->status = HJ_E_DEVICE);
+        CU_OR(cudaMemcpyAsync(s, S, nS * 16, cudaMemcpyHostToDevice, st), out->status = HJ_E_DEVICE);
+        dR = r;
+        dS = s;
+    }
+    hj::MatOut mat;
+    mat.cap = cap;
+    if (pairs_in_arena) {
+        mat.pairs = reinterpret_cast<ulonglong2 *>(cur);
+        cur += align256(cap * 16);
+    } else {
+        mat.pairs = reinterpret_cast<ulonglong2 *>(user_pairs);
+    }
+    CU_OR(cudaMemsetAsync(acc, 0, sizeof(JoinAccum), st), out->status = HJ_E_DEVICE);
+    if (timing) CU_OR(cudaEventRecord(c->ev_start, st), out->status = HJ_E_DEVICE);
+    if (is_phj(algo)) {
+        hj::PhjScratch s;
+        hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s);
+        rc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
+                             timing ? c->ev_mid : nullptr, c->num_sms, nullptr, &launches, &mat);
+    } else {
+        const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
+        rc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
+                              timing ? c->ev_mid : nullptr, c->num_sms, nullptr, &launches, &mat);
+    }
+    if (!rc) {
+        if (timing) CU_OR(cudaEventRecord(c->ev_end, st), out->status = HJ_E_DEVICE);
+        rc = hj::mat_retrieve_enqueue(mat.pairs, &acc->pairs, cap, dR, nR, dS, nS, acc, st, c->num_sms);
+        launches++;
+    }
+    if (rc) {
+        cudaStreamSynchronize(st);
+        return out->status = rc;
+    }
+    if (timing) CU_OR(cudaEventRecord(c->ev_ret, st), out->status = HJ_E_DEVICE);
+    CU_OR(cudaMemcpyAsync(c->acc_host, acc, sizeof(JoinAccum), cudaMemcpyDeviceToHost, st),
+          out->status = HJ_E_DEVICE);
+    CU_OR(cudaStreamSynchronize(st), out->status = HJ_E_DEVICE);
+    const unsigned long long n = c->acc_host->pairs;
+    if (user_pairs && host_in && n)
+        CU_OR(cudaMemcpy(user_pairs, mat.pairs, (size_t)(n < cap ? n : cap) * 16, cudaMemcpyDeviceToHost),
+              out->status = HJ_E_DEVICE);
+    out->matched_cnt = n;
+    out->checksum = c->acc_host->checksum;
+    out->large_partitions = c->acc_host->large_parts;
+    if (timing) {
+        float a = 0, b = 0, r = 0, h = 0;
+        cudaEventElapsedTime(&a, c->ev_start, c->ev_mid);
+        cudaEventElapsedTime(&b, c->ev_mid, c->ev_end);
+        cudaEventElapsedTime(&r, c->ev_end, c->ev_ret);
+        if (host_in) cudaEventElapsedTime(&h, c->ev_h2d, c->ev_start);
+        out->buildpart = a * 1e-3;
+        out->probejoin = b * 1e-3;
+        out->retrieve = r * 1e-3;
+        // The reference's ptr joins time partition/build + join/probe + retrieve (ptr_phj.c:3094-3096).
+        out->total = out->buildpart + out->probejoin + out->retrieve;
+        out->h2d = h * 1e-3;
+    }
+    out->kernel_launches = launches;
+    out->status = map_error_bits(c->acc_host->error);
+    return out->status;
+}
+
+int hj_join_mat_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tuple_t *R, size_t nR,
+                    const hj_tuple_t *S, size_t nS, hj_pair_t *pairs, size_t pair_cap, hj_result_t *out) {
+    if (!c || !out || (int)algo < 0 || algo >= HJ_ALGO_COUNT) return HJ_E_INVAL;
+    memset(out, 0, sizeof(*out));
+    if ((nR && !R) || (nS && !S) || (pair_cap && !pairs)) return out->status = HJ_E_INVAL;
+    hj_params_t p;
+    resolve_params(pin, &p);
+    if (p.device != c->device) return out->status = HJ_E_INVAL;
+    DeviceGuard g(c->device);
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (pairs) return join_mat(c, algo, p, R, nR, S, nS, pairs, pair_cap, 0, out);
+    // Library-owned pairs: first-match joins write at most |S| pairs; for the others |S| is the
+    // guess (exact for PK-FK joins), and one rerun with the exact count follows when it was short.
+    int rc = join_mat(c, algo, p, R, nR, S, nS, nullptr, 0, nS ? nS : 1, out);
+    if (rc == HJ_E_CAPACITY) {
+        const unsigned long long need = out->matched_cnt;
+        memset(out, 0, sizeof(*out));
+        rc = join_mat(c, algo, p, R, nR, S, nS, nullptr, 0, need, out);
+    }
+    return rc;
+}
+
+int hj_join_mat(hj_algo_t algo, const hj_params_t *pin, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,
+                size_t nS, hj_pair_t *pairs, size_t pair_cap, hj_result_t *out) {
+    hj_params_t p;
+    resolve_params(pin, &p);
+    if (p.device < 0 || p.device >= 64) return HJ_E_INVAL;
+    hj_ctx *c;
+    {
+        std::lock_guard<std::mutex> lk(g_default_mu);
+        if (!g_default[p.device]) {
+            int rc = hj_ctx_create(p.device, &g_default[p.device]);
+            if (rc) return rc;
+        }
+        c = g_default[p.device];
+    }
+    return hj_join_mat_ctx(c, algo, &p, R, nR, S, nS, pairs, pair_cap, out);
 }
 
 int hj_join(hj_algo_t algo, const hj_params_t *pin, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,

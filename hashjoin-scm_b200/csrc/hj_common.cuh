@@ -19,6 +19,8 @@ enum : uint32_t {
     kErrSpinLimit = 1u << 1,    // a bounded wait (look-back, barrier) gave up
     kErrBounds = 1u << 2,       // a computed output index fell outside its buffer
     kErrCapacity = 1u << 3,     // a work list or table ran out of room
+    kErrOutput = 1u << 4,       // materialised pairs did not fit the output buffer
+    kErrRowId = 1u << 5,        // a materialised row id is not a 1-based position of its relation
 };
 
 // Device-resident per-join accumulators and flags (one 64-byte line).
@@ -28,7 +30,8 @@ struct JoinAccum {
     unsigned int error;
     unsigned int dup_flag;      // set by NPHJ builds that saw an equal key twice
     unsigned long long large_parts;
-    unsigned long long pad[4];
+    unsigned long long pairs;   // materialising joins: output slots reserved so far
+    unsigned long long pad[3];
 };
 
 __device__ __forceinline__ void set_error(unsigned int *err, uint32_t bit) { atomicOr(err, bit); }
@@ -120,6 +123,34 @@ __device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t *tm
     if (total) *total = tmp[nw - 1];
     __syncthreads();
     return warp_base + x - v;
+}
+
+// Output of a materialising join: (r.row_id, s.row_id) pairs; the slot cursor is JoinAccum::pairs.
+struct MatOut {
+    ulonglong2 *pairs;
+    unsigned long long cap;
+};
+
+// One round of a materialising probe loop: every thread of the block passes the number of pairs it
+// will write; returns the thread's first output slot. One global atomic per block and round. Must be
+// reached by all threads of the block (it contains barriers); s_base is one shared u64.
+__device__ __forceinline__ unsigned long long mat_reserve(uint32_t m, uint32_t *scan_tmp, unsigned long long *s_base,
+                                                          unsigned long long *cursor) {
+    uint32_t total = 0;
+    const uint32_t ex = block_excl_scan_u32(m, scan_tmp, &total);
+    if (threadIdx.x == 0) *s_base = total ? atomicAdd(cursor, (unsigned long long)total) : 0ull;
+    __syncthreads();
+    const unsigned long long b = *s_base + ex;
+    __syncthreads();
+    return b;
+}
+
+__device__ __forceinline__ void mat_put(const MatOut &o, unsigned long long slot, unsigned long long r_rid,
+                                        unsigned long long s_rid, unsigned int *err) {
+    if (slot < o.cap)
+        o.pairs[slot] = make_ulonglong2(r_rid, s_rid);
+    else
+        set_error(err, kErrOutput);
 }
 
 // Hash for the global (non-partitioned) tables: multiply-xorshift, then range reduction by the high

@@ -10,6 +10,7 @@
 namespace hj {
 
 struct JoinAccum;
+struct MatOut;
 
 // Geometry of the radix plan: total bits B split into physical passes of <= 8 bits each
 // (src/algo/params.h:34-35: FANOUT_PASS1 = 1 << (B/P), FANOUT_PASS2 = 1 << (B - B/P)).
@@ -76,14 +77,23 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
 // ev_mid, if non-null, is recorded between the partition phase and the join phase.
 // ph, if non-null, holds HJ_PH_COUNT + 1 events recorded at the phase boundaries; *launches receives
 // the number of kernels enqueued.
+// mat, if non-null, makes the join write one (r.row_id, s.row_id) pair per match into mat->pairs
+// (slots counted in acc->pairs) instead of summing row ids.
 int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                int num_sms, cudaEvent_t *ph, uint32_t *launches);
+                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr);
 
 // Non-partitioned joins on a global open-addressing table.
-size_t nphj_scratch_bytes(size_t nR, double load);
+// mat: as for phj_enqueue; a materialising join needs nphj_scratch_bytes(nR, load, true).
+size_t nphj_scratch_bytes(size_t nR, double load, bool mat = false);
 int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                 int num_sms, cudaEvent_t *ph, uint32_t *launches);
+                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr);
+
+// Checksum of materialised pairs as the reference's retrieve phase computes it: the wrapping sum of
+// R[r_row_id - 1].row_id + S[s_row_id - 1].row_id over the first n pairs (into acc->checksum).
+int mat_retrieve_enqueue(const ulonglong2 *pairs, const unsigned long long *n_dev, unsigned long long cap,
+                         const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, JoinAccum *acc,
+                         cudaStream_t st, int num_sms);
 
 }  // namespace hj

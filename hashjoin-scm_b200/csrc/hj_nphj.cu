@@ -43,6 +43,8 @@ struct NphjArgs {
     JoinAccum *acc;
     int lp;     // first match per probe tuple instead of all matches
     int skip0;  // key 0 never matches (the phj_radix_lp rule)
+    unsigned long long *side_pos;  // materialising joins: input positions of the side record's tuples
+    MatOut mat;
 };
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
@@ -53,7 +55,9 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
 __device__ __forceinline__ void nphj_insert(const NphjArgs &a, const tuple_v t, unsigned long long i, bool &seen_dup) {
     if (a.skip0 && t.x == 0) return;
     if (t.x == kEmpty) {
-        if (atomicAdd(&a.side->cnt, 1ull) >= 1ull) seen_dup = true;
+        const unsigned long long q = atomicAdd(&a.side->cnt, 1ull);
+        if (q >= 1ull) seen_dup = true;
+        if (a.side_pos) a.side_pos[q] = i;
         atomicAdd(&a.side->sum, (unsigned long long)t.y);
         atomicMin(&a.side->minpos, i);
         return;
@@ -175,6 +179,83 @@ __global__ void __launch_bounds__(256, 8) nphj_probe(NphjArgs a) {
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
 }
 
+// Materialising probe: block-wide rounds of one probe tuple per thread; each thread counts its matches,
+// the block reserves output slots with one atomic, then each thread walks again and writes its pairs.
+__global__ void __launch_bounds__(256) nphj_probe_mat(NphjArgs a) {
+    __shared__ uint32_t scan_tmp[32];
+    __shared__ unsigned long long s_base;
+    const bool lp = a.lp != 0, skip0 = a.skip0 != 0;
+    const bool first_only = lp || *reinterpret_cast<volatile unsigned int *>(&a.side->dup) == 0;
+    const unsigned long long side_cnt = a.side->cnt;
+    unsigned int *err = &a.acc->error;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long j0 = blockIdx.x * (unsigned long long)blockDim.x; j0 < a.nS; j0 += stride) {
+        const unsigned long long j = j0 + threadIdx.x;
+        const bool valid = j < a.nS;
+        const tuple_v sv = valid ? ld_stream(a.S + j) : make_ulonglong2(0, 0);
+        uint32_t m = 0;
+        unsigned long long h0 = 0;
+        const bool walk = valid && sv.x != kEmpty && !(skip0 && sv.x == 0);
+        if (valid && sv.x == kEmpty) {
+            m = side_cnt ? (lp ? 1u : (uint32_t)side_cnt) : 0u;
+        } else if (walk) {
+            h0 = table_hash(sv.x, a.cap);
+            unsigned long long h = h0;
+            for (unsigned long long steps = 0;;) {
+                const tuple_v e = ld_slot(a.table + h);
+                if (e.x == kEmpty) break;
+                if (e.x == sv.x) {
+                    m++;
+                    if (first_only) break;
+                }
+                if (++h == a.cap) h = 0;
+                if (++steps >= a.cap) {
+                    set_error(err, kErrProbeLimit);
+                    break;
+                }
+            }
+        }
+        unsigned long long o = mat_reserve(m, scan_tmp, &s_base, &a.acc->pairs);
+        if (!m) continue;
+        if (sv.x == kEmpty) {
+            if (lp)
+                mat_put(a.mat, o, a.R[a.side->minpos].y, sv.y, err);
+            else
+                for (unsigned long long q = 0; q < side_cnt; q++) mat_put(a.mat, o + q, a.R[a.side_pos[q]].y, sv.y, err);
+            continue;
+        }
+        unsigned long long h = h0;
+        for (unsigned long long steps = 0, w = 0; w < m && steps < a.cap; steps++) {
+            const tuple_v e = ld_slot(a.table + h);
+            if (e.x == kEmpty) break;
+            if (e.x == sv.x) mat_put(a.mat, o + w++, e.y, sv.y, err);
+            if (++h == a.cap) h = 0;
+        }
+    }
+}
+
+// Retrieve phase of the materialising joins (the reference's ptr_retrieve, src/inc/utils.c:712-724):
+// gather R[r_row_id - 1].row_id + S[s_row_id - 1].row_id for every pair and sum with wrap-around.
+__global__ void mat_retrieve(const ulonglong2 *__restrict__ pairs, const unsigned long long *n_dev,
+                             unsigned long long cap, const tuple_v *__restrict__ R, unsigned long long nR,
+                             const tuple_v *__restrict__ S, unsigned long long nS, JoinAccum *acc) {
+    unsigned long long n = *n_dev;
+    if (n > cap) n = cap;
+    unsigned long long sum = 0;
+    bool bad = false;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const ulonglong2 p = ld_stream(pairs + i);
+        if (p.x - 1 < nR && p.y - 1 < nS)
+            sum += R[p.x - 1].y + S[p.y - 1].y;
+        else
+            bad = true;
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(&acc->error, kErrRowId);
+    sum = warp_sum_u64(sum);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&acc->checksum, sum);
+}
+
 static unsigned long long nphj_cap(size_t nR, double load) {
     if (!(load > 0.05 && load < 0.95)) load = 0.5;
     unsigned long long cap = (unsigned long long)((double)nR / load) + 2;
@@ -182,8 +263,8 @@ static unsigned long long nphj_cap(size_t nR, double load) {
     return cap;
 }
 
-size_t nphj_scratch_bytes(size_t nR, double load) {
-    return (size_t)nphj_cap(nR, load) * 16 + 256;
+size_t nphj_scratch_bytes(size_t nR, double load, bool mat) {
+    return (size_t)nphj_cap(nR, load) * 16 + 256 + (mat ? (size_t)nR * 8 : 0);
 }
 
 #define HJ_CU(call)                                                                   \
@@ -197,9 +278,9 @@ size_t nphj_scratch_bytes(size_t nR, double load) {
 
 int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                 int num_sms, cudaEvent_t *ph, uint32_t *launches) {
+                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat) {
     const unsigned long long cap = nphj_cap(nR, load);
-    if (cap * 16 + 256 > table_bytes) return HJ_E_INVAL;
+    if (cap * 16 + 256 + (mat ? (unsigned long long)nR * 8 : 0ull) > table_bytes) return HJ_E_INVAL;
     NphjArgs a;
     a.R = R;
     a.S = S;
@@ -211,6 +292,9 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     a.acc = acc;
     a.lp = lp ? 1 : 0;
     a.skip0 = skip0 ? 1 : 0;
+    a.side_pos = mat ? reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(table) + cap * 16 + 256)
+                     : nullptr;
+    a.mat = mat ? *mat : MatOut{nullptr, 0};
     HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
     HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
     HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));
@@ -228,13 +312,24 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     if (ph) {
         for (int i = 1; i <= 4; i++) HJ_CU(cudaEventRecord(ph[i], st));
     }
-    nphj_probe<<<grid, 256, 0, st>>>(a);
+    if (mat)
+        nphj_probe_mat<<<grid, 256, 0, st>>>(a);
+    else
+        nphj_probe<<<grid, 256, 0, st>>>(a);
     HJ_CU(cudaGetLastError());
     if (ph) {
         HJ_CU(cudaEventRecord(ph[5], st));
         HJ_CU(cudaEventRecord(ph[6], st));
     }
     if (launches) *launches = lp ? 5u : 2u;
+    return HJ_OK;
+}
+
+int mat_retrieve_enqueue(const ulonglong2 *pairs, const unsigned long long *n_dev, unsigned long long cap,
+                         const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, JoinAccum *acc,
+                         cudaStream_t st, int num_sms) {
+    mat_retrieve<<<num_sms * 4, 256, 0, st>>>(pairs, n_dev, cap, R, nR, S, nS, acc);
+    HJ_CU(cudaGetLastError());
     return HJ_OK;
 }
 

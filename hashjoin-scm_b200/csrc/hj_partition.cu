@@ -839,6 +839,7 @@ struct JoinArgs {
     int lp;     // first match per probe tuple (lowest build position) instead of all matches
     int skip0;  // build tuples with key 0 never match (key 0 marks an empty slot in lp_join)
     JoinAccum *acc;
+    MatOut mat; // materialising joins (MAT kernels): where the (r.row_id, s.row_id) pairs go
 };
 
 constexpr int kHeadMax = 16384;  // next_pow_2(kSmemCap)
@@ -856,6 +857,9 @@ constexpr size_t kCompactSmem = (size_t)kCompactCap * (4 + 4 + 2 + 2);
 // Partition join with 4-byte keys (key >> bits) and 4-byte row ids in shared memory: 96 KiB per CTA,
 // two CTAs per SM, so one CTA's build overlaps the other's probe. Same results as join_small_kernel;
 // within a partition the low `bits` key bits are equal, so comparing key >> bits is comparing keys.
+// MAT: write one (r.row_id, s.row_id) pair per match (the ptr_* joins) instead of summing; the probe
+// then runs in block-wide rounds (count, reserve output slots, walk again and write).
+template <bool MAT>
 __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t *rkey = reinterpret_cast<uint32_t *>(smem);         // [kCompactCap]
@@ -864,6 +868,8 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
     uint16_t *nxt = head + kCompactCap;                            // [kCompactCap]
     __shared__ unsigned long long red[64];
     __shared__ uint32_t s_item;
+    __shared__ uint32_t scan_tmp[32];
+    __shared__ unsigned long long s_base;
     if (!compact_applies(a)) return;
     const int tid = threadIdx.x;
     unsigned int *err = &a.counters[kCtrErr];
@@ -906,6 +912,40 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
         __syncthreads();
         const tuple_v *S = a.finS + item.s_begin;
         const uint32_t ns = item.s_len;
+        if constexpr (MAT) {
+            for (uint32_t base = 0; base < ns; base += kCompactThreads) {
+                const uint32_t j = base + tid;
+                const tuple_v sv = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
+                const uint64_t khi = sv.x >> B;
+                uint32_t m = 0, best = 0;
+                if (j < ns) {
+                    uint32_t e = head[khi & hmask], steps = 0;
+                    while (e) {
+                        if ((uint64_t)rkey[e - 1] == khi) {
+                            if (!lp) m++;
+                            else if (best == 0 || e < best) best = e;
+                        }
+                        e = nxt[e - 1];
+                        if (++steps > nr) {
+                            set_error(err, kErrProbeLimit);
+                            break;
+                        }
+                    }
+                    if (lp) m = best ? 1u : 0u;
+                }
+                unsigned long long o = mat_reserve(m, scan_tmp, &s_base, &a.acc->pairs);
+                cnt += m;
+                if (lp) {
+                    if (best) mat_put(a.mat, o, rrid[best - 1], sv.y, err);
+                } else if (m) {
+                    uint32_t e = head[khi & hmask], steps = 0;
+                    while (e && steps++ <= nr) {
+                        if ((uint64_t)rkey[e - 1] == khi) mat_put(a.mat, o++, rrid[e - 1], sv.y, err);
+                        e = nxt[e - 1];
+                    }
+                }
+            }
+        } else
         for (uint32_t j0 = tid; j0 < ns; j0 += 4 * kCompactThreads) {
             tuple_v sv[4];
 #pragma unroll
@@ -946,6 +986,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
 }
 
+template <bool MAT>
 __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     tuple_v *rt = reinterpret_cast<tuple_v *>(smem);                      // [kSmemCap]
@@ -954,6 +995,8 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
     __shared__ __align__(8) unsigned long long bar_storage;
     __shared__ unsigned long long red[64];
     __shared__ uint32_t s_item;
+    __shared__ uint32_t scan_tmp[32];
+    __shared__ unsigned long long s_base;
     const int tid = threadIdx.x;
     const uint32_t bar = smem_u32(&bar_storage);
     unsigned int *err = &a.counters[kCtrErr];
@@ -1016,6 +1059,40 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
         // Probe.
         const tuple_v *S = a.finS + item.s_begin;
         const uint32_t ns = item.s_len;
+        if constexpr (MAT) {
+            for (uint32_t base = 0; base < ns; base += kJoinThreads) {
+                const uint32_t j = base + tid;
+                const tuple_v sv = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
+                const uint64_t k = sv.x;
+                uint32_t m = 0, best = 0;
+                if (j < ns) {
+                    uint32_t e = head[(k >> B) & hmask], steps = 0;
+                    while (e) {
+                        if (rt[e - 1].x == k) {
+                            if (!lp) m++;
+                            else if (best == 0 || e < best) best = e;
+                        }
+                        e = nxt[e - 1];
+                        if (++steps > nr) {
+                            set_error(err, kErrProbeLimit);
+                            break;
+                        }
+                    }
+                    if (lp) m = best ? 1u : 0u;
+                }
+                unsigned long long o = mat_reserve(m, scan_tmp, &s_base, &a.acc->pairs);
+                cnt += m;
+                if (lp) {
+                    if (best) mat_put(a.mat, o, rt[best - 1].y, sv.y, err);
+                } else if (m) {
+                    uint32_t e = head[(k >> B) & hmask], steps = 0;
+                    while (e && steps++ <= nr) {
+                        if (rt[e - 1].x == k) mat_put(a.mat, o++, rt[e - 1].y, sv.y, err);
+                        e = nxt[e - 1];
+                    }
+                }
+            }
+        } else
         for (uint32_t j0 = tid; j0 < ns; j0 += 4 * kJoinThreads) {
             tuple_v s[4];
 #pragma unroll
@@ -1093,11 +1170,58 @@ __global__ void join_large_build(JoinArgs a) {
     }
 }
 
+template <bool MAT>
 __global__ void join_large_probe(JoinArgs a) {
     __shared__ unsigned long long red[64];
+    __shared__ uint32_t scan_tmp[32];
+    __shared__ unsigned long long s_base;
     const int nl = (int)a.counters[kCtrNLarge];
     const uint64_t total = ld_u64_pair(&a.counters[kCtrLargeS]);
     unsigned long long cnt = 0, sum = 0;
+    if constexpr (MAT) {
+        unsigned int *err = &a.counters[kCtrErr];
+        // Block-uniform rounds over the flattened probe tuples of all large partitions.
+        for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x; g0 < total; g0 += (uint64_t)gridDim.x * blockDim.x) {
+            const uint64_t g = g0 + threadIdx.x;
+            uint32_t m = 0, best = 0, e0 = 0;
+            tuple_v s = make_ulonglong2(0, 0);
+            const LargePart *Lp = nullptr;
+            if (g < total) {
+                Lp = &a.large[find_large(a.large, nl, g, false)];
+                s = ld_stream(a.finS + Lp->s_begin + (g - Lp->s_flat));
+                const uint32_t *head = a.large_table + Lp->table_off;
+                const uint32_t *nxt = head + (1ull << Lp->nb_log);
+                const tuple_v *rr = a.finR + Lp->r_begin;
+                e0 = head[(s.x >> a.bits) & ((1ull << Lp->nb_log) - 1)];
+                uint64_t steps = 0;
+                for (uint32_t e = e0; e;) {
+                    if (rr[e - 1].x == s.x) {
+                        if (!a.lp) m++;
+                        else if (best == 0 || e < best) best = e;
+                    }
+                    e = nxt[e - 1];
+                    if (++steps > Lp->r_len) {
+                        set_error(err, kErrProbeLimit);
+                        break;
+                    }
+                }
+                if (a.lp) m = best ? 1u : 0u;
+            }
+            unsigned long long o = mat_reserve(m, scan_tmp, &s_base, &a.acc->pairs);
+            cnt += m;
+            if (m) {
+                const uint32_t *nxt = a.large_table + Lp->table_off + (1ull << Lp->nb_log);
+                const tuple_v *rr = a.finR + Lp->r_begin;
+                if (a.lp) {
+                    mat_put(a.mat, o, rr[best - 1].y, s.y, err);
+                } else {
+                    uint64_t steps = 0;
+                    for (uint32_t e = e0; e && steps++ <= Lp->r_len; e = nxt[e - 1])
+                        if (rr[e - 1].x == s.x) mat_put(a.mat, o++, rr[e - 1].y, s.y, err);
+                }
+            }
+        }
+    } else
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const int l = find_large(a.large, nl, g, false);
@@ -1284,8 +1408,11 @@ int phj_prepare_device() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
-    HJ_CU(cudaFuncSetAttribute(join_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
-    HJ_CU(cudaFuncSetAttribute(join_compact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HJ_CU(cudaFuncSetAttribute(join_small_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
+    HJ_CU(cudaFuncSetAttribute(join_small_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
+    HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kCompactSmem));
+    HJ_CU(cudaFuncSetAttribute(join_compact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kCompactSmem));
     g_attr_done[cur_dev] = true;
     return HJ_OK;
@@ -1293,7 +1420,7 @@ int phj_prepare_device() {
 
 int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                int num_sms, cudaEvent_t *ph, uint32_t *launches) {
+                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat) {
     uint32_t nlaunch = 0;
 #define HJ_PH(i) \
     if (ph) HJ_CU(cudaEventRecord(ph[i], st))
@@ -1401,13 +1528,22 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     ja.lp = lp ? 1 : 0;
     ja.skip0 = skip0 ? 1 : 0;
     ja.acc = acc;
-    join_compact_kernel<<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
-    join_small_kernel<<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
+    ja.mat = mat ? *mat : MatOut{nullptr, 0};
+    if (mat) {
+        join_compact_kernel<true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+        join_small_kernel<true><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
+    } else {
+        join_compact_kernel<false><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+        join_small_kernel<false><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
+    }
     HJ_CU(cudaGetLastError());
     HJ_PH(5);
     join_large_clear<<<num_sms * 2, 256, 0, st>>>(ja);
     join_large_build<<<num_sms * 2, 256, 0, st>>>(ja);
-    join_large_probe<<<num_sms * 2, 256, 0, st>>>(ja);
+    if (mat)
+        join_large_probe<true><<<num_sms * 2, 256, 0, st>>>(ja);
+    else
+        join_large_probe<false><<<num_sms * 2, 256, 0, st>>>(ja);
     copy_error<<<1, 32, 0, st>>>(s.counters, acc);
     HJ_CU(cudaGetLastError());
     HJ_PH(6);

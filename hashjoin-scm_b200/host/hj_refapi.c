@@ -87,7 +87,7 @@ int hj_ref_last_result(hj_result_t *out) {
 }
 
 /* Shared body of the entry points: the part of join_init_run / nphj_sc outside the thread pools. */
-static void run_ref_p1(hj_algo_t algo, int bits_pass1, const datameta_t datameta, timekeeper_t *const tk) {
+static void run_ref_any(hj_algo_t algo, int bits_pass1, int mat, const datameta_t datameta, timekeeper_t *const tk) {
     char prefix[4096], rpath[8192], spath[8192];
     hj_params_t p;
     current_config(prefix, sizeof(prefix), &p);
@@ -104,7 +104,7 @@ static void run_ref_p1(hj_algo_t algo, int bits_pass1, const datameta_t datameta
     int rc = (!R || !S) ? HJ_E_OOM : HJ_OK;
     if (!rc) rc = hj_load_bin(rpath, nR, R);
     if (!rc) rc = hj_load_bin(spath, nS, S);
-    if (!rc) rc = hj_join(algo, &p, R, nR, S, nS, &res);
+    if (!rc) rc = mat ? hj_join_mat(algo, &p, R, nR, S, nS, NULL, 0, &res) : hj_join(algo, &p, R, nR, S, nS, &res);
     free(R);
     free(S);
     res.status = rc;
@@ -120,10 +120,12 @@ static void run_ref_p1(hj_algo_t algo, int bits_pass1, const datameta_t datameta
     tk->total = res.total;
 }
 
-static void run_ref(hj_algo_t algo, const datameta_t d, timekeeper_t *const tk) { run_ref_p1(algo, 0, d, tk); }
+static void run_ref(hj_algo_t algo, const datameta_t d, timekeeper_t *const tk) { run_ref_any(algo, 0, 0, d, tk); }
 static void run_asymm(hj_algo_t algo, const datameta_t d, timekeeper_t *const tk) {
-    run_ref_p1(algo, asymm_bits_pass1(), d, tk);
+    run_ref_any(algo, asymm_bits_pass1(), 0, d, tk);
 }
+/* ptr_* joins: materialise (r_row_id, s_row_id) pairs, then retrieve the checksum (hj_join_mat). */
+static void run_ptr(hj_algo_t algo, const datameta_t d, timekeeper_t *const tk) { run_ref_any(algo, 0, 1, d, tk); }
 
 void nphj_sc(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_NPHJ_SC, d, tk); }
 void nphj_lp(const datameta_t d, timekeeper_t *const tk) { run_ref(HJ_ALGO_NPHJ_LP, d, tk); }
@@ -145,6 +147,16 @@ void phj_asymm_radix_bw_reg_bc(const datameta_t d, timekeeper_t *const tk) { run
 void phj_asymm_radix_bw_reg_sc(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_SC, d, tk); }
 void phj_asymm_radix_bw_reg_hr(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_HR, d, tk); }
 void phj_asymm_radix_bw_reg_hro(const datameta_t d, timekeeper_t *const tk) { run_asymm(HJ_ALGO_PHJ_RADIX_HRO, d, tk); }
+void ptr_nphj_sc(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_NPHJ_SC, d, tk); }
+void ptr_nphj_lp(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_NPHJ_LP, d, tk); }
+void ptr_phj_radix_bc(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_BC, d, tk); }
+void ptr_phj_radix_sc(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_SC, d, tk); }
+void ptr_phj_radix_lp(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_LP, d, tk); }
+void ptr_phj_radix_hr(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_HR, d, tk); }
+void ptr_phj_radix_bw_reg_bc(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_BC, d, tk); }
+void ptr_phj_radix_bw_reg_sc(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_SC, d, tk); }
+void ptr_phj_radix_bw_reg_lp(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_LP, d, tk); }
+void ptr_phj_radix_bw_reg_hr(const datameta_t d, timekeeper_t *const tk) { run_ptr(HJ_ALGO_PHJ_RADIX_HR, d, tk); }
 
 const algo_t hj_ref_algos[] = {
     {"nphj_sc", nphj_sc},
@@ -167,6 +179,16 @@ const algo_t hj_ref_algos[] = {
     {"phj_asymm_radix_bw_reg_sc", phj_asymm_radix_bw_reg_sc},
     {"phj_asymm_radix_bw_reg_hr", phj_asymm_radix_bw_reg_hr},
     {"phj_asymm_radix_bw_reg_hro", phj_asymm_radix_bw_reg_hro},
+    {"ptr_nphj_sc", ptr_nphj_sc},
+    {"ptr_nphj_lp", ptr_nphj_lp},
+    {"ptr_phj_radix_bc", ptr_phj_radix_bc},
+    {"ptr_phj_radix_sc", ptr_phj_radix_sc},
+    {"ptr_phj_radix_lp", ptr_phj_radix_lp},
+    {"ptr_phj_radix_hr", ptr_phj_radix_hr},
+    {"ptr_phj_radix_bw_reg_bc", ptr_phj_radix_bw_reg_bc},
+    {"ptr_phj_radix_bw_reg_sc", ptr_phj_radix_bw_reg_sc},
+    {"ptr_phj_radix_bw_reg_lp", ptr_phj_radix_bw_reg_lp},
+    {"ptr_phj_radix_bw_reg_hr", ptr_phj_radix_bw_reg_hr},
 };
 const int hj_ref_algo_count = (int)(sizeof(hj_ref_algos) / sizeof(hj_ref_algos[0]));
 

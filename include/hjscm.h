@@ -72,7 +72,10 @@ enum {
     HJ_E_NOT_FOUND = 6,   /* unknown --algo name */
     HJ_E_IO = 7,          /* a relation file could not be read */
     HJ_E_OVERFLOW = 8,    /* a device-side bound check fired (internal error, results invalid) */
-    HJ_E_BUDGET = 9       /* a request does not fit the serving HBM budget */
+    HJ_E_BUDGET = 9,      /* a request does not fit the serving HBM budget */
+    HJ_E_CAPACITY = 10,   /* materialising join: the pair buffer is too small; matched_cnt = pairs needed */
+    HJ_E_ROWID = 11       /* materialising join: a matched row id is not a 1-based position of its
+                             relation, so the retrieve phase cannot gather it */
 };
 
 /* Runtime knobs. The reference fixes these at compile time with -D (CMakeLists.txt:51-373,
@@ -118,6 +121,7 @@ typedef struct {
     double phase[HJ_PH_COUNT]; /* per-kernel-group seconds (HJ_F_PHASE_TIMES) */
     uint32_t kernel_launches;  /* kernels this join launched */
     uint32_t pad;
+    double retrieve;           /* materialising joins: seconds of the retrieve phase (included in total) */
 } hj_result_t;
 
 typedef struct hj_ctx hj_ctx_t;
@@ -151,6 +155,22 @@ int hj_join_ctx(hj_ctx_t *ctx, hj_algo_t algo, const hj_params_t *p,
 /* hj_join_ctx on a per-device default context (created on first use, guarded by a mutex). */
 int hj_join(hj_algo_t algo, const hj_params_t *p,
             const hj_tuple_t *R, size_t nR, const hj_tuple_t *S, size_t nS, hj_result_t *out);
+
+/* Materialising join: the reference's ptr_* joins (src/algo/ptr_phj.c:3100-3114 ptr_phj_radix_bc/lp/
+ * sc/hr, src/algo/ptr_nphj.c ptr_nphj_sc/lp). The join writes one hj_pair_t {r.row_id, s.row_id} per
+ * match (one per matched probe tuple for the lp algorithms), then a retrieve phase recomputes the
+ * checksum as the wrapping sum of R[r_row_id - 1].row_id + S[s_row_id - 1].row_id
+ * (src/inc/utils.c:712-724), so row ids must be 1-based positions (the reference's payload_gen_*
+ * data; otherwise HJ_E_ROWID). out->total = buildpart + probejoin + retrieve, as the reference times
+ * its ptr joins (src/algo/ptr_phj.c:3094-3096).
+ *   pairs: NULL keeps the pairs in library scratch (only the count and checksum come back); else
+ *   the caller's buffer of pair_cap pairs, in device memory when p->inputs_on_device, else in host
+ *   memory (copied back after the join). Pair order is unspecified. If pair_cap is too small the call
+ *   returns HJ_E_CAPACITY with out->matched_cnt = the pairs needed. */
+int hj_join_mat_ctx(hj_ctx_t *ctx, hj_algo_t algo, const hj_params_t *p, const hj_tuple_t *R, size_t nR,
+                    const hj_tuple_t *S, size_t nS, hj_pair_t *pairs, size_t pair_cap, hj_result_t *out);
+int hj_join_mat(hj_algo_t algo, const hj_params_t *p, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,
+                size_t nS, hj_pair_t *pairs, size_t pair_cap, hj_result_t *out);
 
 /* ----------------------------------------------------------------------------------------------
  * Data generation. The seeded generators replay the reference's src/gen.c exactly (glibc srand/rand,

@@ -86,6 +86,18 @@ void phj_asymm_radix_bw_reg_bc(const datameta_t datameta, timekeeper_t *const ti
 void phj_asymm_radix_bw_reg_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
 void phj_asymm_radix_bw_reg_hr(const datameta_t datameta, timekeeper_t *const timekeeper);
 void phj_asymm_radix_bw_reg_hro(const datameta_t datameta, timekeeper_t *const timekeeper);
+/* Materialising joins (src/main.c:87-92, 119-122): pairs, then the retrieve checksum (hj_join_mat);
+ * the timekeeper's total includes the retrieve phase. */
+void ptr_nphj_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_nphj_lp(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_bc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_lp(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_hr(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_bw_reg_bc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_bw_reg_sc(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_bw_reg_lp(const datameta_t datameta, timekeeper_t *const timekeeper);
+void ptr_phj_radix_bw_reg_hr(const datameta_t datameta, timekeeper_t *const timekeeper);
 
 /* The dispatch table (src/main.c:72-143 restricted to the names above) and its length. */
 extern const algo_t hj_ref_algos[];

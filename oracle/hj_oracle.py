@@ -216,6 +216,37 @@ def join(mode_or_algo, R: np.ndarray, S: np.ndarray) -> tuple[int, int]:
     return c.value, s.value
 
 
+def join_pairs(mode_or_algo, R: np.ndarray, S: np.ndarray) -> np.ndarray:
+    """The (r.row_id, s.row_id) pairs of a join from its definition, sorted (n, 2) uint64: what the
+    reference's ptr_* joins write into their materialisation buffer (src/algo/ptr_phj.c:689-783, one
+    pair per match; lp joins: one pair per probe tuple with a match, the first build tuple in input
+    order, key 0 never matching for phj_radix_lp)."""
+    mode = MODE_OF_ALGO[mode_or_algo[4:] if isinstance(mode_or_algo, str) and mode_or_algo.startswith("ptr_")
+                        else mode_or_algo] if isinstance(mode_or_algo, str) else mode_or_algo
+    R, S = _arr(R), _arr(S)
+    rpos = np.arange(R.shape[0])
+    if mode == FIRST:
+        rpos = rpos[R[:, 0] != 0]  # key 0 is an empty slot of lp_join (src/algo/phj.c:614)
+    rk = R[rpos, 0]
+    order = np.argsort(rk, kind="stable")  # equal keys stay in input order
+    rks, rps = rk[order], rpos[order]
+    sk = S[:, 0]
+    lo = np.searchsorted(rks, sk, "left")
+    hi = np.searchsorted(rks, sk, "right")
+    if mode == ALL:
+        cnt = hi - lo
+        s_idx = np.repeat(np.arange(S.shape[0]), cnt)
+        start = np.repeat(lo, cnt)
+        within = np.arange(s_idx.shape[0]) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+        r_idx = rps[start + within]
+    else:
+        m = hi > lo
+        s_idx = np.nonzero(m)[0]
+        r_idx = rps[lo[m]]
+    out = np.stack([R[r_idx, 1], S[s_idx, 1]], axis=1).astype(np.uint64)
+    return out[np.lexsort((out[:, 1], out[:, 0]))]
+
+
 def join_dense(mode_or_algo, R: np.ndarray, S: np.ndarray, max_key: int) -> tuple[int, int]:
     mode = MODE_OF_ALGO[mode_or_algo] if isinstance(mode_or_algo, str) else mode_or_algo
     R, S = _arr(R), _arr(S)

@@ -6,7 +6,9 @@
  * reference functions unmodified:
  *   hjref_pN --algo=NAME --prefix=DIR --r=REL --s=REL --nr=N --ns=M [--bits=14] [--bits1=11]
  *            [--threads=T] [--trials=K]
- *       NAME: nphj_sc, nphj_lp, phj_radix_{bc,lp,sc,hr,hro}, and with N = 2 phj_asymm_radix_{bc,sc,hr,hro}
+ *       NAME: nphj_sc, nphj_lp, phj_radix_{bc,lp,sc,hr,hro}, ptr_nphj_{sc,lp}, ptr_phj_radix_{bc,lp,sc,hr}
+ *       (materialising joins: pairs, then the retrieve checksum), and with N = 2
+ *       phj_asymm_radix_{bc,sc,hr,hro}
  *       (pass-1 bits --bits1, NUM_RADIX_BITS_PASS1, default 11 and at most --bits as
  *       src/algo/phj_asymm_radix.h:10-17 rules).
  *       Each trial prints the reference's "matched_cnt: ..\tcheck_sum: .." line, then
@@ -39,6 +41,12 @@ void phj_radix_lp(const datameta_t, timekeeper_t *const);
 void phj_radix_sc(const datameta_t, timekeeper_t *const);
 void phj_radix_hr(const datameta_t, timekeeper_t *const);
 void phj_radix_hro(const datameta_t, timekeeper_t *const);
+void ptr_nphj_sc(const datameta_t, timekeeper_t *const);
+void ptr_nphj_lp(const datameta_t, timekeeper_t *const);
+void ptr_phj_radix_bc(const datameta_t, timekeeper_t *const);
+void ptr_phj_radix_lp(const datameta_t, timekeeper_t *const);
+void ptr_phj_radix_sc(const datameta_t, timekeeper_t *const);
+void ptr_phj_radix_hr(const datameta_t, timekeeper_t *const);
 #if NUM_PASSES == 2
 void phj_asymm_radix_bc(const datameta_t, timekeeper_t *const);
 void phj_asymm_radix_sc(const datameta_t, timekeeper_t *const);
@@ -98,6 +106,12 @@ int main(int argc, char **argv) {
     else if (algo && !strcmp(algo, "phj_radix_sc")) fn = phj_radix_sc;
     else if (algo && !strcmp(algo, "phj_radix_hr")) fn = phj_radix_hr;
     else if (algo && !strcmp(algo, "phj_radix_hro")) fn = phj_radix_hro;
+    else if (algo && !strcmp(algo, "ptr_nphj_sc")) fn = ptr_nphj_sc;
+    else if (algo && !strcmp(algo, "ptr_nphj_lp")) fn = ptr_nphj_lp;
+    else if (algo && !strcmp(algo, "ptr_phj_radix_bc")) fn = ptr_phj_radix_bc;
+    else if (algo && !strcmp(algo, "ptr_phj_radix_lp")) fn = ptr_phj_radix_lp;
+    else if (algo && !strcmp(algo, "ptr_phj_radix_sc")) fn = ptr_phj_radix_sc;
+    else if (algo && !strcmp(algo, "ptr_phj_radix_hr")) fn = ptr_phj_radix_hr;
 #if NUM_PASSES == 2
     else if (algo && !strcmp(algo, "phj_asymm_radix_bc")) fn = phj_asymm_radix_bc;
     else if (algo && !strcmp(algo, "phj_asymm_radix_sc")) fn = phj_asymm_radix_sc;

@@ -195,6 +195,25 @@ def test_reference_sc_hr_hro_and_asymm_equal_bc(oracle):
             assert oracle.ref_join(algo, R2, S, bits=bits, passes=2, threads=4, bits1=bits1) == want2, (algo, bits)
 
 
+@pytest.mark.skipif(not pathlib.Path("/root/reference/src").exists(), reason="reference sources absent")
+def test_reference_ptr_joins_equal_definition(hj, oracle):
+    """The reference's materialising joins (pairs, then the retrieve checksum) on payload PK-FK data equal
+    the definition, and so does the pairs oracle. One thread: the reference sizes each thread's pair
+    buffer |S| * 1.2 / threads (src/algo/ptr_phj.h:144-145), which overflows (SIGSEGV / heap corruption)
+    when the matches are spread unevenly over threads or exceed 1.2 per probe tuple."""
+    if not (oracle.ref_available(1) and oracle.ref_available(2)):
+        pytest.skip("reference not built")
+    R, S = hj.gen_pkfk_uniform(4096, 16384, payload=True)
+    for algo in ("ptr_phj_radix_bc", "ptr_phj_radix_sc", "ptr_phj_radix_hr", "ptr_phj_radix_lp", "ptr_nphj_sc",
+                 "ptr_nphj_lp"):
+        want = oracle.join(algo[4:], R, S)
+        P = oracle.join_pairs(algo, R, S)
+        assert P.shape[0] == want[0]
+        assert int((P[:, 0].astype(object) + P[:, 1].astype(object)).sum()) % 2**64 == want[1]
+        for bits, passes in ((6, 1), (10, 2)):
+            assert oracle.ref_join(algo, R, S, bits=bits, passes=passes, threads=1) == want, (algo, bits)
+
+
 @pytest.mark.skipif(os.environ.get("HJ_SLOW") != "1", reason="minutes of CPU; set HJ_SLOW=1")
 def test_generator_reproduces_published_skew_and_dup_logs(hj, oracle):
     """Full-size replays of the reference's published skew/dup datasets (2^24 x 2^28)."""
