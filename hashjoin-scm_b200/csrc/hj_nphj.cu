@@ -243,13 +243,28 @@ __global__ void mat_retrieve(const ulonglong2 *__restrict__ pairs, const unsigne
     if (n > cap) n = cap;
     unsigned long long sum = 0;
     bool bad = false;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        const ulonglong2 p = ld_stream(pairs + i);
-        if (p.x - 1 < nR && p.y - 1 < nS)
-            sum += R[p.x - 1].y + S[p.y - 1].y;
-        else
-            bad = true;
+    // Eight pairs per thread and step: their 16 gathers are all in flight before any is summed.
+    constexpr int U = 8;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < n;
+         i0 += U * stride) {
+        ulonglong2 p[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned long long i = i0 + u * stride;
+            p[u] = i < n ? ld_stream(pairs + i) : make_ulonglong2(0, 0);
+        }
+        unsigned long long rv[U], sv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool live = i0 + u * stride < n;
+            const bool ok = p[u].x - 1 < nR && p[u].y - 1 < nS;
+            bad = bad || (live && !ok);
+            rv[u] = live && ok ? __ldg(&R[p[u].x - 1].y) : 0ull;
+            sv[u] = live && ok ? __ldg(&S[p[u].y - 1].y) : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) sum += rv[u] + sv[u];
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(&acc->error, kErrRowId);
     sum = warp_sum_u64(sum);
@@ -328,7 +343,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
 int mat_retrieve_enqueue(const ulonglong2 *pairs, const unsigned long long *n_dev, unsigned long long cap,
                          const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, JoinAccum *acc,
                          cudaStream_t st, int num_sms) {
-    mat_retrieve<<<num_sms * 4, 256, 0, st>>>(pairs, n_dev, cap, R, nR, S, nS, acc);
+    mat_retrieve<<<num_sms * 8, 256, 0, st>>>(pairs, n_dev, cap, R, nR, S, nS, acc);
     HJ_CU(cudaGetLastError());
     return HJ_OK;
 }

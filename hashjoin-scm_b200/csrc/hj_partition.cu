@@ -913,17 +913,25 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
         const tuple_v *S = a.finS + item.s_begin;
         const uint32_t ns = item.s_len;
         if constexpr (MAT) {
-            for (uint32_t base = 0; base < ns; base += kCompactThreads) {
-                const uint32_t j = base + tid;
-                const tuple_v sv = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
-                const uint64_t khi = sv.x >> B;
-                uint32_t m = 0, best = 0;
-                if (j < ns) {
+            constexpr int U = 4;  // probe tuples per thread and round: loads in flight, fewer rounds
+            for (uint32_t base = 0; base < ns; base += U * kCompactThreads) {
+                tuple_v sv[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const uint32_t j = base + u * kCompactThreads + tid;
+                    sv[u] = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
+                }
+                uint32_t mm[U], best[U], m = 0;
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    mm[u] = best[u] = 0;
+                    if (base + u * kCompactThreads + tid >= ns) continue;
+                    const uint64_t khi = sv[u].x >> B;
                     uint32_t e = head[khi & hmask], steps = 0;
                     while (e) {
                         if ((uint64_t)rkey[e - 1] == khi) {
-                            if (!lp) m++;
-                            else if (best == 0 || e < best) best = e;
+                            if (!lp) mm[u]++;
+                            else if (best[u] == 0 || e < best[u]) best[u] = e;
                         }
                         e = nxt[e - 1];
                         if (++steps > nr) {
@@ -931,16 +939,22 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                             break;
                         }
                     }
-                    if (lp) m = best ? 1u : 0u;
+                    if (lp) mm[u] = best[u] ? 1u : 0u;
+                    m += mm[u];
                 }
                 unsigned long long o = mat_reserve(m, scan_tmp, &s_base, &a.acc->pairs);
                 cnt += m;
-                if (lp) {
-                    if (best) mat_put(a.mat, o, rrid[best - 1], sv.y, err);
-                } else if (m) {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (!mm[u]) continue;
+                    if (lp) {
+                        mat_put(a.mat, o++, rrid[best[u] - 1], sv[u].y, err);
+                        continue;
+                    }
+                    const uint64_t khi = sv[u].x >> B;
                     uint32_t e = head[khi & hmask], steps = 0;
                     while (e && steps++ <= nr) {
-                        if ((uint64_t)rkey[e - 1] == khi) mat_put(a.mat, o++, rrid[e - 1], sv.y, err);
+                        if ((uint64_t)rkey[e - 1] == khi) mat_put(a.mat, o++, rrid[e - 1], sv[u].y, err);
                         e = nxt[e - 1];
                     }
                 }
@@ -1060,17 +1074,25 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
         const tuple_v *S = a.finS + item.s_begin;
         const uint32_t ns = item.s_len;
         if constexpr (MAT) {
-            for (uint32_t base = 0; base < ns; base += kJoinThreads) {
-                const uint32_t j = base + tid;
-                const tuple_v sv = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
-                const uint64_t k = sv.x;
-                uint32_t m = 0, best = 0;
-                if (j < ns) {
+            constexpr int U = 4;  // probe tuples per thread and round
+            for (uint32_t base = 0; base < ns; base += U * kJoinThreads) {
+                tuple_v sv[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const uint32_t j = base + u * kJoinThreads + tid;
+                    sv[u] = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
+                }
+                uint32_t mm[U], best[U], m = 0;
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    mm[u] = best[u] = 0;
+                    if (base + u * kJoinThreads + tid >= ns) continue;
+                    const uint64_t k = sv[u].x;
                     uint32_t e = head[(k >> B) & hmask], steps = 0;
                     while (e) {
                         if (rt[e - 1].x == k) {
-                            if (!lp) m++;
-                            else if (best == 0 || e < best) best = e;
+                            if (!lp) mm[u]++;
+                            else if (best[u] == 0 || e < best[u]) best[u] = e;
                         }
                         e = nxt[e - 1];
                         if (++steps > nr) {
@@ -1078,16 +1100,22 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
                             break;
                         }
                     }
-                    if (lp) m = best ? 1u : 0u;
+                    if (lp) mm[u] = best[u] ? 1u : 0u;
+                    m += mm[u];
                 }
                 unsigned long long o = mat_reserve(m, scan_tmp, &s_base, &a.acc->pairs);
                 cnt += m;
-                if (lp) {
-                    if (best) mat_put(a.mat, o, rt[best - 1].y, sv.y, err);
-                } else if (m) {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (!mm[u]) continue;
+                    if (lp) {
+                        mat_put(a.mat, o++, rt[best[u] - 1].y, sv[u].y, err);
+                        continue;
+                    }
+                    const uint64_t k = sv[u].x;
                     uint32_t e = head[(k >> B) & hmask], steps = 0;
                     while (e && steps++ <= nr) {
-                        if (rt[e - 1].x == k) mat_put(a.mat, o++, rt[e - 1].y, sv.y, err);
+                        if (rt[e - 1].x == k) mat_put(a.mat, o++, rt[e - 1].y, sv[u].y, err);
                         e = nxt[e - 1];
                     }
                 }
