@@ -34,6 +34,8 @@ inline bool algo_skip0(hj_algo_t a) { return a == HJ_ALGO_PHJ_RADIX_LP; }
 // Tile and work-item constants shared by the plan and the kernels.
 constexpr int kScatterThreads = 256;
 constexpr int kScatterItems = 8;
+constexpr int kScatterBufs = 2;       // tile buffers per CTA (2: double-buffered TMA loads)
+constexpr int kScatterCtasPerSm = 3;  // resident scatter CTAs per SM (registers and shared memory)
 constexpr int kTile = kScatterThreads * kScatterItems;  // tuples per partition tile
 constexpr int kJoinThreads = 1024;
 constexpr int kSmemCap = 10240;        // largest build partition joined in shared memory

@@ -596,13 +596,15 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
 // the first match in input order). Otherwise the rank of a tuple within its digit is taken with one
 // shared-memory atomic, in whatever order the warps reach it: the partitions hold the same tuples,
 // and the joins that count every match do not depend on their order.
-template <int THREADS, int ITEMS, bool STABLE>
-__global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
+// NBUF = 2: the next tile streams into a second buffer while this one is processed; NBUF = 1: one
+// buffer per CTA, the CTAs of an SM overlap each other's loads instead.
+template <int THREADS, int ITEMS, bool STABLE, int NBUF, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     constexpr int T = THREADS * ITEMS;
     constexpr int NW = THREADS / 32;
     extern __shared__ __align__(128) unsigned char smem[];
-    tuple_v *inbuf = reinterpret_cast<tuple_v *>(smem);                // [2][T]
-    long long *gbase = reinterpret_cast<long long *>(inbuf + 2 * T);     // [256]
+    tuple_v *inbuf = reinterpret_cast<tuple_v *>(smem);                // [NBUF][T]
+    long long *gbase = reinterpret_cast<long long *>(inbuf + NBUF * T);  // [256]
     long long *running = gbase + 256;                                   // [256]
     uint32_t *tdstart = reinterpret_cast<uint32_t *>(running + 256);    // [256]
     uint16_t *whist = reinterpret_cast<uint16_t *>(tdstart + 256);      // STABLE: [NW][F]
@@ -629,20 +631,32 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        const TileSlot s0 = next_tile<T>(a, it, nitems);
-        slots[0] = s0;
-        if (s0.item != ~0u) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
+        if (NBUF == 2) {
+            const TileSlot s0 = next_tile<T>(a, it, nitems);
+            slots[0] = s0;
+            if (s0.item != ~0u) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
+        }
     }
     __syncthreads();
 
     for (uint32_t k = 0;; k++) {
-        const uint32_t cur = k & 1u;
+        const uint32_t cur = NBUF == 2 ? (k & 1u) : 0u;
+        if (NBUF == 1) {
+            // One buffer: load this tile now (the barrier that ended the previous iteration ordered
+            // every read of the buffer before this copy).
+            if (tid == 0) {
+                const TileSlot sn = next_tile<T>(a, it, nitems);
+                slots[0] = sn;
+                if (sn.item != ~0u) tma_load_1d(inbuf, sn.in, sn.cnt * 16u, bar0);
+            }
+            __syncthreads();
+        }
         const TileSlot sl = slots[cur];
         if (sl.item == ~0u) break;
         tuple_v *buf = inbuf + (size_t)cur * T;
         // Prefetch the next tile into the other buffer; the barrier that ended the previous iteration
         // ordered every read of it before this copy.
-        if (tid == 0) {
+        if (NBUF == 2 && tid == 0) {
             const TileSlot sn = next_tile<T>(a, it, nitems);
             slots[cur ^ 1u] = sn;
             if (sn.item != ~0u) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
@@ -663,7 +677,7 @@ __global__ void __launch_bounds__(THREADS, 3) scatter_kernel(ScatterArgs a) {
             running[tid] = off;
         }
         const uint32_t cnt = sl.cnt;
-        const bool ok = mbar_wait(bar0 + 8u * cur, (k >> 1) & 1u);
+        const bool ok = mbar_wait(bar0 + 8u * cur, NBUF == 2 ? ((k >> 1) & 1u) : (k & 1u));
         if (__syncthreads_or(!ok)) {
             if (tid == 0) set_error(err, kErrSpinLimit);
             break;
@@ -1430,11 +1444,11 @@ int phj_prepare_device() {
     HJ_CU(cudaGetDevice(&cur_dev));
     if (cur_dev < 0 || cur_dev >= 64) return HJ_E_INVAL;
     if (g_attr_done[cur_dev]) return HJ_OK;
-    const size_t scatter_smem = (size_t)2 * kTile * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
+    const size_t scatter_smem = (size_t)kScatterBufs * kTile * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
     HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 136 * 1024));
-    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, true>,
+    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, true, kScatterBufs, kScatterCtasPerSm>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
-    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false>,
+    HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
@@ -1456,7 +1470,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     const int np = g.nparts();
     const int F1 = g.F1, F2 = g.F2;
     constexpr int T = kTile;
-    const size_t scatter_smem = (size_t)2 * T * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
+    const size_t scatter_smem = (size_t)kScatterBufs * T * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
     const size_t hist_smem = (size_t)np * 4 + (size_t)16 * F1 * 4;  // 16 warps
     ChunkGeom cg;
     cg.chunk = s.chunk;
@@ -1507,7 +1521,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     HJ_PH(2);
 
     // 5. scatter passes
-    const int scatter_grid = num_sms * 3;
+    const int scatter_grid = num_sms * kScatterCtasPerSm;
     for (int pass = 0; pass < g.passes; pass++) {
         ScatterArgs sa;
         sa.pass = pass;
@@ -1534,9 +1548,11 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.counters = s.counters;
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
         if (lp)
-            scatter_kernel<kScatterThreads, kScatterItems, true><<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+            scatter_kernel<kScatterThreads, kScatterItems, true, kScatterBufs, kScatterCtasPerSm>
+                <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
         else
-            scatter_kernel<kScatterThreads, kScatterItems, false><<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+            scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
+                <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
         HJ_CU(cudaGetLastError());
         nlaunch++;
         HJ_PH(3 + pass);
