@@ -74,7 +74,7 @@ class Params(ctypes.Structure):
         ("flags", ctypes.c_uint32),
         ("table_load", ctypes.c_double),
         ("radix_bits_pass1", ctypes.c_int),
-        ("reserved", ctypes.c_int),
+        ("watchdog_ms", ctypes.c_int),
     ]
 
 
@@ -188,7 +188,8 @@ def _ptr_len(rel, on_device: bool):
 
 
 def make_params(bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
-                stream: int | None = None, flags: int = 0, load: float = 0.5, bits_pass1: int = 0) -> Params:
+                stream: int | None = None, flags: int = 0, load: float = 0.5, bits_pass1: int = 0,
+                watchdog_ms: int = 0) -> Params:
     p = Params()
     lib().hj_params_init(ctypes.byref(p))
     p.num_radix_bits, p.num_passes, p.device = bits, passes, device
@@ -197,12 +198,13 @@ def make_params(bits: int = 14, passes: int = 2, device: int = 0, on_device: boo
     p.flags = flags
     p.table_load = load
     p.radix_bits_pass1 = bits_pass1
+    p.watchdog_ms = watchdog_ms
     return p
 
 
 def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
          stream: int | None = None, flags: int = 0, load: float = 0.5, ctx: "Context | None" = None,
-         check: bool = True, bits_pass1: int | None = None) -> Result:
+         check: bool = True, bits_pass1: int | None = None, watchdog_ms: int = 0) -> Result:
     """Run one join (synchronous). Raises JoinError on a non-zero status when check is set.
     bits_pass1: pass-1 radix bits of a two-pass join (None: 11 for phj_asymm_radix_* names, as the
     reference's NUM_RADIX_BITS_PASS1 default, else an even split)."""
@@ -210,7 +212,7 @@ def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, o
     a = ALGOS[algo]
     if bits_pass1 is None:
         bits_pass1 = ASYMM_DEFAULT_BITS_PASS1 if algo.startswith("phj_asymm_radix") else 0
-    p = make_params(bits, passes, device, on_device, stream, flags, load, bits_pass1)
+    p = make_params(bits, passes, device, on_device, stream, flags, load, bits_pass1, watchdog_ms)
     pr, nr = _ptr_len(R, on_device)
     ps, ns = _ptr_len(S, on_device)
     res = Result()
@@ -365,6 +367,7 @@ def header_functions() -> list[str]:
 # Batched joins and the autotuner (include/hjscm.h, "Batched joins")
 # ---------------------------------------------------------------------------------------------
 HJ_F_NO_GRAPH = 0x8
+HJ_F_TEST_STALL = 0x100
 IMPL_NAMES = {0: "nphj", 1: "phj"}
 
 

@@ -6,7 +6,9 @@
 // carves its scratch out of the arena and enqueues the whole kernel pipeline on one stream, reading
 // back only the 64-byte accumulator at the end.
 #include <cstdio>
+#include <chrono>
 #include <cstring>
+#include <thread>
 #include <mutex>
 
 #include "hj_common.cuh"
@@ -179,6 +181,7 @@ int hj_ctx_create(int device, hj_ctx_t **out) {
     CU_OR(cudaEventCreate(&c->ev_mid), HJ_E_DEVICE);
     CU_OR(cudaEventCreate(&c->ev_end), HJ_E_DEVICE);
     CU_OR(cudaEventCreate(&c->ev_ret), HJ_E_DEVICE);
+    CU_OR(cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming), HJ_E_DEVICE);
     for (int i = 0; i <= HJ_PH_COUNT; i++) CU_OR(cudaEventCreate(&c->ev_ph[i]), HJ_E_DEVICE);
     CU_OR(cudaMallocHost(&c->acc_host, sizeof(JoinAccum)), HJ_E_OOM);
     c->tuner.nphj_max_table_bytes = 64e6;
@@ -201,6 +204,7 @@ int hj_ctx_destroy(hj_ctx_t *c) {
         cudaEventDestroy(c->ev_start);
         cudaEventDestroy(c->ev_mid);
         if (c->ev_ret) cudaEventDestroy(c->ev_ret);
+        if (c->ev_done) cudaEventDestroy(c->ev_done);
         cudaEventDestroy(c->ev_end);
         for (int i = 0; i <= HJ_PH_COUNT; i++) cudaEventDestroy(c->ev_ph[i]);
         if (c->stream) cudaStreamDestroy(c->stream);
@@ -248,6 +252,8 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     rc = ensure_arena(c, need);
     if (rc) return out->status = rc;
     cudaStream_t st = p.stream ? (cudaStream_t)p.stream : c->stream;
+    // A join that a watchdog gave up on may still run; its arena use must end before this one starts.
+    CU_OR(cudaStreamWaitEvent(st, c->ev_done, 0), out->status = HJ_E_DEVICE);
     const bool timing = !(p.flags & HJ_F_NO_TIMING);
     const bool phases = (p.flags & HJ_F_PHASE_TIMES) != 0;
     cudaEvent_t *ph = phases ? c->ev_ph : nullptr;
@@ -275,7 +281,8 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
         hj::PhjScratch s;
         hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s);
         rc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
-                             timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
+                             timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches, nullptr,
+                             (p.flags & HJ_F_TEST_STALL) ? 1 : 0);
     } else {
         const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
         rc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
@@ -288,7 +295,20 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     if (timing) CU_OR(cudaEventRecord(c->ev_end, st), out->status = HJ_E_DEVICE);
     CU_OR(cudaMemcpyAsync(c->acc_host, acc, sizeof(JoinAccum), cudaMemcpyDeviceToHost, st),
           out->status = HJ_E_DEVICE);
-    CU_OR(cudaStreamSynchronize(st), out->status = HJ_E_DEVICE);
+    if (p.watchdog_ms > 0) {
+        // Host watchdog: poll the join's completion against a deadline instead of blocking.
+        CU_OR(cudaEventRecord(c->ev_done, st), out->status = HJ_E_DEVICE);
+        const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(p.watchdog_ms);
+        for (;;) {
+            const cudaError_t q = cudaEventQuery(c->ev_done);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) return out->status = HJ_E_DEVICE;
+            if (std::chrono::steady_clock::now() > deadline) return out->status = HJ_E_TIMEOUT;
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    } else {
+        CU_OR(cudaStreamSynchronize(st), out->status = HJ_E_DEVICE);
+    }
     out->matched_cnt = c->acc_host->matched;
     out->checksum = c->acc_host->checksum;
     out->large_partitions = c->acc_host->large_parts;
@@ -342,6 +362,7 @@ static int join_mat(hj_ctx *c, hj_algo_t algo, const hj_params_t &p, const hj_tu
     int rc = ensure_arena(c, need);
     if (rc) return out->status = rc;
     cudaStream_t st = p.stream ? (cudaStream_t)p.stream : c->stream;
+    CU_OR(cudaStreamWaitEvent(st, c->ev_done, 0), out->status = HJ_E_DEVICE);
     const bool timing = !(p.flags & HJ_F_NO_TIMING);
     uint32_t launches = 0;
 

@@ -16,7 +16,8 @@ struct hj_ctx {
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_h2d = nullptr, ev_start = nullptr, ev_mid = nullptr, ev_end = nullptr;
-    cudaEvent_t ev_ret = nullptr;  // materialising joins: end of the retrieve phase
+    cudaEvent_t ev_ret = nullptr;   // materialising joins: end of the retrieve phase
+    cudaEvent_t ev_done = nullptr;  // watchdog: the result copy has landed
     cudaEvent_t ev_ph[HJ_PH_COUNT + 1] = {};
     char *arena = nullptr;
     size_t arena_bytes = 0;

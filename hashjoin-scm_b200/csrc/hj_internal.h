@@ -80,10 +80,12 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
 // ph, if non-null, holds HJ_PH_COUNT + 1 events recorded at the phase boundaries; *launches receives
 // the number of kernels enqueued.
 // mat, if non-null, makes the join write one (r.row_id, s.row_id) pair per match into mat->pairs
-// (slots counted in acc->pairs) instead of summing row ids.
+// (slots counted in acc->pairs) instead of summing row ids. test_flags bit 0: the partition pass's
+// first CTA withholds one tile load, so its bounded wait expires (failure-detection tests).
 int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr);
+                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr,
+                int test_flags = 0);
 
 // Non-partitioned joins on a global open-addressing table.
 // mat: as for phj_enqueue; a materialising join needs nphj_scratch_bytes(nR, load, true).

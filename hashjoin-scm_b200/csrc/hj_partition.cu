@@ -113,8 +113,18 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 }
 
 // Bounded wait for the completion of phase `parity` of an mbarrier.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for an mbarrier phase: gives up after kWaitNs of wall time (try_wait may suspend the
+// thread for a hardware-defined time per call, so an iteration count alone is no time bound).
+constexpr uint64_t kWaitNs = 2000000000ull;
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int it = 0; it < (1 << 24); it++) {
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 0; it < (1u << 30); it++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -124,6 +134,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
             : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((it & 63u) == 63u && globaltimer_ns() - t0 > kWaitNs) return false;
     }
     return false;
 }
@@ -509,6 +520,7 @@ struct ScatterArgs {
     const uint64_t *unit_off;   // [chunk][F1]
     const uint32_t *unit_cnt;   // [chunk][F1]
     const uint32_t *subpre;     // [chunk][spc][F1] start of (sub-chunk, d1) within (chunk, d1)
+    int test_stall;             // test hook: CTA 0 withholds its first tile load (its wait must expire)
     uint32_t *counters;
     int ctr_item;
 };
@@ -634,7 +646,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         if (NBUF == 2) {
             const TileSlot s0 = next_tile<T>(a, it, nitems);
             slots[0] = s0;
-            if (s0.item != ~0u) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
+            if (s0.item != ~0u && !(a.test_stall && blockIdx.x == 0)) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
         }
     }
     __syncthreads();
@@ -647,7 +659,8 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             if (tid == 0) {
                 const TileSlot sn = next_tile<T>(a, it, nitems);
                 slots[0] = sn;
-                if (sn.item != ~0u) tma_load_1d(inbuf, sn.in, sn.cnt * 16u, bar0);
+                if (sn.item != ~0u && !(a.test_stall && blockIdx.x == 0 && k == 0))
+                    tma_load_1d(inbuf, sn.in, sn.cnt * 16u, bar0);
             }
             __syncthreads();
         }
@@ -679,7 +692,12 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         const uint32_t cnt = sl.cnt;
         const bool ok = mbar_wait(bar0 + 8u * cur, NBUF == 2 ? ((k >> 1) & 1u) : (k & 1u));
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) set_error(err, kErrSpinLimit);
+            if (tid == 0) {
+                set_error(err, kErrSpinLimit);
+                // Before leaving, let the prefetch into the other buffer land (bounded as well): the
+                // copy must not write into shared memory this CTA no longer owns.
+                if (NBUF == 2 && slots[cur ^ 1u].item != ~0u) mbar_wait(bar0 + 8u * (cur ^ 1u), ((k + 1) >> 1) & 1u);
+            }
             break;
         }
 
@@ -1462,7 +1480,7 @@ int phj_prepare_device() {
 
 int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat) {
+                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat, int test_flags) {
     uint32_t nlaunch = 0;
 #define HJ_PH(i) \
     if (ph) HJ_CU(cudaEventRecord(ph[i], st))
@@ -1545,6 +1563,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.unit_off = s.unit_off;
         sa.unit_cnt = s.unit_cnt;
         sa.subpre = s.subhist;
+        sa.test_stall = (pass == 0 && (test_flags & 1)) ? 1 : 0;
         sa.counters = s.counters;
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
         if (lp)

@@ -91,12 +91,17 @@ typedef struct {
     int radix_bits_pass1; /* two passes: bits of pass 1 (NUM_RADIX_BITS_PASS1 of phj_asymm_radix,
                              src/algo/phj_asymm_radix.h:10-19); 0 selects bits / 2. Clamped to the
                              split where each pass has 1..8 bits. */
-    int reserved;
+    int watchdog_ms;      /* > 0: hj_join / hj_join_ctx return HJ_E_TIMEOUT if the join has not finished
+                             after this many milliseconds (its kernels keep running; later calls on the
+                             context queue behind them). 0: wait as long as it takes. */
 } hj_params_t;
 
 #define HJ_F_NO_TIMING   0x1u /* skip the per-phase CUDA events (buildpart/probejoin stay 0) */
 #define HJ_F_PINNED_HOST 0x2u /* host inputs are already page-locked */
 #define HJ_F_PHASE_TIMES 0x4u /* also time each kernel group (fills hj_result_t.phase) */
+/* Test hook for failure detection: the first partition pass of a radix join withholds one tile load,
+ * so a bounded device wait (2 s) expires and the join returns HJ_E_TIMEOUT; the context stays usable. */
+#define HJ_F_TEST_STALL  0x100u
 
 /* hj_result_t.phase[] slots (seconds), filled with HJ_F_PHASE_TIMES. PHJ: histogram, plan, partition
  * pass 1, partition pass 2, shared-memory partition joins, global-memory (large) partition joins.
