@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=1000, help="serve mode: requests per rate")
     ap.add_argument("--slots", type=int, default=8, help="serve mode: concurrent requests on the GPU")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serve mode: HBM pool budget")
+    ap.add_argument("--large-share", type=float, default=None,
+                    help="serve mode: SM share of large requests' kernels (default: the library's)")
     ap.add_argument("--batch-jobs", type=int, default=512)
     ap.add_argument("--calibrate", action="store_true", help="batch mode: calibrate the autotuner first")
     ap.add_argument("--algo", default="phj_radix_bc")
@@ -563,7 +565,7 @@ def run_serve_mode(a, rank, world, local_rank):
     # 1. the join server
     srv_out, peak, budget = [], 0.0, 0.0
     impl_counts = {0: 0, 1: 0}
-    with hj.Server(local_rank, slots=a.slots, hbm_budget_bytes=a.budget_gb * 1e9) as srv:
+    with hj.Server(local_rank, slots=a.slots, hbm_budget_bytes=a.budget_gb * 1e9, large_sm_share=a.large_share) as srv:
         for R, S, _ in small[:8] + [big]:  # warm-up: kernel attributes, first launches
             srv.wait_all([srv.submit("phj_radix_bc", R, S, on_device=True)])
         for lam, arrivals, picks in streams:

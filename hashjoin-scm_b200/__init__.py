@@ -481,7 +481,8 @@ class Batch:
 # ---------------------------------------------------------------------------------------------
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double),
-                ("autotune", ctypes.c_int), ("tuner", Tuner), ("small_request_tuples", ctypes.c_double)]
+                ("autotune", ctypes.c_int), ("tuner", Tuner), ("small_request_tuples", ctypes.c_double),
+                ("large_sm_share", ctypes.c_double)]
 
 
 class Completion(ctypes.Structure):
@@ -527,13 +528,15 @@ class Server:
     server keeps a reference to them until their completion has been polled."""
 
     def __init__(self, device: int = 0, slots: int = 8, hbm_budget_bytes: float = 150e9, autotune: bool = True,
-                 tuner: dict | None = None):
+                 tuner: dict | None = None, large_sm_share: float | None = None):
         L = _bind_server()
         cfg = ServerConfig()
         L.hj_server_config_init(ctypes.byref(cfg))
         cfg.device, cfg.slots, cfg.hbm_budget_bytes, cfg.autotune = device, slots, hbm_budget_bytes, int(autotune)
         for k, v in (tuner or {}).items():
             setattr(cfg.tuner, k, v)
+        if large_sm_share is not None:
+            cfg.large_sm_share = large_sm_share
         h = ctypes.c_void_p()
         rc = L.hj_server_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc:

@@ -10,6 +10,9 @@
 //     are on the GPU is admitted as soon as a slot and its memory are free and its kernels overlap with
 //     theirs; small requests run on high-priority streams, so their thread blocks are scheduled ahead of
 //     the waiting blocks of a large join and their latency stays near their own run time;
+//   - large requests size their persistent kernels for a share of the SMs (large_sm_share, 0.75 by
+//     default), so the blocks of small requests find free SMs instead of waiting for a whole partition
+//     pass of a large join to drain (stream priority orders pending blocks, it does not preempt);
 //   - the dispatcher thread polls the slots' completion events without sleeping while any request is
 //     on the GPU (a sleep of a few microseconds costs tens of microseconds of timer slack per request);
 //   - admission is first come, first served, except that requests behind a head that does not fit yet
@@ -162,6 +165,12 @@ int launch(hj_server *s, Slot &sl) {
     Request &r = sl.req;
     const bool small = (double)(r.nR + r.nS) <= s->cfg.small_request_tuples;
     cudaStream_t st = sl.cur = small ? sl.stream_hi : sl.stream;
+    // Grids of a large request's persistent kernels scale with the SMs they are sized for.
+    int sms = s->ctx->num_sms;
+    if (!small && s->cfg.large_sm_share > 0.0 && s->cfg.large_sm_share < 1.0) {
+        sms = (int)(s->ctx->num_sms * s->cfg.large_sm_share);
+        if (sms < 1) sms = 1;
+    }
     char *base = s->pool_mem + r.off;
     hj::JoinAccum *acc = reinterpret_cast<hj::JoinAccum *>(base);
     char *cur = base + 256;
@@ -183,14 +192,14 @@ int launch(hj_server *s, Slot &sl) {
     if (r.nR && r.nS) {
         if (r.impl == 0) {
             const size_t tb = r.need - (size_t)(cur - base);
-            rc = hj::nphj_enqueue(lp, skip0, R, r.nR, S, r.nS, cur, tb, 0.5, acc, st, nullptr, s->ctx->num_sms,
+            rc = hj::nphj_enqueue(lp, skip0, R, r.nR, S, r.nS, cur, tb, 0.5, acc, st, nullptr, sms,
                                   nullptr, nullptr);
         } else {
             hj::RadixGeom g;
             hj::radix_geom(r.bits, r.passes, &g);
             hj::PhjScratch ps;
             hj::phj_carve(g, r.nR, r.nS, s->ctx->num_sms, cur, &ps);
-            rc = hj::phj_enqueue(g, lp, skip0, R, r.nR, S, r.nS, ps, acc, st, nullptr, s->ctx->num_sms, nullptr,
+            rc = hj::phj_enqueue(g, lp, skip0, R, r.nR, S, r.nS, ps, acc, st, nullptr, sms, nullptr,
                                  nullptr);
         }
     }
@@ -311,6 +320,7 @@ int hj_server_config_init(hj_server_config_t *c) {
     c->hbm_budget_bytes = 150e9;
     c->autotune = 1;
     c->small_request_tuples = (double)(1u << 25);
+    c->large_sm_share = 0.75;
     return HJ_OK;
 }
 

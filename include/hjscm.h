@@ -327,6 +327,8 @@ typedef struct {
     int autotune;                /* 1: per-request implementation from the tuner (default) */
     hj_tuner_t tuner;            /* used when tuner.partition_target > 0, else the context defaults */
     double small_request_tuples; /* requests with |R| + |S| <= this run on high-priority streams */
+    double large_sm_share;       /* larger requests launch their kernels sized for this share of the SMs
+                                    (0..1], leaving room for small requests' blocks; 1 = all SMs */
 } hj_server_config_t;
 
 typedef struct {
@@ -348,7 +350,8 @@ typedef struct hj_server hj_server_t;
 
 /* Monotonic clock in seconds, the one completions are stamped with. */
 double hj_now(void);
-/* Defaults: device 0, 8 slots, 150e9 bytes, autotune, small requests up to 2^25 tuples. */
+/* Defaults: device 0, 8 slots, 150e9 bytes, autotune, small requests up to 2^25 tuples, large requests
+ * on 0.75 of the SMs. */
 int hj_server_config_init(hj_server_config_t *cfg);
 int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out);
 int hj_server_submit(hj_server_t *srv, hj_algo_t algo, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,

@@ -137,6 +137,7 @@ def test_server_config_defaults(hj):
     cfg = hj.ServerConfig()
     assert L.hj_server_config_init(cfg) == 0
     assert (cfg.device, cfg.slots, cfg.hbm_budget_bytes, cfg.autotune) == (0, 8, 150e9, 1)
+    assert (cfg.small_request_tuples, cfg.large_sm_share) == (2.0**25, 0.75)
     assert L.hj_server_config_init(None) == hj.HJ_E_INVAL
     assert 0 < hj.now()
 
