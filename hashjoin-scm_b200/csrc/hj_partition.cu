@@ -329,36 +329,50 @@ __device__ __forceinline__ uint32_t part_to_value(int f, int passes, int b1, int
     return d1 | (d2 << b1);
 }
 
+// Dynamic shared memory: the relation totals ([2][2^B] u32) when they fit (B <= 14), so that the
+// per-partition loops below read shared memory instead of waiting on one global load after another.
+constexpr int kPlanStageBits = 14;
+
 __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
+    extern __shared__ uint32_t sm_tot[];
     __shared__ uint32_t tmp[32];
     __shared__ uint64_t s_item_run, s_large_run;
     const int tid = threadIdx.x;
     const int nparts = 1 << a.bits;
+    const uint32_t *tot_all = a.total;
+    if (a.bits <= kPlanStageBits) {
+#pragma unroll 8
+        for (int i = tid; i < 2 * nparts; i += 1024) sm_tot[i] = a.total[i];
+        __syncthreads();
+        tot_all = sm_tot;
+    }
     // Each thread owns a contiguous range of partitions.
     const int per = (nparts + 1023) / 1024;
     const int f0 = tid * per < nparts ? tid * per : nparts;
     const int f1 = f0 + per < nparts ? f0 + per : nparts;
+    uint64_t base[2];  // start of this thread's first partition, per relation
     for (int rel = 0; rel < 2; rel++) {
         uint64_t *start = a.start + (size_t)rel * (nparts + 1);
-        const uint32_t *tot = a.total + (size_t)rel * nparts;
+        const uint32_t *tot = tot_all + (size_t)rel * nparts;
         uint32_t sum = 0;
         for (int f = f0; f < f1; f++) sum += tot[part_to_value(f, a.passes, a.b1, a.F2)];
         uint32_t all;
         uint64_t run = block_excl_scan_u32(sum, tmp, &all);
+        base[rel] = run;
         for (int f = f0; f < f1; f++) {
             start[f] = run;
             run += tot[part_to_value(f, a.passes, a.b1, a.F2)];
         }
         if (tid == 0) start[nparts] = all;
     }
-    __syncthreads();
 
     // Join work items (partitions with both sides non-empty, src/algo/phj.c:459-491) and large
-    // partitions.
-    const uint64_t *stR = a.start, *stS = a.start + (nparts + 1);
+    // partitions. Partition sizes come from the totals, starts from the running sums above.
+    const uint32_t *totR = tot_all, *totS = tot_all + nparts;
     uint32_t asum = 0, bsum = 0, lsum = 0;  // items with |R_p| <= compact cap, other small items, large
     for (int f = f0; f < f1; f++) {
-        const uint64_t nr = stR[f + 1] - stR[f], ns = stS[f + 1] - stS[f];
+        const uint32_t v = part_to_value(f, a.passes, a.b1, a.F2);
+        const uint64_t nr = totR[v], ns = totS[v];
         if (nr > 0 && ns > 0) {
             if (nr <= (uint64_t)kCompactCap) asum += ceil_div_u64(ns, kProbeChunk);
             else if (nr <= (uint64_t)kSmemCap) bsum += ceil_div_u64(ns, kProbeChunk);
@@ -370,8 +384,13 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
     uint64_t b_idx = block_excl_scan_u32(bsum, tmp, &btot) + atot;
     uint64_t large_idx = block_excl_scan_u32(lsum, tmp, &ltot);
     const uint32_t ktot = atot + btot;
+    uint64_t rR = base[0], rS = base[1];
     for (int f = f0; f < f1; f++) {
-        const uint64_t nr = stR[f + 1] - stR[f], ns = stS[f + 1] - stS[f];
+        const uint32_t v = part_to_value(f, a.passes, a.b1, a.F2);
+        const uint64_t nr = totR[v], ns = totS[v];
+        const uint64_t sR = rR, sS = rS;
+        rR += nr;
+        rS += ns;
         if (!(nr > 0 && ns > 0)) continue;
         if (nr <= (uint64_t)kSmemCap) {
             uint64_t &item_idx = nr <= (uint64_t)kCompactCap ? a_idx : b_idx;
@@ -379,8 +398,8 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
             for (uint32_t q = 0; q < k; q++, item_idx++) {
                 if (item_idx < a.max_items) {
                     JoinItem it;
-                    it.r_begin = stR[f];
-                    it.s_begin = stS[f] + (uint64_t)q * kProbeChunk;
+                    it.r_begin = sR;
+                    it.s_begin = sS + (uint64_t)q * kProbeChunk;
                     it.r_len = (uint32_t)nr;
                     const uint64_t rem = ns - (uint64_t)q * kProbeChunk;
                     it.s_len = (uint32_t)(rem < (uint64_t)kProbeChunk ? rem : (uint64_t)kProbeChunk);
@@ -393,8 +412,8 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
         } else {
             if (large_idx < a.max_large) {
                 LargePart lp;
-                lp.r_begin = stR[f];
-                lp.s_begin = stS[f];
+                lp.r_begin = sR;
+                lp.s_begin = sS;
                 lp.r_len = nr;
                 lp.s_len = ns;
                 uint32_t nb_log = 0;
@@ -1464,6 +1483,8 @@ int phj_prepare_device() {
     if (g_attr_done[cur_dev]) return HJ_OK;
     const size_t scatter_smem = (size_t)kScatterBufs * kTile * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
     HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 136 * 1024));
+    HJ_CU(cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)((size_t)2 * (1u << kPlanStageBits) * 4)));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, true, kScatterBufs, kScatterCtasPerSm>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>,
@@ -1528,7 +1549,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     pa.large = reinterpret_cast<LargePart *>(s.large);
     pa.max_large = s.max_large;
     pa.large_table_words = s.large_table_words;
-    plan_kernel<<<1, 1024, 0, st>>>(pa);
+    plan_kernel<<<1, 1024, g.bits <= kPlanStageBits ? (size_t)2 * np * 4 : 0, st>>>(pa);
     {
         const int ut = F1 < 32 ? 32 : F1;
         units_kernel<<<nchunks, ut, 0, st>>>(s.chunk_hist, s.prefix, s.start, g.bits, g.b1, F1, g.passes == 2 ? F2 : 1,
