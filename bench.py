@@ -320,20 +320,33 @@ def run_ours(a, rank, world, local_rank):
     phases = {name: statistics.mean(r.phase[i] for r in results) for i, name in enumerate(hj.PHASES)}
     launches = sum(r.kernel_launches for r in results)
 
-    # Roofline of the dominant kernel: a partition pass reads and writes every tuple once (32 B).
+    # Roofline of the dominant kernel. Radix joins: a partition pass reads and writes every tuple once
+    # (32 B); the pipeline with P materialised passes moves 16 (2P + 1) B per tuple. Non-partitioned
+    # joins: build and probe read every tuple and touch one 16-byte table slot each (32 B per tuple).
     peak, peak_kind = measured_peaks()
-    pass_s = statistics.mean([phases["pass1"], phases["pass2"]]) if a.passes == 2 else phases["pass1"]
-    scatter_bytes = 32 * (nR + nS)
-    achieved = scatter_bytes / pass_s / 1e9
-    prof = traffic_profile("scatter_kernel")
-    traffic = prof["dram_bytes_per_tuple"] * (nR + nS) if prof else None
-    roofline = {"kernel": "scatter_kernel (one radix partition pass)", "bound": "hbm",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_launch": scatter_bytes, "launch_ms": pass_s * 1e3}
-    pipe_bytes = 16 * (2 * a.passes + 1) * (nR + nS)
     step_s = ms / 1e3 / a.steps
-    pipeline = {"algorithmic_bytes_per_tuple": 16 * (2 * a.passes + 1), "bytes_per_step": pipe_bytes,
+    if a.algo.startswith("phj"):
+        P = results[-1].physical_passes
+        pass_s = statistics.mean([phases["pass1"], phases["pass2"]]) if P == 2 else phases["pass1"]
+        scatter_bytes = 32 * (nR + nS)
+        achieved = scatter_bytes / pass_s / 1e9
+        prof = traffic_profile("scatter_kernel")
+        traffic = prof["dram_bytes_per_tuple"] * (nR + nS) if prof else None
+        roofline = {"kernel": "scatter_kernel (one radix partition pass)", "bound": "hbm",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_source": peak_kind, "traffic": traffic,
+                    "algorithmic_bytes_per_launch": scatter_bytes, "launch_ms": pass_s * 1e3}
+        per_tuple = 16 * (2 * P + 1)
+    else:
+        per_tuple = 32
+        join_bytes = per_tuple * (nR + nS)
+        achieved = join_bytes / step_s / 1e9
+        roofline = {"kernel": "nphj_build + nphj_probe (the whole join)", "bound": "hbm",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_source": peak_kind, "traffic": None,
+                    "algorithmic_bytes_per_launch": join_bytes, "launch_ms": step_s * 1e3}
+    pipe_bytes = per_tuple * (nR + nS)
+    pipeline = {"algorithmic_bytes_per_tuple": per_tuple, "bytes_per_step": pipe_bytes,
                 "achieved_gbs": pipe_bytes / step_s / 1e9, "frac": pipe_bytes / step_s / 1e9 / peak,
                 "phase_ms": {k: v * 1e3 for k, v in phases.items()}}
 

@@ -34,7 +34,8 @@ static const char *arg_value(int argc, char **argv, const char *name) {
 
 /* Minimal reader of the reference's libconfig workload files (the files under config/data): lines of
  * `name = value;` with quoted strings; only the keys data_cfg reads (src/inc/utils.c:258-273). */
-static int read_cfg(const char *path, datameta_t *d, char *rbuf, char *sbuf, char *wbuf, size_t blen) {
+static int read_cfg(const char *path, datameta_t *d, char *rbuf, size_t rlen, char *sbuf, size_t slen, char *wbuf,
+                    size_t wlen) {
     FILE *f = fopen(path, "r");
     if (!f) return HJ_E_IO;
     memset(d, 0, sizeof(*d));
@@ -55,9 +56,9 @@ static int read_cfg(const char *path, datameta_t *d, char *rbuf, char *sbuf, cha
             if (q) *q = 0;
         }
         snprintf(val, sizeof(val), "%s", v);
-        if (!strcmp(key, "r_path_suffix")) snprintf(rbuf, blen, "%s", val);
-        else if (!strcmp(key, "s_path_suffix")) snprintf(sbuf, blen, "%s", val);
-        else if (!strcmp(key, "workload_name")) snprintf(wbuf, blen, "%s", val);
+        if (!strcmp(key, "r_path_suffix")) snprintf(rbuf, rlen, "%s", val);
+        else if (!strcmp(key, "s_path_suffix")) snprintf(sbuf, slen, "%s", val);
+        else if (!strcmp(key, "workload_name")) snprintf(wbuf, wlen, "%s", val);
         else if (!strcmp(key, "r_tuple_num")) d->r_tuple_num = strtoull(val, NULL, 10);
         else if (!strcmp(key, "s_tuple_num")) d->s_tuple_num = strtoull(val, NULL, 10);
         else if (!strcmp(key, "r_tuple_size")) d->r_tuple_size = strtoull(val, NULL, 10);
@@ -151,7 +152,7 @@ int main(int argc, char **argv) {
         const char *cfgp = getenv("HJ_DATA_CFG_PATH_PREFIX");
         char cfg[8192];
         snprintf(cfg, sizeof(cfg), "%s/data/%s/%s_%s.cfg", cfgp ? cfgp : "config", wl, pa, st);
-        if (read_cfg(cfg, &d, rbuf, sbuf, wbuf, sizeof(rbuf))) {
+        if (read_cfg(cfg, &d, rbuf, sizeof(rbuf), sbuf, sizeof(sbuf), wbuf, sizeof(wbuf))) {
             fprintf(stderr, "[ERROR] cannot read %s\n", cfg);
             return 1;
         }

@@ -14,6 +14,7 @@ def random_case(rng):
     nR = int(rng.choice([0, 1, 2, int(rng.integers(3, 300)), int(rng.integers(300, 50_000))]))
     nS = int(rng.choice([0, 1, int(rng.integers(2, 500)), int(rng.integers(500, 60_000))]))
     key_range = int(rng.choice([2, 50, max(nR // 8, 1), max(nR, 1), 4 * max(nR, 1), 2**40]))
+    key_range = max(key_range, nR * nS // 5_000_000 + 1)  # at most ~5M matches: chains stay short
     R = np.empty((nR, 2), dtype=np.uint64)
     S = np.empty((nS, 2), dtype=np.uint64)
     R[:, 0] = rng.integers(0, key_range, nR, dtype=np.uint64)

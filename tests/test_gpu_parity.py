@@ -272,3 +272,33 @@ def test_asymm_cli_entry_point(hj, tmp_path):
     assert out.returncode == 0, out.stderr
     want = hj.join("phj_radix_bc", R, S)
     assert f"matched_cnt: {want.matched_cnt}\tcheck_sum: {want.checksum}" in out.stdout
+
+
+def test_cli_workload_config_files(hj, tmp_path):
+    # bin/main's way of naming a workload: --workload/--subtype/--param select
+    # $HJ_DATA_CFG_PATH_PREFIX/data/<workload>/<param>_<subtype>.cfg, whose path suffixes are read under
+    # $HJ_DATA_PATH_PREFIX; per-trial and averaged lines as src/main.c:439-459 prints them.
+    import os
+    import subprocess
+
+    nR, nS = 1 << 12, 1 << 14
+    R, S = hj.gen_pkfk_uniform(nR, nS, payload=True)
+    (tmp_path / "data" / "t").mkdir(parents=True)
+    (tmp_path / "rel" / "t").mkdir(parents=True)
+    R.tofile(tmp_path / "rel" / "t" / "pk_TR.bin")
+    S.tofile(tmp_path / "rel" / "t" / "fk_TS.bin")
+    (tmp_path / "data" / "t" / "pkfk_T.cfg").write_text(
+        'r_path_suffix = "t/pk_TR.bin";\ns_path_suffix = "t/fk_TS.bin";\n\n'
+        f"r_tuple_num = {nR};\ns_tuple_num = {nS};\nr_tuple_size = 16;\ns_tuple_size = 16;\n\n"
+        "theta = 0.0;\nselectivity = 1.0;\ndensity = 1.0;\nsparsity = 1.0;\n\n"
+        f'min_key = 1;\nmax_key = {nR};\n\nworkload_name = "test_pkfk_T";\n')
+    env = dict(os.environ, HJ_DATA_CFG_PATH_PREFIX=str(tmp_path), HJ_DATA_PATH_PREFIX=str(tmp_path / "rel"))
+    want = hj.join("phj_radix_bc", R, S)
+    for algo in ("phj_radix_bc", "ptr_phj_radix_bc", "nphj_lp"):
+        out = subprocess.run([str(hj.MAIN_PATH), f"--algo={algo}", "--workload=t", "--subtype=T", "--param=pkfk",
+                              "--trials=3"], capture_output=True, text=True, env=env)
+        assert out.returncode == 0, out.stdout + out.stderr
+        assert out.stdout.count(f"matched_cnt: {want.matched_cnt}\tcheck_sum: {want.checksum}") == 3
+        trial_lines = [ln for ln in out.stdout.splitlines() if ln.startswith("memory_type: HBM\talgo: " + algo)]
+        assert len(trial_lines) == 3 and all("\tworkload: test_pkfk_T\t" in ln for ln in trial_lines)
+        assert "num_trials: 2\t" in out.stdout
