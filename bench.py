@@ -63,7 +63,8 @@ def parse_args():
     ap.add_argument("--large-share", type=float, default=None,
                     help="serve mode: SM share of large requests' kernels (default: the library's)")
     ap.add_argument("--batch-jobs", type=int, default=512)
-    ap.add_argument("--calibrate", action="store_true", help="batch mode: calibrate the autotuner first")
+    ap.add_argument("--calibrate", action="store_true",
+                    help="batch mode: tune the batch plan on the device first (HJ_F_TUNE)")
     ap.add_argument("--algo", default="phj_radix_bc")
     ap.add_argument("--nr-log", type=int, default=27)
     ap.add_argument("--ns-log", type=int, default=29)
@@ -437,8 +438,11 @@ def run_batch_mode(a, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     jobs, want, total, buf = batch_workload(hj, torch, dev, a.batch_jobs, seed=12345 + 1000 * rank)
     ctx = hj.Context(local_rank)
-    calib = hj.tuner_calibrate(ctx) if a.calibrate else None
+    # With --calibrate the batch is planned under several table budgets, each timed on the device; the
+    # fastest plan is kept and its budget stays in the tuner (the tuned loop below uses it too).
+    batch = hj.Batch(ctx, jobs, tune=a.calibrate)
     tuner = hj.tuner_get(ctx)
+    calib = None
 
     def check(results):
         for r, w in zip(results, want):
@@ -478,7 +482,7 @@ def run_batch_mode(a, rank, world, local_rank):
     check(loop(True))
     t_loop_tuned, res = timed(lambda: loop(True), max(1, a.steps // 5))
     check(res)
-    with hj.Batch(ctx, jobs) as b:
+    with batch as b:
         for _ in range(a.warmup):
             res, st = b.run()
             check(res)
@@ -504,7 +508,7 @@ def run_batch_mode(a, rank, world, local_rank):
             "tuples_per_s": total / t_batch, "batch_stats": {"nphj_jobs": st.nphj_jobs, "phj_jobs": st.phj_jobs,
                                                              "waves": st.waves, "kernels": st.kernel_launches},
             "tuner": {"nphj_max_table_bytes": tuner.nphj_max_table_bytes, "calibrated": tuner.calibrated,
-                      "calibration": calib},
+                      "phj_fixed_s": tuner.phj_fixed, "calibration": calib},
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -367,13 +367,20 @@ def header_functions() -> list[str]:
 # Batched joins and the autotuner (include/hjscm.h, "Batched joins")
 # ---------------------------------------------------------------------------------------------
 HJ_F_NO_GRAPH = 0x8
+HJ_F_TUNE = 0x10
 HJ_F_TEST_STALL = 0x100
 IMPL_NAMES = {0: "nphj", 1: "phj"}
 
 
+TUNER_LEVELS = 8
+
+
 class Tuner(ctypes.Structure):
     _fields_ = [("nphj_max_table_bytes", ctypes.c_double), ("wave_table_bytes", ctypes.c_double),
-                ("partition_target", ctypes.c_int), ("calibrated", ctypes.c_int)]
+                ("partition_target", ctypes.c_int), ("calibrated", ctypes.c_int),
+                ("level_nR", ctypes.c_double * TUNER_LEVELS), ("nphj_build", ctypes.c_double * TUNER_LEVELS),
+                ("nphj_probe", ctypes.c_double * TUNER_LEVELS), ("phj", ctypes.c_double * TUNER_LEVELS),
+                ("phj_fixed", ctypes.c_double)]
 
 
 class BatchJob(ctypes.Structure):
@@ -440,7 +447,7 @@ class Batch:
 
     jobs: list of (algo name, R, S) where R and S are CUDA tensors of shape (n, 2) or (pointer, n)."""
 
-    def __init__(self, ctx: "Context", jobs, graph: bool = True):
+    def __init__(self, ctx: "Context", jobs, graph: bool = True, tune: bool = False):
         L = _bind_batch()
         arr = (BatchJob * max(len(jobs), 1))()
         self._keep = []
@@ -449,7 +456,8 @@ class Batch:
             ps, ns = _ptr_len(S, True)
             arr[i].algo, arr[i].R, arr[i].nR, arr[i].S, arr[i].nS = ALGOS[algo], pr, nr, ps, ns
             self._keep.append((R, S))
-        p = make_params(device=ctx.device, on_device=True, flags=0 if graph else HJ_F_NO_GRAPH)
+        p = make_params(device=ctx.device, on_device=True,
+                        flags=(0 if graph else HJ_F_NO_GRAPH) | (HJ_F_TUNE if tune else 0))
         h = ctypes.c_void_p()
         rc = L.hj_batch_plan(ctx.handle, arr, len(jobs), ctypes.byref(p), ctypes.byref(h))
         if rc:

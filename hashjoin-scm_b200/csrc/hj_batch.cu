@@ -307,6 +307,8 @@ struct hj_batch {
     JoinAccum *accs_host = nullptr; // pinned
     char *phj_scratch = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream_phj = nullptr;            // partitioned joins, forked from `stream`
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -316,10 +318,34 @@ struct hj_batch {
 
 namespace {
 
+// Calibrated cost of each implementation for a join of (nR, nS), from the level of the nearest build
+// size (log scale). Returns false when the tuner has no cost model.
+bool model_prefers_nphj(const hj_tuner_t &t, size_t nR, size_t nS, bool *nphj) {
+    if (!t.calibrated) return false;
+    int best = -1;
+    double bd = 1e300;
+    for (int i = 0; i < HJ_TUNER_LEVELS; i++) {
+        if (!(t.level_nR[i] > 0) || !(t.phj[i] > 0)) continue;
+        const double d = std::fabs(std::log2((double)(nR ? nR : 1)) - std::log2(t.level_nR[i]));
+        if (d < bd) {
+            bd = d;
+            best = i;
+        }
+    }
+    if (best < 0) return false;
+    const double tn = (double)nR * t.nphj_build[best] + (double)nS * t.nphj_probe[best];
+    const double tp = t.phj_fixed + (double)(nR + nS) * t.phj[best];
+    *nphj = tn <= tp;
+    return true;
+}
+
 void decide(const hj_ctx *c, size_t nR, size_t nS, int *impl, int *bits, int *passes) {
-    (void)nS;
     const hj_tuner_t &t = c->tuner;
-    if ((double)nphj_slots(nR) * 16.0 <= t.nphj_max_table_bytes) {
+    const bool fits = (double)nphj_slots(nR) * 16.0 <= t.nphj_max_table_bytes;
+    bool use_nphj = fits;
+    bool pref = false;
+    if (fits && model_prefers_nphj(t, nR, nS, &pref)) use_nphj = pref;
+    if (use_nphj) {
         *impl = kImplNphj;
         *bits = 0;
         *passes = 0;
@@ -346,6 +372,15 @@ int enqueue_batch(hj_batch *b) {
     cudaStream_t st = b->stream;
     BCU(cudaMemsetAsync(b->accs, 0, sizeof(JoinAccum) * b->njobs, st));
     uint32_t launches = 0;
+    // The partitioned joins run on a second stream forked here and joined at the end: they share
+    // nothing with the waves of non-partitioned joins, and their kernels fill the SMs that a wave's
+    // small kernels leave idle (in the captured graph these become two parallel branches).
+    const bool fork = !b->phj_jobs.empty();
+    cudaStream_t sp = fork ? b->stream_phj : st;
+    if (fork) {
+        BCU(cudaEventRecord(b->ev_fork, st));
+        BCU(cudaStreamWaitEvent(sp, b->ev_fork, 0));
+    }
     for (const Wave &w : b->waves) {
         if (w.total_r == 0 && w.total_s == 0) continue;
         BCU(cudaMemsetAsync(w.tables, 0xff, w.total_t * 16, st));
@@ -377,10 +412,14 @@ int enqueue_batch(hj_batch *b) {
         hj::phj_carve(g, J.nR, J.nS, sms, b->phj_scratch, &s);
         uint32_t l = 0;
         int rc = hj::phj_enqueue(g, sem_lp(J.algo), sem_skip0(J.algo), reinterpret_cast<const ulonglong2 *>(J.R), J.nR,
-                                 reinterpret_cast<const ulonglong2 *>(J.S), J.nS, s, b->accs + j, st, nullptr, sms,
+                                 reinterpret_cast<const ulonglong2 *>(J.S), J.nS, s, b->accs + j, sp, nullptr, sms,
                                  nullptr, &l);
         if (rc) return rc;
         launches += l;
+    }
+    if (fork) {
+        BCU(cudaEventRecord(b->ev_join, sp));
+        BCU(cudaStreamWaitEvent(st, b->ev_join, 0));
     }
     b->launches = launches;
     return HJ_OK;
@@ -408,7 +447,68 @@ int hj_tuner_decide(hj_ctx_t *c, size_t nR, size_t nS, int *impl, int *bits, int
     return HJ_OK;
 }
 
+static int plan_one(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_params_t *p, hj_batch_t **out);
+
+// Empirical tuning of a batch (HJ_F_TUNE): plan it under a few table budgets around the current one,
+// time each plan's graph, keep the fastest and leave its budget in the context's tuner. Timings of
+// single joins in isolation do not predict a batch well (waves share tables' L2 room, partitioned
+// joins overlap the waves on their own branch), the batch itself does.
 int hj_batch_plan(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_params_t *p, hj_batch_t **out) {
+    if (!c || !out) return HJ_E_INVAL;
+    if (!(p && (p->flags & HJ_F_TUNE))) return plan_one(c, jobs, njobs, p, out);
+    *out = nullptr;
+    const hj_tuner_t saved = c->tuner;
+    const double base = saved.nphj_max_table_bytes > 0 ? saved.nphj_max_table_bytes : 64e6;
+    const double scales[] = {1.0 / 32, 1.0 / 16, 0.125, 0.25, 0.5, 1.0, 2.0, 4.0};
+    hj_batch_t *best = nullptr;
+    double best_s = 1e300, best_budget = base;
+    std::vector<int> last_impl;
+    for (double sc : scales) {
+        hj_tuner_t t = saved;
+        t.nphj_max_table_bytes = base * sc;
+        t.calibrated = 0;  // the table-budget rule
+        c->tuner = t;
+        hj_batch_t *b = nullptr;
+        int rc = plan_one(c, jobs, njobs, p, &b);
+        if (rc) {
+            c->tuner = saved;
+            if (best) hj_batch_destroy(best);
+            return rc;
+        }
+        if (best && b->impl == last_impl) {  // same decisions as the previous budget: nothing to time
+            hj_batch_destroy(b);
+            continue;
+        }
+        last_impl = b->impl;
+        double s = 1e300;
+        for (int rep = 0; rep < 3 && !rc; rep++) {
+            hj_batch_stats_t st;
+            rc = hj_batch_run(b, nullptr, &st);
+            if (!rc && rep > 0) s = std::min(s, st.seconds);
+        }
+        if (rc) {
+            hj_batch_destroy(b);
+            c->tuner = saved;
+            if (best) hj_batch_destroy(best);
+            return rc;
+        }
+        if (s < best_s) {
+            if (best) hj_batch_destroy(best);
+            best = b;
+            best_s = s;
+            best_budget = t.nphj_max_table_bytes;
+        } else {
+            hj_batch_destroy(b);
+        }
+    }
+    c->tuner = saved;
+    c->tuner.nphj_max_table_bytes = best_budget;
+    c->tuner.calibrated = 0;
+    *out = best;
+    return HJ_OK;
+}
+
+static int plan_one(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_params_t *p, hj_batch_t **out) {
     if (!c || !out || njobs < 0 || (njobs && !jobs)) return HJ_E_INVAL;
     *out = nullptr;
     for (int j = 0; j < njobs; j++) {
@@ -490,7 +590,11 @@ int hj_batch_plan(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj_p
         return fail(HJ_E_OOM);
     }
     if (cudaMallocHost(&b->accs_host, sizeof(JoinAccum) * (njobs ? njobs : 1)) != cudaSuccess) return fail(HJ_E_OOM);
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(HJ_E_DEVICE);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream_phj, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        return fail(HJ_E_DEVICE);
     if (cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) return fail(HJ_E_DEVICE);
     char *cur = b->mem;
     b->accs = reinterpret_cast<JoinAccum *>(cur);
@@ -633,6 +737,9 @@ int hj_batch_destroy(hj_batch_t *b) {
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->stream_phj) cudaStreamDestroy(b->stream_phj);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
     delete b;
     return HJ_OK;
 }
@@ -665,13 +772,13 @@ int hj_tuner_calibrate(hj_ctx_t *c, double *report, int report_len) {
         return HJ_E_OOM;
     }
     hj_tuner_t saved = c->tuner;
-    double best_nphj_table = 0;
+    hj_tuner_t model = saved;
     int rc = HJ_OK;
     for (int q = 0; q < nl && !rc; q++) {
         const size_t nR = 1ull << logs[q], nS = 8 * nR;
         hj_gen_fast_device(nR, nS, 777 + q, 0, 1, R, S, nullptr);
         cudaDeviceSynchronize();
-        double t[2] = {1e30, 1e30};
+        double t[2] = {1e30, 1e30}, tb = 1e30, tpr = 1e30;
         for (int impl = 0; impl < 2 && !rc; impl++) {
             hj_params_t p;
             hj_params_init(&p);
@@ -693,21 +800,47 @@ int hj_tuner_calibrate(hj_ctx_t *c, double *report, int report_len) {
                 hj_result_t r;
                 rc = hj_join_ctx(c, algo, &p, R, nR, S, nS, &r);
                 if (rc) break;
-                if (rep > 0) t[impl] = std::min(t[impl], r.total);
+                if (rep > 0 && r.total < t[impl]) {
+                    t[impl] = r.total;
+                    if (impl == 0) {
+                        tb = r.buildpart;
+                        tpr = r.probejoin;
+                    }
+                }
             }
+        }
+        if (q < HJ_TUNER_LEVELS && !rc) {
+            model.level_nR[q] = (double)nR;
+            model.nphj_build[q] = tb / (double)nR;
+            model.nphj_probe[q] = tpr / (double)nS;
+            model.phj[q] = t[1];  // whole time for now: split into fixed + per tuple below
         }
         if (report && 3 * q + 2 < report_len) {
             report[3 * q] = (double)nR;
             report[3 * q + 1] = t[0];
             report[3 * q + 2] = t[1];
         }
-        if (t[0] <= t[1]) best_nphj_table = (double)nphj_slots(nR) * 16.0;
     }
     cudaFree(R);
     cudaFree(S);
     if (!rc) {
-        c->tuner.nphj_max_table_bytes = best_nphj_table;
-        c->tuner.calibrated = 1;
+        // Partitioned joins: the smallest size is dominated by the fixed cost; take as fixed cost what
+        // it took beyond the per-tuple rate of the largest size, and charge the rest per tuple.
+        const int last = std::min(nl, HJ_TUNER_LEVELS) - 1;
+        const double n0 = model.level_nR[0] * 9.0, nl_t = model.level_nR[last] * 9.0;
+        const double rate = model.phj[last] / nl_t;
+        double fixed = model.phj[0] - n0 * rate;
+        if (fixed < 0) fixed = 0;
+        model.phj_fixed = fixed;
+        for (int q = 0; q <= last; q++) {
+            const double n = model.level_nR[q] * 9.0;
+            const double per = (model.phj[q] - fixed) / n;
+            model.phj[q] = per > 0.25 * rate ? per : 0.25 * rate;
+        }
+        // The cost model decides per join; the table budget only bounds it to the sizes measured.
+        model.nphj_max_table_bytes = (double)nphj_slots(maxR) * 16.0;
+        model.calibrated = 1;
+        c->tuner = model;
     }
     if (dev_prev >= 0) cudaSetDevice(dev_prev);
     return rc;

@@ -221,12 +221,25 @@ void hj_pkfk_closed_form(size_t nR, size_t nS, uint64_t *matched, uint64_t *chec
  * radix-partitioned pipeline with its own radix bits; results always equal the named algorithm's.
  * -------------------------------------------------------------------------------------------- */
 #define HJ_F_NO_GRAPH 0x8u /* batches: launch the kernels one by one instead of one captured graph */
+#define HJ_F_TUNE 0x10u    /* batches: plan under a few table budgets around the tuner's, time each plan
+                              on the device (the joins run), keep the fastest and its budget */
+
+#define HJ_TUNER_LEVELS 8
 
 typedef struct {
     double nphj_max_table_bytes; /* joins whose global table (32 B per build tuple) fits run as nphj */
     double wave_table_bytes;     /* table bytes per wave of non-partitioned joins (a share of L2) */
     int partition_target;        /* partitioned joins: radix bits so build partitions hold ~this many */
-    int calibrated;              /* 1 after hj_tuner_calibrate */
+    int calibrated;              /* 1 after hj_tuner_calibrate: the cost model below decides */
+    /* Cost model measured by hj_tuner_calibrate at |R| = level_nR[i] (|S| = 8|R|): seconds per build
+     * tuple and per probe tuple of the non-partitioned join, seconds per tuple of the partitioned one
+     * beyond its fixed cost phj_fixed (the pipeline's ten-odd kernels). A join of (nR, nS) takes the
+     * level of its build size and runs non-partitioned when
+     * nR * nphj_build + nS * nphj_probe <= phj_fixed + (nR + nS) * phj (and its table fits
+     * nphj_max_table_bytes). */
+    double level_nR[HJ_TUNER_LEVELS];
+    double nphj_build[HJ_TUNER_LEVELS], nphj_probe[HJ_TUNER_LEVELS], phj[HJ_TUNER_LEVELS];
+    double phj_fixed;
 } hj_tuner_t;
 
 typedef struct {
@@ -259,8 +272,10 @@ int hj_tuner_get(hj_ctx_t *ctx, hj_tuner_t *out);
 int hj_tuner_set(hj_ctx_t *ctx, const hj_tuner_t *in);
 /* Decision for one join of the given sizes (impl 0/1 as in hj_batch_result_t). */
 int hj_tuner_decide(hj_ctx_t *ctx, size_t nR, size_t nS, int *impl, int *bits, int *passes);
-/* Time both implementations on PK-FK joins with |S| = 8|R|, |R| = 2^16..2^24, and set the table budget
- * to the largest build where the non-partitioned join won. report (optional) receives triples
+/* For single joins (hj_tuner_decide, the server): time both implementations on PK-FK joins with
+ * |S| = 8|R|, |R| = 2^16..2^24: fills the cost model
+ * (per-tuple build and probe costs of the non-partitioned join, per-tuple cost of the partitioned one)
+ * and sets the table budget to the largest table measured. report (optional) receives triples
  * (|R|, seconds non-partitioned, seconds partitioned). Allocates temporary device memory. */
 int hj_tuner_calibrate(hj_ctx_t *ctx, double *report, int report_len);
 /* Plan a batch: decisions, device memory for all of it, and (unless HJ_F_NO_GRAPH) the captured

@@ -75,3 +75,17 @@ def test_batch_empty_and_degenerate_jobs(hj, cuda):
     with hj.Context(0) as ctx, hj.Batch(ctx, jobs) as b:
         res, _ = b.run()
         assert [(r.matched_cnt, r.checksum) for r in res] == [(0, 0), (0, 0), (1, 100), (1, 100)]
+
+
+def test_batch_tuning_keeps_results(hj, oracle, cuda):
+    # HJ_F_TUNE plans the batch under several table budgets and keeps the fastest plan; whichever it
+    # keeps, every result is the oracle's and the tuner keeps the chosen budget.
+    jobs, host = _jobs(cuda, 7, 30)
+    with hj.Context(0) as ctx:
+        before = hj.tuner_get(ctx).nphj_max_table_bytes
+        with hj.Batch(ctx, jobs, tune=True) as b:
+            res, st = b.run()
+            for (algo, R, S), r, (_, Rh, Sh) in zip(jobs, res, host):
+                assert r.status == 0 and (r.matched_cnt, r.checksum) == oracle.join(algo, Rh, Sh)
+        after = hj.tuner_get(ctx).nphj_max_table_bytes
+        assert after in [before * f for f in (1 / 32, 1 / 16, 0.125, 0.25, 0.5, 1.0, 2.0, 4.0)]
