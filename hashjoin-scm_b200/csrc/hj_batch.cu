@@ -3,17 +3,21 @@
 // The reference runs one join per process invocation (src/main.c:429-448). A batch here takes N joins of
 // uneven sizes on device-resident relations and
 //   1. decides per join how to run it (the autotuner): joins whose global hash table (32 B per build
-//      tuple at load 0.5) fits the L2-sized budget run as non-partitioned joins; larger ones run the
+//      tuple at load 0.5) fits the table budget run as non-partitioned joins; larger ones run the
 //      radix-partitioned pipeline with radix bits chosen so build partitions hold about
 //      `partition_target` tuples (two passes above 8 bits). The join's result semantics - every match
-//      (nphj_sc, phj_radix_bc), first match (nphj_lp), first match with key 0 never matching
-//      (phj_radix_lp) - are kept whichever implementation runs, so results equal the named algorithm's;
-//   2. packs the non-partitioned joins into waves whose tables together stay within the budget, and
-//      runs each wave as one set of multi-join kernels over a flattened index space (build over all
+//      (nphj_sc, phj_radix_bc/sc/hr/hro), first match (nphj_lp), first match with key 0 never matching
+//      (phj_radix_lp) - are kept whichever implementation runs, so results equal the named algorithm's.
+//      With HJ_F_TUNE the budget is chosen by timing the batch's own graph under several budgets; a
+//      calibrated cost model (hj_tuner_calibrate) serves single joins;
+//   2. packs the non-partitioned joins into waves whose tables together stay within the wave budget,
+//      and runs each wave as one set of multi-join kernels over a flattened index space (build over all
 //      build tuples of the wave, then probe over all probe tuples), so the tables are still in L2 when
 //      probed;
-//   3. enqueues the partitioned joins one after another on the same stream, sharing one scratch area;
-//   4. captures the whole sequence in a CUDA graph once, so a run is one graph launch.
+//   3. enqueues the partitioned joins one after another on a second stream forked from the first
+//      (sharing one scratch area), so they overlap the waves;
+//   4. captures the whole sequence in a CUDA graph once (two parallel branches), so a run is one graph
+//      launch.
 #include <algorithm>
 #include <chrono>
 #include <cmath>

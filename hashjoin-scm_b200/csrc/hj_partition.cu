@@ -11,24 +11,32 @@
 //           which is the first R tuple of the partition in input order.
 //
 // B200 pipeline (one stream, no host round trip). Each relation is cut into equal chunks (about three
-// per SM); a chunk plays the role of one reference thread's contiguous input slice.
+// per SM) and each chunk into ~32 sub-chunks; a chunk plays the role of one reference thread's
+// contiguous input slice.
 //   hist_chunk_kernel  one read of R and S: per chunk, the joint histogram of the low B key bits (the
-//                      pass-1 digit and the pass-2 digit together) in shared memory
+//                      pass-1 digit and the pass-2 digit together) in shared memory; per sub-chunk (one
+//                      warp each) the histogram of the pass-1 digit
 //   colscan_kernel     per bin, exclusive prefix over the chunks of a relation (the reference's
 //                      cross-thread output_offset sums, phj.c:188-200, for both passes at once)
 //   plan_kernel        final partition starts, join work items, large partitions
-//   units_kernel       per (chunk, pass-1 partition): its size and its start in the pass-1 output
-//   scatter_kernel     per pass: persistent CTAs take work items (pass 1: chunks; pass 2: (chunk,
+//   units_kernel       per (chunk, pass-1 partition): its size and its start in the pass-1 output; per
+//                      sub-chunk its start within that
+//   scatter_kernel     per pass: persistent CTAs take work items (pass 1: sub-chunks; pass 2: (chunk,
 //                      pass-1 partition) units) whose per-digit output offsets are known in advance;
-//                      each 2048-tuple tile arrives by a TMA bulk copy (the next one is in flight while the
-//                      current one is processed), is ranked per digit with warp match (stable), staged
-//                      in shared memory sorted by digit and written back as coalesced 16-byte streaming
-//                      stores per digit run (the shared-memory analogue of the reference's SWWCB +
-//                      non-temporal flush). No inter-CTA waiting.
-//   join_small         persistent CTAs take (partition, S chunk) items; R_p arrives in shared memory by one
-//                      TMA bulk copy; the bucket chains (u16 head/next) are built with shared-memory atomics;
-//                      S is streamed with evict-first vector loads
+//                      each 2048-tuple tile arrives by a TMA bulk copy (the next one is in flight while
+//                      the current one is processed), is ranked per digit (one shared-memory atomic per
+//                      tuple; stably with bit ballots for the lp joins, whose result depends on input
+//                      order), staged in shared memory sorted by digit and written back as coalesced
+//                      16-byte streaming stores per digit run (the shared-memory analogue of the
+//                      reference's SWWCB + non-temporal flush). No inter-CTA waiting.
+//   join_compact       when keys (after the radix shift) and row ids fit 32 bits: persistent CTAs take
+//                      (partition, S chunk) items; 12-byte table entries with u16 bucket heads and chains
+//                      built by shared-memory atomics; S streamed with evict-first vector loads
+//   join_small         the general case: R_p arrives in shared memory by one TMA bulk copy, 16-byte
+//                      entries, u16 head/next chains
 //   join_large_*       partitions whose R side exceeds shared memory: chains in global memory
+// The join kernels have a materialising variant (MAT) for the ptr_* joins: one (r.row_id, s.row_id)
+// pair per match instead of the sums.
 #include <cstdio>
 
 #include "hj_common.cuh"
