@@ -269,12 +269,21 @@ def phj_literal(bits: int, passes: int, lp: bool, R: np.ndarray, S: np.ndarray) 
 # ------------------------------------------------------------------------------------------------
 # The reference itself (oracle/_ref, built from its sources by oracle/Makefile)
 # ------------------------------------------------------------------------------------------------
+# Where the reference's sources are mounted in the build container (oracle/Makefile's REF); the GPU
+# machines have only the binaries built from them.
+REF_SOURCES = pathlib.Path("/root/reference/src")
+
+
+def ref_sources_present() -> bool:
+    return REF_SOURCES.exists()
+
+
 def ref_available(passes: int = 2) -> bool:
     return (REF_DIR / f"hjref_p{passes}").exists()
 
 
 def ref_build() -> bool:
-    if not pathlib.Path("/root/reference/src").exists():
+    if not ref_sources_present():
         return ref_available(1) and ref_available(2)
     out = subprocess.run(["make", "-C", str(HERE), "ref"], capture_output=True, text=True)
     return out.returncode == 0

@@ -1,6 +1,6 @@
 /*
  * ref_driver.c - command-line driver around the reference's own join and generator functions, built
- * from the reference sources by oracle/Makefile into oracle/_ref. TEST / BASELINE INFRASTRUCTURE ONLY.
+ * from the reference sources by oracle/Makefile into oracle/_ref. TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.
  *
  * It replaces src/main.c's libconfig-driven setup (src/main.c:147-255) with flags and calls the
  * reference functions unmodified:

@@ -12,6 +12,18 @@ import json
 import os
 import pathlib
 
+def _load_oracle_module():
+    import importlib.util
+
+    root = pathlib.Path(__file__).resolve().parents[1]
+    spec = importlib.util.spec_from_file_location("hj_oracle_probe", root / "oracle" / "hj_oracle.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_REF_SOURCES = _load_oracle_module().ref_sources_present()
+
 import numpy as np
 import pytest
 
@@ -150,7 +162,7 @@ def test_key_zero_rule(oracle):
     assert oracle.join(oracle.FIRST_NP, R, S) == (2, 5 + 100 + 7 + 200)
 
 
-@pytest.mark.skipif(not pathlib.Path("/root/reference/src").exists(), reason="reference sources absent")
+@pytest.mark.skipif(not _REF_SOURCES, reason="reference sources absent")
 def test_oracle_matches_reference_binary_random(oracle):
     """Random keys with heavy duplication, straight through the reference's own joins."""
     if not (oracle.ref_available(1) and oracle.ref_available(2)):
@@ -166,7 +178,7 @@ def test_oracle_matches_reference_binary_random(oracle):
     assert oracle.ref_join("nphj_lp", R, S, threads=1) == oracle.join("nphj_lp", R, S)
 
 
-@pytest.mark.skipif(not pathlib.Path("/root/reference/src").exists(), reason="reference sources absent")
+@pytest.mark.skipif(not _REF_SOURCES, reason="reference sources absent")
 def test_reference_sc_hr_hro_and_asymm_equal_bc(oracle):
     """The reference's separate-chaining, histogram-sorted and AVX-512 partition joins, and its
     asymmetric-radix joins, return bc_join's count and checksum: the claim the library's phj_radix_sc /
@@ -195,7 +207,7 @@ def test_reference_sc_hr_hro_and_asymm_equal_bc(oracle):
             assert oracle.ref_join(algo, R2, S, bits=bits, passes=2, threads=4, bits1=bits1) == want2, (algo, bits)
 
 
-@pytest.mark.skipif(not pathlib.Path("/root/reference/src").exists(), reason="reference sources absent")
+@pytest.mark.skipif(not _REF_SOURCES, reason="reference sources absent")
 def test_reference_ptr_joins_equal_definition(hj, oracle):
     """The reference's materialising joins (pairs, then the retrieve checksum) on payload PK-FK data equal
     the definition, and so does the pairs oracle. One thread: the reference sizes each thread's pair
