@@ -152,6 +152,8 @@ def lib() -> ctypes.CDLL:
     L.hj_join_mat_ctx.restype = i32
     L.hj_join_mat.argtypes = [i32, ctypes.POINTER(Params), vp, sz, vp, sz, vp, sz, ctypes.POINTER(Result)]
     L.hj_join_mat.restype = i32
+    L.hj_join_streamed.argtypes = [vp, i32, ctypes.POINTER(Params), vp, sz, vp, sz, sz, ctypes.POINTER(Result)]
+    L.hj_join_streamed.restype = i32
     L.hj_gen_pkfk_uniform.argtypes = [sz, sz, ctypes.c_uint, i32, vp, vp]
     L.hj_gen_pkfk_uniform.restype = i32
     L.hj_gen_dup_uniform.argtypes = [sz, sz, ctypes.c_uint, vp, vp]
@@ -251,6 +253,26 @@ def join_mat(algo: str, R, S, *, pairs=None, pair_cap: int | None = None, bits: 
         rc = L.hj_join_mat_ctx(ctx.handle, a, ctypes.byref(p), pr, nr, ps, ns, pp, cap, ctypes.byref(res))
     else:
         rc = L.hj_join_mat(a, ctypes.byref(p), pr, nr, ps, ns, pp, cap, ctypes.byref(res))
+    if check and rc != 0:
+        raise JoinError(rc, algo)
+    res.status = rc
+    return res
+
+
+def join_streamed(algo: str, R, S, ctx: "Context", *, chunk_tuples: int = 0, bits: int = 14, passes: int = 2,
+                  flags: int = 0, load: float = 0.5, check: bool = True, bits_pass1: int | None = None) -> Result:
+    """Streamed join (hj_join_streamed): R stays on the device, S streams from host memory in chunks.
+    R and S are host relations: numpy (n, 2) uint64 arrays or (pointer, n) pairs (pinned memory copies
+    at full link speed)."""
+    L = lib()
+    a = ALGOS[algo]
+    if bits_pass1 is None:
+        bits_pass1 = ASYMM_DEFAULT_BITS_PASS1 if algo.startswith("phj_asymm_radix") else 0
+    p = make_params(bits, passes, ctx.device, False, None, flags, load, bits_pass1)
+    pr, nr = _ptr_len(R, False)
+    ps, ns = _ptr_len(S, False)
+    res = Result()
+    rc = L.hj_join_streamed(ctx.handle, a, ctypes.byref(p), pr, nr, ps, ns, chunk_tuples, ctypes.byref(res))
     if check and rc != 0:
         raise JoinError(rc, algo)
     res.status = rc

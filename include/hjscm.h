@@ -177,6 +177,17 @@ int hj_join_mat_ctx(hj_ctx_t *ctx, hj_algo_t algo, const hj_params_t *p, const h
 int hj_join_mat(hj_algo_t algo, const hj_params_t *p, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,
                 size_t nS, hj_pair_t *pairs, size_t pair_cap, hj_result_t *out);
 
+/* Streamed join for relations beyond what hj_join holds in device memory (both relations plus two
+ * partition buffers): the build relation R is copied to the device once, the probe relation S streams
+ * from host memory in chunks of chunk_tuples (0: the largest that fits) through two device buffers, so
+ * the copy of one chunk overlaps the join of the previous one; each chunk is joined with all of R and
+ * the counts and checksums add up to hj_join's result. R and S are host pointers (pinned memory copies
+ * at full link speed), p->inputs_on_device must be 0. out->total covers the copies and the joins. This
+ * is the device-side counterpart of the reference's billion-scale workloads (2^30 x 2^34 tuples,
+ * config/billion-data), whose probe side no single device holds. */
+int hj_join_streamed(hj_ctx_t *ctx, hj_algo_t algo, const hj_params_t *p, const hj_tuple_t *R, size_t nR,
+                     const hj_tuple_t *S, size_t nS, size_t chunk_tuples, hj_result_t *out);
+
 /* ----------------------------------------------------------------------------------------------
  * Data generation. The seeded generators replay the reference's src/gen.c exactly (glibc srand/rand,
  * Knuth shuffle), so the relations are byte-identical to the .bin files bin/gen writes.
