@@ -71,6 +71,8 @@ def parse_args():
     ap.add_argument("--ns-log", type=int, default=29)
     ap.add_argument("--bits", type=int, default=14)
     ap.add_argument("--passes", type=int, default=2)
+    ap.add_argument("--pipeline", choices=["auto", "segments", "exact"], default="auto",
+                    help="radix joins: segment mode (no histogram pass) by size, always, or never")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -285,7 +287,8 @@ def run_ours(a, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     want = hj.pkfk_closed_form(nR, nS)
     ctx = hj.Context(local_rank)
-    flags = hj.HJ_F_PHASE_TIMES
+    pipe_flag = {"auto": 0, "segments": hj.HJ_F_SEGMENTS, "exact": hj.HJ_F_EXACT}[a.pipeline]
+    flags = hj.HJ_F_PHASE_TIMES | pipe_flag
 
     def step():
         r = hj.join(a.algo, R, S, on_device=True, bits=a.bits, passes=a.passes, device=local_rank,
@@ -321,6 +324,7 @@ def run_ours(a, rank, world, local_rank):
     value = whole_job_rate((nR + nS) * a.steps, world, ms / 1e3)
     phases = {name: statistics.mean(r.phase[i] for r in results) for i, name in enumerate(hj.PHASES)}
     launches = sum(r.kernel_launches for r in results)
+    seg_mode = a.algo.startswith("phj") and phases["hist"] == 0.0
 
     # Roofline of the dominant kernel. Radix joins: a partition pass reads and writes every tuple once
     # (32 B); the pipeline with P materialised passes moves 16 (2P + 1) B per tuple. Non-partitioned
@@ -334,7 +338,9 @@ def run_ours(a, rank, world, local_rank):
         achieved = scatter_bytes / pass_s / 1e9
         prof = traffic_profile("scatter_kernel")
         traffic = prof["dram_bytes_per_tuple"] * (nR + nS) if prof else None
-        roofline = {"kernel": "scatter_kernel (one radix partition pass)", "bound": "hbm",
+        kname = ("seg_pass1_kernel / scatter_kernel (mean of the two radix partition passes)" if seg_mode
+                 else "scatter_kernel (one radix partition pass)")
+        roofline = {"kernel": kname, "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": peak_kind, "traffic": traffic,
                     "algorithmic_bytes_per_launch": scatter_bytes, "launch_ms": pass_s * 1e3}
@@ -365,7 +371,7 @@ def run_ours(a, rank, world, local_rank):
 
         def e2e_step():
             r = hj.join(a.algo, (Rh.data_ptr(), nR), (Sh.data_ptr(), nS), bits=a.bits, passes=a.passes,
-                        device=local_rank, flags=hj.HJ_F_PINNED_HOST, ctx=host_ctx)
+                        device=local_rank, flags=hj.HJ_F_PINNED_HOST | pipe_flag, ctx=host_ctx)
             if (r.matched_cnt, r.checksum) != want:
                 raise RuntimeError("wrong e2e result")
             return r
@@ -396,7 +402,12 @@ def run_ours(a, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": workload_config(a, world),
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": dict(workload_config(a, world),
+                           **({"partition_pipeline": "segment mode: pass 1 writes segment chains and counts "
+                               "the histograms (no histogram pass)" if seg_mode else
+                               "exact offsets: histogram pass, then two scatter passes"}
+                              if a.algo.startswith("phj") else {})),
             "roofline": roofline, "pipeline": pipeline, "e2e": e2e, "cpu_baseline": cpu,
             "clocks": clocks, "gpu_launches": launches,
         }

@@ -58,15 +58,22 @@ void resolve_params(const hj_params_t *p, hj_params_t *out) {
 
 bool is_phj(hj_algo_t a) { return hj::algo_is_phj(a); }
 
+// Segment mode for a radix join (see HJ_F_SEGMENTS): by size unless a flag decides.
+bool want_seg(hj_algo_t algo, const hj_params_t &p, const hj::RadixGeom &g, size_t nR, size_t nS) {
+    if (!is_phj(algo) || (p.flags & HJ_F_EXACT)) return false;
+    if (p.flags & HJ_F_SEGMENTS) return hj::phj_seg_applies(g, hj::algo_lp(algo), 1ull << 40, 0);
+    return hj::phj_seg_applies(g, hj::algo_lp(algo), nR, nS);
+}
+
 int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, bool host_inputs, int num_sms,
-                 size_t *bytes) {
+                 size_t *bytes, bool seg) {
     size_t need = kAccBytes;
     if (host_inputs) need += align256(nR * 16) + align256(nS * 16);
     if (is_phj(algo)) {
         hj::RadixGeom g;
         int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &g, p.radix_bits_pass1);
         if (rc) return rc;
-        need += hj::phj_scratch_bytes(g, nR, nS, num_sms);
+        need += hj::phj_scratch_bytes(g, nR, nS, num_sms, seg);
     } else {
         need += align256(hj::nphj_scratch_bytes(nR, p.table_load));
     }
@@ -220,11 +227,23 @@ int hj_ctx_reserve(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, size_t n
     hj_params_t p;
     resolve_params(pin, &p);
     size_t need = 0;
-    int rc = scratch_need(algo, p, nR, nS, !p.inputs_on_device, c->num_sms, &need);
+    bool seg = false;
+    if (is_phj(algo)) {
+        hj::RadixGeom geom;
+        const int rc = hj::radix_geom(p.num_radix_bits, p.num_passes, &geom, p.radix_bits_pass1);
+        if (rc) return rc;
+        seg = want_seg(algo, p, geom, nR, nS);
+    }
+    int rc = scratch_need(algo, p, nR, nS, !p.inputs_on_device, c->num_sms, &need, seg);
     if (rc) return rc;
     DeviceGuard g(c->device);
     std::lock_guard<std::mutex> lk(c->mu);
-    return ensure_arena(c, need);
+    rc = ensure_arena(c, need);
+    if (rc == HJ_E_OOM && seg) {
+        rc = scratch_need(algo, p, nR, nS, !p.inputs_on_device, c->num_sms, &need, false);
+        if (!rc) rc = ensure_arena(c, need);
+    }
+    return rc;
 }
 
 int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tuple_t *R, size_t nR,
@@ -247,9 +266,15 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     std::lock_guard<std::mutex> lk(c->mu);
     const bool host_in = !p.inputs_on_device;
     size_t need = 0;
-    int rc = scratch_need(algo, p, nR, nS, host_in, c->num_sms, &need);
+    bool seg = want_seg(algo, p, geom, nR, nS);
+    int rc = scratch_need(algo, p, nR, nS, host_in, c->num_sms, &need, seg);
     if (rc) return out->status = rc;
     rc = ensure_arena(c, need);
+    if (rc == HJ_E_OOM && seg) {  // the exact-offset pipeline needs less memory
+        seg = false;
+        rc = scratch_need(algo, p, nR, nS, host_in, c->num_sms, &need, false);
+        if (!rc) rc = ensure_arena(c, need);
+    }
     if (rc) return out->status = rc;
     cudaStream_t st = p.stream ? (cudaStream_t)p.stream : c->stream;
     // A join that a watchdog gave up on may still run; its arena use must end before this one starts.
@@ -279,7 +304,7 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     if (timing) CU_OR(cudaEventRecord(c->ev_start, st), out->status = HJ_E_DEVICE);
     if (is_phj(algo)) {
         hj::PhjScratch s;
-        hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s);
+        hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s, seg);
         rc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
                              timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches, nullptr,
                              (p.flags & HJ_F_TEST_STALL) ? 1 : 0);
@@ -325,7 +350,8 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     if (phases) {
         for (int i = 0; i < HJ_PH_COUNT; i++) {
             float ms = 0;
-            cudaEventElapsedTime(&ms, c->ev_ph[i], c->ev_ph[i + 1]);
+            int from = 0, to = 0;
+            if (hj::phj_phase_span(seg, i, &from, &to)) cudaEventElapsedTime(&ms, c->ev_ph[from], c->ev_ph[to]);
             out->phase[i] = ms * 1e-3;
         }
     }
@@ -352,14 +378,22 @@ static int join_mat(hj_ctx *c, hj_algo_t algo, const hj_params_t &p, const hj_tu
     // buffer).
     const bool pairs_in_arena = !user_pairs || host_in;
     const unsigned long long cap = user_pairs ? (unsigned long long)user_cap : cap_guess;
-    size_t need = kAccBytes;
-    if (host_in) need += align256(nR * 16) + align256(nS * 16);
-    if (is_phj(algo))
-        need += hj::phj_scratch_bytes(geom, nR, nS, c->num_sms);
-    else
-        need += align256(hj::nphj_scratch_bytes(nR, p.table_load, true));
-    if (pairs_in_arena) need += align256(cap * 16);
-    int rc = ensure_arena(c, need);
+    bool seg = want_seg(algo, p, geom, nR, nS);
+    auto need_of = [&](bool sg) {
+        size_t need = kAccBytes;
+        if (host_in) need += align256(nR * 16) + align256(nS * 16);
+        if (is_phj(algo))
+            need += hj::phj_scratch_bytes(geom, nR, nS, c->num_sms, sg);
+        else
+            need += align256(hj::nphj_scratch_bytes(nR, p.table_load, true));
+        if (pairs_in_arena) need += align256(cap * 16);
+        return need;
+    };
+    int rc = ensure_arena(c, need_of(seg));
+    if (rc == HJ_E_OOM && seg) {
+        seg = false;
+        rc = ensure_arena(c, need_of(false));
+    }
     if (rc) return out->status = rc;
     cudaStream_t st = p.stream ? (cudaStream_t)p.stream : c->stream;
     CU_OR(cudaStreamWaitEvent(st, c->ev_done, 0), out->status = HJ_E_DEVICE);
@@ -394,7 +428,7 @@ static int join_mat(hj_ctx *c, hj_algo_t algo, const hj_params_t &p, const hj_tu
     if (timing) CU_OR(cudaEventRecord(c->ev_start, st), out->status = HJ_E_DEVICE);
     if (is_phj(algo)) {
         hj::PhjScratch s;
-        hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s);
+        hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s, seg);
         rc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
                              timing ? c->ev_mid : nullptr, c->num_sms, nullptr, &launches, &mat);
     } else {

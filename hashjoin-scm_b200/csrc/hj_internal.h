@@ -62,23 +62,41 @@ struct PhjScratch {
     size_t max_large;
     uint32_t *large_table;   // head/next chains for large partitions (>= 12 B per R tuple)
     size_t large_table_words;
-    ulonglong2 *tmp1;        // pass-1 output [nR + nS]
+    ulonglong2 *tmp1;        // pass-1 output [nR + nS]; segment storage [max_segs * kTile] in segment mode
     ulonglong2 *tmp2;        // pass-2 output [nR + nS] (== tmp1 for one pass)
+    // Segment mode (phj_seg_applies): pass 1 writes chains of kTile-tuple segments and counts the
+    // histograms itself, so no histogram pass reads the relations first. "Chunks" are then the pass-1
+    // CTAs: cR = cS = seg_grid.
+    bool seg;
+    uint32_t seg_grid;       // pass-1 CTAs
+    uint32_t max_segs;       // segments that tmp1 holds
+    uint32_t it_tiles;       // tiles per pass-1 work item
+    uint32_t *seg_head;      // [2 * seg_grid][F1] first segment of (CTA, relation, pass-1 digit)
+    uint32_t *seg_next;      // [max_segs] next segment of the same chain
 };
+
+// Segment mode applies to the joins that count every match (the order of tuples within a partition
+// does not matter), two physical passes, at most 14 radix bits, and relations large enough that the
+// histogram read it saves outweighs the memory it reserves (one partly filled segment per CTA,
+// relation and pass-1 digit).
+bool phj_seg_applies(const RadixGeom &g, bool lp, size_t nR, size_t nS);
 
 // Kernel attributes (dynamic shared memory limits) for the current device; phj_enqueue calls it too,
 // but callers that capture a stream into a graph call it before the capture.
 int phj_prepare_device();
 
-size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms);
-void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base, PhjScratch *s);
+// seg: lay the scratch out for segment mode (callers pass phj_seg_applies(...) or false).
+size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms, bool seg = false);
+void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base, PhjScratch *s, bool seg = false);
 
 // Result semantics: lp = first match per probe tuple (lowest build position) instead of all matches;
 // skip0 = build tuples with key 0 never match (the phj_radix_lp empty-slot rule, src/algo/phj.c:614).
 // Enqueue a full partitioned join on `st`; matches/checksum accumulate into acc (zeroed by caller).
 // ev_mid, if non-null, is recorded between the partition phase and the join phase.
-// ph, if non-null, holds HJ_PH_COUNT + 1 events recorded at the phase boundaries; *launches receives
-// the number of kernels enqueued.
+// ph, if non-null, holds HJ_PH_COUNT + 1 events recorded at the phase boundaries (in segment mode,
+// see phj_phase_span, in a different order); *launches receives the number of kernels enqueued.
+// A scratch carved for segment mode runs in segment mode unless lp is set; lp then runs the
+// exact-offset pipeline, which a segment-mode scratch does not fit: carve it with seg = false.
 // mat, if non-null, makes the join write one (r.row_id, s.row_id) pair per match into mat->pairs
 // (slots counted in acc->pairs) instead of summing row ids. test_flags bit 0: the partition pass's
 // first CTA withholds one tile load, so its bounded wait expires (failure-detection tests).
@@ -86,6 +104,22 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr,
                 int test_flags = 0);
+
+// The events of phase slot i (HJ_PH_*) that phj_enqueue recorded: elapsed(ph[*from], ph[*to]);
+// false for a slot that the mode does not time (segment mode has no histogram pass).
+inline bool phj_phase_span(bool seg_mode, int i, int *from, int *to) {
+    if (!seg_mode) {
+        *from = i;
+        *to = i + 1;
+        return true;
+    }
+    // Segment mode records: start, pass 1, plan, pass 2, joins, large joins.
+    static const int kFrom[HJ_PH_COUNT] = {-1, 1, 0, 2, 3, 4};
+    if (i < 0 || i >= HJ_PH_COUNT || kFrom[i] < 0) return false;
+    *from = kFrom[i];
+    *to = kFrom[i] + 1;
+    return true;
+}
 
 // Non-partitioned joins on a global open-addressing table.
 // mat: as for phj_enqueue; a materialising join needs nphj_scratch_bytes(nR, load, true).

@@ -70,6 +70,7 @@ enum : int {
     kCtrItem2 = 1,       // scatter pass-2 work-item counter
     kCtrNItemsA = 2,     // join items whose build side fits the compact shared-memory table (listed first)
     kCtrItemA = 3,       // compact join work-item counter
+    kCtrSegAlloc = 4,    // segment mode: segment ids handed out
     kCtrNItems = 6,
     kCtrNLarge = 7,
     kCtrItem = 8,        // join work-item counter
@@ -527,7 +528,7 @@ __global__ void units_kernel(const uint32_t *__restrict__ chunk_hist, const uint
         sh[(size_t)j * F1] = run;
         run += x;
     }
-    if (run != (uint32_t)cnt) set_error(err, kErrCapacity);
+    if (cg.spc && run != (uint32_t)cnt) set_error(err, kErrCapacity);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -547,6 +548,11 @@ struct ScatterArgs {
     const uint64_t *unit_off;   // [chunk][F1]
     const uint32_t *unit_cnt;   // [chunk][F1]
     const uint32_t *subpre;     // [chunk][spc][F1] start of (sub-chunk, d1) within (chunk, d1)
+    // Segment mode, pass 2: unit (chunk, d1) is a chain of kTile-tuple segments in inR (the pass-1
+    // output of both relations): seg_head[unit], then seg_next[segment]; all but the last are full.
+    const uint32_t *seg_head;   // nullptr: units are contiguous ranges (unit_off)
+    const uint32_t *seg_next;
+    uint32_t max_segs;
     int test_stall;             // test hook: CTA 0 withholds its first tile load (its wait must expire)
     uint32_t *counters;
     int ctr_item;
@@ -569,6 +575,7 @@ struct ItemIter {
     const tuple_v *in = nullptr;
     tuple_v *out = nullptr;
     uint64_t len = 0, out_len = 0, done = 0;
+    uint32_t seg = 0;   // segment mode: segment of the next tile
 };
 
 __device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item, ItemIter &it) {
@@ -592,42 +599,59 @@ __device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item,
         const uint32_t c = item / a.F1;
         const int rel = c < cg.cR ? 0 : 1;
         it.len = a.unit_cnt[item];
-        it.in = (rel ? a.inS : a.inR) + a.unit_off[item];
+        if (a.seg_head) {
+            it.in = a.inR;
+            it.seg = it.len ? a.seg_head[item] : 0u;
+        } else {
+            it.in = (rel ? a.inS : a.inR) + a.unit_off[item];
+        }
         it.out = rel ? a.outS : a.outR;
         it.out_len = rel ? a.nS : a.nR;
     }
 }
 
 // Claim the next tile (thread 0 only): continue the current item or claim new items until one has
-// tuples. Returns a slot with item == ~0u when the work is exhausted.
+// tuples. Returns a slot with item == ~0u when the work is exhausted. Segment mode: `pend` carries
+// seg_next of the tile returned last, loaded then so that its latency passes while that tile is
+// processed.
 template <int T>
-__device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it, uint32_t nitems) {
+__device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it, uint32_t nitems,
+                                              uint32_t &pend) {
     TileSlot s;
-    while (it.item == ~0u || it.done >= it.len) {
-        const uint32_t item = atomicAdd(&a.counters[a.ctr_item], 1u);
-        if (item >= nitems) {
-            s.item = ~0u;
-            s.in = nullptr;
-            s.out = nullptr;
-            s.out_len = 0;
-            s.cnt = 0;
-            s.first = 0;
-            s.pad = 0;
-            it.item = ~0u;
-            it.len = 0;
-            it.done = 0;
-            return s;
+    if (a.seg_head && it.item != ~0u && it.done > 0 && it.done < it.len) it.seg = pend;
+    for (;;) {
+        while (it.item == ~0u || it.done >= it.len) {
+            const uint32_t item = atomicAdd(&a.counters[a.ctr_item], 1u);
+            if (item >= nitems) {
+                s.item = ~0u;
+                s.in = nullptr;
+                s.out = nullptr;
+                s.out_len = 0;
+                s.cnt = 0;
+                s.first = 0;
+                s.pad = 0;
+                it.item = ~0u;
+                it.len = 0;
+                it.done = 0;
+                return s;
+            }
+            item_decode(a, item, it);
         }
-        item_decode(a, item, it);
+        if (!a.seg_head) break;
+        if (it.seg < a.max_segs) break;
+        // A chain that leaves the segment storage (pass 1 stopped early): drop the rest of the unit.
+        set_error(&a.counters[kCtrErr], kErrCapacity);
+        it.done = it.len;
     }
     s.item = it.item;
-    s.in = it.in + it.done;
+    s.in = a.seg_head ? it.in + (uint64_t)it.seg * T : it.in + it.done;
     s.out = it.out;
     s.out_len = it.out_len;
     s.cnt = (uint32_t)(it.len - it.done < (uint64_t)T ? it.len - it.done : (uint64_t)T);
     s.first = it.done == 0;
     s.pad = 0;
     it.done += s.cnt;
+    if (a.seg_head && it.done < it.len) pend = a.seg_next[it.seg];
     return s;
 }
 
@@ -662,6 +686,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     const uint32_t bar0 = smem_addr(&bars[0]);
     const int nbins = 1 << a.bits;
     __shared__ ItemIter it;  // used by thread 0 only
+    uint32_t pend = 0;       // thread 0: next segment of the chain (segment mode)
 
     if (!STABLE)
         for (int j = tid; j < 256; j += THREADS) thist[j] = 0;
@@ -671,7 +696,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         if (NBUF == 2) {
-            const TileSlot s0 = next_tile<T>(a, it, nitems);
+            const TileSlot s0 = next_tile<T>(a, it, nitems, pend);
             slots[0] = s0;
             if (s0.item != ~0u && !(a.test_stall && blockIdx.x == 0)) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
         }
@@ -684,7 +709,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             // One buffer: load this tile now (the barrier that ended the previous iteration ordered
             // every read of the buffer before this copy).
             if (tid == 0) {
-                const TileSlot sn = next_tile<T>(a, it, nitems);
+                const TileSlot sn = next_tile<T>(a, it, nitems, pend);
                 slots[0] = sn;
                 if (sn.item != ~0u && !(a.test_stall && blockIdx.x == 0 && k == 0))
                     tma_load_1d(inbuf, sn.in, sn.cnt * 16u, bar0);
@@ -697,7 +722,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         // Prefetch the next tile into the other buffer; the barrier that ended the previous iteration
         // ordered every read of it before this copy.
         if (NBUF == 2 && tid == 0) {
-            const TileSlot sn = next_tile<T>(a, it, nitems);
+            const TileSlot sn = next_tile<T>(a, it, nitems, pend);
             slots[cur ^ 1u] = sn;
             if (sn.item != ~0u) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
         }
@@ -867,6 +892,394 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
                 set_error(err, kErrBounds);
         }
         __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// 5b. Segment mode, pass 1: partition into chains of segments, counting the histograms on the way.
+//
+// The exact-offset pipeline reads both relations once for histograms before pass 1 may write. For
+// the joins that count every match, the order of tuples within a partition does not matter, and
+// pass 1 can write without knowing offsets: every (CTA, relation, pass-1 digit) owns a chain of
+// kTile-tuple segments, taken from a global counter (in slabs of kSegSlab per CTA), filled in order
+// and linked through seg_next. Since a tile holds at most kTile tuples of one digit, a tile's run of
+// a digit ends the current segment at most once. The same CTA counts the joint histogram of the low
+// `bits` key bits of its tuples in 16-bit counters (two per word), and adds them to its row of hist
+// when the relation ends. No counter overflows: `since` bounds every counter (a tile adds at most its
+// size), and before a tile could take the bound past 65535 the CTA moves every counter above
+// kSegSpillAt into its row and sets the bound to the largest counter left. That gives pass 2 its exact
+// offsets: pass 2 takes (CTA, digit) chains as its units and writes the final partitions as in the
+// exact-offset pipeline.
+// ------------------------------------------------------------------------------------------------
+constexpr uint32_t kSegNone = 0xffffffffu;
+constexpr uint32_t kSegSlab = 32;          // segment ids a CTA takes from the global counter at once
+constexpr int kSegCtasPerSm = 2;           // shared memory: two tile buffers + 32 KB of counters
+constexpr int kSegMaxBits = 14;
+constexpr uint32_t kSegSpillAt = 8192;
+
+struct SegArgs {
+    const tuple_v *R, *S;
+    uint64_t nR, nS;
+    int bits, F1;              // joint bins 2^bits; pass-1 digit = key & (F1 - 1)
+    uint32_t it_tiles;         // tiles per work item
+    uint32_t tilesR, tilesS;   // tiles of each relation
+    uint32_t itemsR, items;    // items of R (first), all items
+    tuple_v *out;              // segment storage: segment i holds tuples [i*kTile, (i+1)*kTile)
+    uint32_t max_segs;
+    uint32_t *seg_head;        // [2*grid][F1]
+    uint32_t *seg_next;        // [max_segs]
+    uint32_t *hist;            // [2*grid][2^bits]: row c = R tuples of CTA c, row grid + c = its S tuples
+    uint32_t *counters;        // kCtrItem1 (items), kCtrSegAlloc, kCtrErr, kCtrMaxKey/kCtrMaxRid
+    int test_stall;            // test hook: CTA 0 withholds its first tile load (its wait must expire)
+};
+
+struct SegSlot {
+    const tuple_v *in;
+    uint32_t cnt;              // tuples in the tile (0: no more tiles)
+    int rel;
+};
+
+// Where a digit's run of the staged tile goes: staged index j < split to base + j (the rest of the
+// current segment), j >= split to base + j + jump * kTile (the new segment).
+struct SegRun {
+    long long base;
+    int jump;
+    uint32_t split;
+};
+
+// Thread 0: the next tile of this CTA's current work item, claiming items as needed.
+__device__ __forceinline__ SegSlot seg_next_tile(const SegArgs &a, uint32_t &item, uint32_t &t_next,
+                                                 uint32_t &t_end) {
+    SegSlot s;
+    while (item == ~0u || t_next >= t_end) {
+        item = atomicAdd(&a.counters[kCtrItem1], 1u);
+        if (item >= a.items) {
+            item = ~0u;
+            s.in = nullptr;
+            s.cnt = 0;
+            s.rel = 0;
+            return s;
+        }
+        const bool rel = item >= a.itemsR;
+        const uint32_t k = rel ? item - a.itemsR : item;
+        const uint32_t nt = rel ? a.tilesS : a.tilesR;
+        t_next = k * a.it_tiles;
+        t_end = t_next + a.it_tiles < nt ? t_next + a.it_tiles : nt;
+    }
+    const bool rel = item >= a.itemsR;
+    const uint64_t n = rel ? a.nS : a.nR;
+    const uint64_t lo = (uint64_t)t_next * kTile;
+    s.in = (rel ? a.S : a.R) + lo;
+    s.cnt = (uint32_t)(n - lo < (uint64_t)kTile ? n - lo : (uint64_t)kTile);
+    s.rel = rel ? 1 : 0;
+    t_next++;
+    return s;
+}
+
+// Add the CTA's 16-bit counter pairs to its histogram row (reductions: no round trip) and clear them.
+// All threads; the caller synchronises before and after.
+__device__ __forceinline__ void seg_flush(uint32_t *jh, uint32_t *row, int nbins) {
+    for (int w = threadIdx.x; w < (nbins >> 1); w += blockDim.x) {
+        const uint32_t v = jh[w];
+        if (!v) continue;
+        jh[w] = 0;
+        if (v & 0xffffu) atomicAdd(&row[2 * w], v & 0xffffu);
+        if (v >> 16) atomicAdd(&row[2 * w + 1], v >> 16);
+    }
+}
+
+// K = ceil(F1 / 32): pass-1 digits per lane of warp 0, which keeps their segment state in registers.
+template <int THREADS, int ITEMS, int K>
+__global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegArgs a) {
+    constexpr int T = THREADS * ITEMS;
+    static_assert(T == kTile, "a segment holds one tile");
+    static_assert(K >= 1 && K <= 8, "at most 256 pass-1 digits");
+    extern __shared__ __align__(128) unsigned char smem[];
+    tuple_v *inbuf = reinterpret_cast<tuple_v *>(smem);              // [2][T]
+    SegRun *runs = reinterpret_cast<SegRun *>(inbuf + 2 * T);          // [256] where each digit's run goes
+    uint32_t *thist = reinterpret_cast<uint32_t *>(runs + 256);        // [256] tile histogram
+    uint32_t *tdstart = thist + 256;                                   // [256] digit start in the staged tile
+    uint32_t *jh = tdstart + 256;                                      // [2^bits / 2] counter pairs
+    __shared__ __align__(8) unsigned long long bars[2];
+    __shared__ SegSlot slots[2];
+    __shared__ uint32_t s_item, s_tnext, s_tend;  // thread 0's item iterator
+
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int F = a.F1;
+    const uint32_t dmask = (uint32_t)F - 1u;
+    const int nbins = 1 << a.bits;
+    const uint64_t bmask = (uint64_t)nbins - 1;
+    const uint32_t G = gridDim.x, c = blockIdx.x;
+    unsigned int *err = &a.counters[kCtrErr];
+    const uint32_t bar0 = smem_addr(&bars[0]);
+    const uint64_t cap = (uint64_t)a.max_segs * T;
+
+    for (int j = tid; j < 256; j += THREADS) thist[j] = 0;
+    for (int j = tid; j < (nbins >> 1); j += THREADS) jh[j] = 0;
+    // Warp 0, lane l: current segment and fill of digits l*K .. l*K + K - 1.
+    uint32_t scur[K], sfill[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        scur[j] = kSegNone;
+        sfill[j] = 0;
+    }
+    // This CTA's rows of hist start at zero; counters are added to them.
+    for (int j = tid; j < 2 * nbins; j += THREADS)
+        a.hist[((size_t)(j >= nbins ? G : 0) + c) * nbins + (j >= nbins ? j - nbins : j)] = 0;
+    uint32_t slab_lo = 0, slab_rem = 0;  // thread 0 (lane 0 of warp 0): ids left in this CTA's slab
+    if (tid == 0) {
+        s_item = ~0u;
+        s_tnext = s_tend = 0;
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        uint32_t item = s_item, tn = s_tnext, te = s_tend;
+        const SegSlot s0 = seg_next_tile(a, item, tn, te);
+        s_item = item;
+        s_tnext = tn;
+        s_tend = te;
+        slots[0] = s0;
+        if (s0.cnt && !(a.test_stall && blockIdx.x == 0)) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
+    }
+    __syncthreads();
+
+    int phase_rel = 0;           // relation whose tuples the counters and segment state hold
+    uint32_t since = 0;          // upper bound of every counter (uniform)
+    unsigned long long kor = 0, ror = 0;
+    __shared__ uint32_t s_max[THREADS / 32];
+
+    for (uint32_t k = 0;; k++) {
+        const uint32_t cur = k & 1u;
+        const SegSlot sl = slots[cur];
+        if (sl.cnt == 0) break;
+        tuple_v *buf = inbuf + (size_t)cur * T;
+        if (tid == 0) {
+            uint32_t item = s_item, tn = s_tnext, te = s_tend;
+            const SegSlot sn = seg_next_tile(a, item, tn, te);
+            s_item = item;
+            s_tnext = tn;
+            s_tend = te;
+            slots[cur ^ 1u] = sn;
+            if (sn.cnt) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
+        }
+        // R tiles come before S tiles in every CTA's sequence: on the first S tile, R's counters go
+        // to their row and the segment state starts over.
+        if (sl.rel != phase_rel) {
+            seg_flush(jh, a.hist + ((size_t)phase_rel * G + c) * nbins, nbins);
+#pragma unroll
+            for (int j = 0; j < K; j++) {
+                scur[j] = kSegNone;
+                sfill[j] = 0;
+            }
+            phase_rel = sl.rel;
+            since = 0;
+            __syncthreads();
+        }
+        const uint32_t cnt = sl.cnt;
+        if (since + cnt > 65535u) {
+            // Move the large counters to the row; the largest one kept is the new bound.
+            uint32_t *hrow = a.hist + ((size_t)phase_rel * G + c) * nbins;
+            uint32_t mx = 0;
+            for (int q = tid; q < (nbins >> 1); q += THREADS) {
+                const uint32_t v0 = jh[q];
+                uint32_t lo = v0 & 0xffffu, hi = v0 >> 16;
+                if (lo > kSegSpillAt) {
+                    atomicAdd(&hrow[2 * q], lo);
+                    lo = 0;
+                }
+                if (hi > kSegSpillAt) {
+                    atomicAdd(&hrow[2 * q + 1], hi);
+                    hi = 0;
+                }
+                if (v0 != (lo | (hi << 16))) jh[q] = lo | (hi << 16);
+                mx = max(mx, max(lo, hi));
+            }
+            mx = __reduce_max_sync(0xffffffffu, mx);
+            if (lane == 0) s_max[w] = mx;
+            __syncthreads();
+            since = 0;
+#pragma unroll
+            for (int q = 0; q < THREADS / 32; q++) since = max(since, s_max[q]);
+            __syncthreads();
+        }
+        since += cnt;
+        const bool ok = mbar_wait(bar0 + 8u * cur, (k >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                set_error(err, kErrSpinLimit);
+                if (slots[cur ^ 1u].cnt) mbar_wait(bar0 + 8u * (cur ^ 1u), ((k + 1) >> 1) & 1u);
+            }
+            break;
+        }
+
+        tuple_v v[ITEMS];
+        uint32_t rk[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
+            if (idx < cnt) {
+                v[i] = buf[idx];
+                const uint32_t d = (uint32_t)v[i].x & dmask;
+                rk[i] = atomicAdd(&thist[d], 1u);
+                const uint32_t bin = (uint32_t)(v[i].x & bmask);
+                atomicAdd(&jh[bin >> 1], 1u << ((bin & 1u) << 4));
+                if (sl.rel == 0) {
+                    kor |= v[i].x;
+                    ror |= v[i].y;
+                }
+            }
+        }
+        __syncthreads();
+        // Warp 0: digit starts in the staged tile and where each digit's run goes: the rest of its
+        // current segment, then (when that fills) a new segment. Lane l owns digits [l*K, l*K + K).
+        if (w == 0) {
+            const int d0 = lane * K;
+            uint32_t hv[K];
+            uint32_t packed = 0;  // tuples (low 16 bits) and new segments (high 16 bits) of this lane
+#pragma unroll
+            for (int j = 0; j < K; j++) {
+                hv[j] = d0 + j < F ? thist[d0 + j] : 0u;
+                const bool nw = hv[j] && (scur[j] == kSegNone || sfill[j] + hv[j] > (uint32_t)T);
+                packed += hv[j] + (nw ? 0x10000u : 0u);
+            }
+            uint32_t incl = packed;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const uint32_t ntot = __shfl_sync(0xffffffffu, incl, 31) >> 16;
+            // New segment ids: first what is left of the slab, then a fresh slab.
+            uint32_t old_lo = 0, old_rem = 0, nb = 0;
+            if (ntot) {
+                if (lane == 0) {
+                    old_lo = slab_lo;
+                    old_rem = slab_rem;
+                    if (ntot <= slab_rem) {
+                        slab_lo += ntot;
+                        slab_rem -= ntot;
+                    } else {
+                        const uint32_t deficit = ntot - slab_rem;
+                        const uint32_t take = deficit > kSegSlab ? deficit : kSegSlab;
+                        nb = atomicAdd(&a.counters[kCtrSegAlloc], take);
+                        slab_lo = nb + deficit;
+                        slab_rem = take - deficit;
+                    }
+                }
+                old_lo = __shfl_sync(0xffffffffu, old_lo, 0);
+                old_rem = __shfl_sync(0xffffffffu, old_rem, 0);
+                nb = __shfl_sync(0xffffffffu, nb, 0);
+            }
+            const uint32_t exl = incl - packed;
+            uint32_t ex = exl & 0xffffu, e = exl >> 16;
+#pragma unroll
+            for (int j = 0; j < K; j++) {
+                const int d = d0 + j;
+                if (d < F) {
+                    const uint32_t h = hv[j];
+                    thist[d] = 0;
+                    tdstart[d] = ex;
+                    if (h) {
+                        const uint32_t sc = scur[j], fill = sfill[j];
+                        SegRun r;
+                        if (sc != kSegNone && fill + h <= (uint32_t)T) {
+                            r.base = (long long)sc * T + fill - ex;
+                            r.jump = 0;
+                            r.split = ex + h;
+                            sfill[j] = fill + h;
+                        } else {
+                            const uint32_t id = e < old_rem ? old_lo + e : nb + (e - old_rem);
+                            e++;
+                            if (id < a.max_segs) {
+                                if (sc == kSegNone) {
+                                    // The whole run starts the chain.
+                                    a.seg_head[((size_t)phase_rel * G + c) * F + d] = id;
+                                    r.base = (long long)id * T - ex;
+                                    r.jump = 0;
+                                    r.split = ex + h;
+                                    sfill[j] = h;
+                                } else {
+                                    // The run fills the current segment, then goes on in segment
+                                    // id: staged index ex + (T - fill) lands at id * T.
+                                    a.seg_next[sc] = id;
+                                    r.base = (long long)sc * T + fill - ex;
+                                    r.jump = (int)id - (int)sc - 1;
+                                    r.split = ex + ((uint32_t)T - fill);
+                                    sfill[j] = h - ((uint32_t)T - fill);
+                                }
+                                scur[j] = id;
+                            } else {
+                                // Cannot happen with the storage phj_carve reserves; the run's
+                                // stores fail their bounds check and report it.
+                                set_error(err, kErrCapacity);
+                                r.base = -(long long)cap - (long long)T;
+                                r.jump = 0;
+                                r.split = ex + h;
+                                scur[j] = kSegNone;
+                                sfill[j] = 0;
+                            }
+                        }
+                        runs[d] = r;
+                    }
+                    ex += h;
+                }
+            }
+        }
+        __syncthreads();
+        // Stage the tile sorted by digit, in place.
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
+            if (idx < cnt) buf[tdstart[(uint32_t)v[i].x & dmask] + rk[i]] = v[i];
+        }
+        __syncthreads();
+        // Write each digit run: consecutive threads write consecutive 16-byte tuples.
+        if (cnt == (uint32_t)T) {
+#pragma unroll
+            for (int hh = 0; hh < 2; hh++) {
+                tuple_v t[ITEMS / 2];
+                long long dst[ITEMS / 2];
+#pragma unroll
+                for (int i = 0; i < ITEMS / 2; i++) t[i] = buf[tid + (hh * ITEMS / 2 + i) * THREADS];
+#pragma unroll
+                for (int i = 0; i < ITEMS / 2; i++) {
+                    const uint32_t j = (uint32_t)(tid + (hh * ITEMS / 2 + i) * THREADS);
+                    const SegRun r = runs[(uint32_t)t[i].x & dmask];
+                    dst[i] = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * T);
+                }
+#pragma unroll
+                for (int i = 0; i < ITEMS / 2; i++) {
+                    if (dst[i] >= 0 && (uint64_t)dst[i] < cap)
+                        st_stream(a.out + dst[i], t[i]);
+                    else
+                        set_error(err, kErrBounds);
+                }
+            }
+        } else {
+            for (uint32_t j = tid; j < cnt; j += THREADS) {
+                const tuple_v t = buf[j];
+                const SegRun r = runs[(uint32_t)t.x & dmask];
+                const long long dst = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * T);
+                if (dst >= 0 && (uint64_t)dst < cap)
+                    st_stream(a.out + dst, t);
+                else
+                    set_error(err, kErrBounds);
+            }
+        }
+        __syncthreads();
+    }
+    // The counters of the relation in progress go to their row (the other row is complete).
+    __syncthreads();
+    seg_flush(jh, a.hist + ((size_t)phase_rel * G + c) * nbins, nbins);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        kor |= __shfl_xor_sync(0xffffffffu, kor, o);
+        ror |= __shfl_xor_sync(0xffffffffu, ror, o);
+    }
+    if (lane == 0 && (kor | ror)) {
+        unsigned long long *mx = reinterpret_cast<unsigned long long *>(a.counters + kCtrMaxKey);
+        atomicOr(mx, kor);
+        atomicOr(mx + 1, ror);
     }
 }
 
@@ -1404,15 +1817,45 @@ static ChunkGeom chunk_geom(size_t nR, size_t nS, int num_sms) {
 
 struct PhjSizes {
     size_t chunk_hist, prefix, total, start, units_off, units_cnt, subhist, counters, items, large, large_table,
-        tmp1, tmp2;
+        tmp1, tmp2, seg_head, seg_next;
     size_t max_items, max_large, large_table_words;
+    uint32_t max_segs, seg_grid, it_tiles;
     ChunkGeom cg;
 };
 
-static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms) {
+// Segment mode from 2^26 tuples: below that the histogram read it saves is small next to the
+// storage of the partly filled segments (2 * CTAs * F1 * kTile tuples).
+constexpr uint64_t kSegMinTuples = 1ull << 26;
+
+bool phj_seg_applies(const RadixGeom &g, bool lp, size_t nR, size_t nS) {
+    return !lp && g.passes == 2 && g.bits <= kSegMaxBits && (uint64_t)nR + nS >= kSegMinTuples;
+}
+
+static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms, bool seg) {
     PhjSizes z;
     const size_t np = (size_t)g.nparts();
-    z.cg = chunk_geom(nR, nS, num_sms);
+    const int sms = num_sms > 0 ? num_sms : 148;
+    if (seg) {
+        // "Chunks" are the pass-1 CTAs, one per relation each.
+        z.seg_grid = (uint32_t)(sms * kSegCtasPerSm);
+        z.cg.chunk = 0;
+        z.cg.cR = z.cg.cS = z.seg_grid;
+        z.cg.sub = 0;
+        z.cg.spc = 0;
+        z.cg.pad = 0;
+        const uint64_t tiles = (uint64_t)ceil_div_u64(nR, kTile) + ceil_div_u64(nS, kTile);
+        uint64_t it = tiles / ((uint64_t)z.seg_grid * 8);
+        z.it_tiles = (uint32_t)(it < 1 ? 1 : it > 16 ? 16 : it);
+        // Every segment but the current one of each (CTA, relation, digit) is full; each CTA leaves
+        // fewer than kSegSlab ids of its last slab unused.
+        const uint64_t segs = (uint64_t)(nR + nS) / kTile + 2ull * z.seg_grid * g.F1 + (uint64_t)z.seg_grid * kSegSlab;
+        z.max_segs = (uint32_t)segs;
+    } else {
+        z.cg = chunk_geom(nR, nS, num_sms);
+        z.seg_grid = 0;
+        z.it_tiles = 0;
+        z.max_segs = 0;
+    }
     const size_t nchunks = (size_t)z.cg.cR + z.cg.cS;
     z.chunk_hist = align_up(nchunks * np * 4, 256);
     z.prefix = z.chunk_hist;
@@ -1426,8 +1869,10 @@ static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms)
     z.items = align_up(z.max_items * sizeof(JoinItem), 256);
     z.max_large = np < nR / kSmemCap + 1 ? np : nR / kSmemCap + 1;
     z.large = align_up(z.max_large * sizeof(LargePart), 256);
-    z.tmp1 = align_up((nR + nS) * 16, 256);
-    z.tmp2 = g.passes == 2 ? z.tmp1 : 0;
+    z.tmp1 = seg ? align_up((size_t)z.max_segs * kTile * 16, 256) : align_up((nR + nS) * 16, 256);
+    z.tmp2 = g.passes == 2 ? align_up((nR + nS) * 16, 256) : 0;
+    z.seg_head = seg ? align_up((size_t)2 * z.seg_grid * g.F1 * 4, 256) : 0;
+    z.seg_next = seg ? align_up((size_t)z.max_segs * 4, 256) : 0;
     // Large-partition chains: head <= 2*|R_p| words, next = |R_p| words. With two passes they reuse
     // the pass-1 buffer, which is dead once pass 2 has run.
     z.large_table_words = 3 * nR + 2;
@@ -1435,15 +1880,19 @@ static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms)
     return z;
 }
 
-size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms) {
-    PhjSizes z = phj_sizes(g, nR, nS, num_sms);
+size_t phj_scratch_bytes(const RadixGeom &g, size_t nR, size_t nS, int num_sms, bool seg) {
+    PhjSizes z = phj_sizes(g, nR, nS, num_sms, seg);
     return z.chunk_hist + z.prefix + z.total + z.start + z.units_off + z.units_cnt + z.subhist + z.counters + z.items +
-           z.large + z.large_table + z.tmp1 + z.tmp2;
+           z.large + z.large_table + z.tmp1 + z.tmp2 + z.seg_head + z.seg_next;
 }
 
-void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base, PhjScratch *s) {
-    PhjSizes z = phj_sizes(g, nR, nS, num_sms);
+void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base, PhjScratch *s, bool seg) {
+    PhjSizes z = phj_sizes(g, nR, nS, num_sms, seg);
     char *p = base;
+    s->seg = seg;
+    s->seg_grid = z.seg_grid;
+    s->max_segs = z.max_segs;
+    s->it_tiles = z.it_tiles;
     s->chunk = z.cg.chunk;
     s->cR = z.cg.cR;
     s->cS = z.cg.cS;
@@ -1456,6 +1905,8 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
     s->unit_off = reinterpret_cast<uint64_t *>(p); p += z.units_off;
     s->unit_cnt = reinterpret_cast<uint32_t *>(p); p += z.units_cnt;
     s->subhist = reinterpret_cast<uint32_t *>(p); p += z.subhist;
+    s->seg_head = reinterpret_cast<uint32_t *>(p); p += z.seg_head;
+    s->seg_next = reinterpret_cast<uint32_t *>(p); p += z.seg_next;
     s->counters = reinterpret_cast<uint32_t *>(p); p += z.counters;
     s->items = p; p += z.items;
     s->max_items = z.max_items;
@@ -1484,6 +1935,12 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
 
 static bool g_attr_done[64] = {};
 
+// Dynamic shared memory of seg_pass1_kernel: two tile buffers, per-digit state, 2^bits 16-bit counters.
+static size_t seg_smem_bytes(int bits) {
+    // tile buffers, runs[256], thist[256], tdstart[256], counter pairs
+    return (size_t)2 * kTile * 16 + 256 * sizeof(SegRun) + 256 * 4 * 2 + ((size_t)1 << bits) * 2;
+}
+
 int phj_prepare_device() {
     int cur_dev = 0;
     HJ_CU(cudaGetDevice(&cur_dev));
@@ -1497,6 +1954,14 @@ int phj_prepare_device() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 1>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 4>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 8>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1527,17 +1992,54 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     cg.spc = s.spc;
     cg.pad = 0;
     const uint32_t nchunks = cg.cR + cg.cS;
+    // A segment-mode scratch holds the segment storage, not the exact-offset pipeline's buffers.
+    const bool segm = s.seg;
+    if (segm && (lp || g.passes != 2 || g.bits > kSegMaxBits)) return HJ_E_INVAL;
     {
         const int rc = phj_prepare_device();
         if (rc) return rc;
     }
     HJ_CU(cudaMemsetAsync(s.counters, 0, kNumCounters * 4, st));
 
-    // 1. per-chunk histograms
     HJ_PH(0);
-    hist_chunk_kernel<<<nchunks, 512, hist_smem, st>>>(R, nR, S, nS, g.bits, F1, cg, s.chunk_hist, s.subhist,
-                                                       s.counters + kCtrMaxKey);
-    HJ_CU(cudaGetLastError());
+    if (segm) {
+        // 1'. pass 1 into segment chains, with the per-CTA histograms
+        SegArgs ga;
+        ga.R = R;
+        ga.S = S;
+        ga.nR = nR;
+        ga.nS = nS;
+        ga.bits = g.bits;
+        ga.F1 = F1;
+        ga.it_tiles = s.it_tiles;
+        ga.tilesR = ceil_div_u64(nR, T);
+        ga.tilesS = ceil_div_u64(nS, T);
+        ga.itemsR = (ga.tilesR + s.it_tiles - 1) / s.it_tiles;
+        ga.items = ga.itemsR + (ga.tilesS + s.it_tiles - 1) / s.it_tiles;
+        ga.out = s.tmp1;
+        ga.max_segs = s.max_segs;
+        ga.seg_head = s.seg_head;
+        ga.seg_next = s.seg_next;
+        ga.hist = s.chunk_hist;
+        ga.counters = s.counters;
+        ga.test_stall = (test_flags & 1) ? 1 : 0;
+        const size_t sm = seg_smem_bytes(g.bits);
+        if (F1 <= 32)
+            seg_pass1_kernel<kScatterThreads, kScatterItems, 1><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
+        else if (F1 <= 64)
+            seg_pass1_kernel<kScatterThreads, kScatterItems, 2><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
+        else if (F1 <= 128)
+            seg_pass1_kernel<kScatterThreads, kScatterItems, 4><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
+        else
+            seg_pass1_kernel<kScatterThreads, kScatterItems, 8><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
+        HJ_CU(cudaGetLastError());
+        nlaunch++;
+    } else {
+        // 1. per-chunk histograms
+        hist_chunk_kernel<<<nchunks, 512, hist_smem, st>>>(R, nR, S, nS, g.bits, F1, cg, s.chunk_hist, s.subhist,
+                                                           s.counters + kCtrMaxKey);
+        HJ_CU(cudaGetLastError());
+    }
     HJ_PH(1);
     // 2. prefix over chunks, 3. plan, 4. units
     colscan_kernel<<<(8 * np + 255) / 256, 256, 0, st>>>(s.chunk_hist, s.prefix, s.total, np, cg);
@@ -1564,12 +2066,12 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
                                              cg, s.unit_off, s.unit_cnt, s.subhist, s.counters + kCtrErr);
     }
     HJ_CU(cudaGetLastError());
-    nlaunch += 4;
+    nlaunch += segm ? 3 : 4;
     HJ_PH(2);
 
-    // 5. scatter passes
+    // 5. scatter passes (segment mode: pass 2 only, its units are the pass-1 chains)
     const int scatter_grid = num_sms * kScatterCtasPerSm;
-    for (int pass = 0; pass < g.passes; pass++) {
+    for (int pass = segm ? 1 : 0; pass < g.passes; pass++) {
         ScatterArgs sa;
         sa.pass = pass;
         sa.F = pass == 0 ? F1 : F2;
@@ -1592,6 +2094,9 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.unit_off = s.unit_off;
         sa.unit_cnt = s.unit_cnt;
         sa.subpre = s.subhist;
+        sa.seg_head = segm ? s.seg_head : nullptr;
+        sa.seg_next = segm ? s.seg_next : nullptr;
+        sa.max_segs = segm ? s.max_segs : 0;
         sa.test_stall = (pass == 0 && (test_flags & 1)) ? 1 : 0;
         sa.counters = s.counters;
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
@@ -1603,7 +2108,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
                 <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
         HJ_CU(cudaGetLastError());
         nlaunch++;
-        HJ_PH(3 + pass);
+        HJ_PH(segm ? 3 : 3 + pass);
     }
     if (ph && g.passes == 1) HJ_CU(cudaEventRecord(ph[4], st));
     if (ev_mid) HJ_CU(cudaEventRecord(ev_mid, st));
@@ -1629,7 +2134,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         join_small_kernel<false><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
     }
     HJ_CU(cudaGetLastError());
-    HJ_PH(5);
+    HJ_PH(segm ? 4 : 5);
     join_large_clear<<<num_sms * 2, 256, 0, st>>>(ja);
     join_large_build<<<num_sms * 2, 256, 0, st>>>(ja);
     if (mat)
@@ -1638,7 +2143,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         join_large_probe<false><<<num_sms * 2, 256, 0, st>>>(ja);
     copy_error<<<1, 32, 0, st>>>(s.counters, acc);
     HJ_CU(cudaGetLastError());
-    HJ_PH(6);
+    HJ_PH(segm ? 5 : 6);
     nlaunch += 6;
     if (launches) *launches = nlaunch;
 #undef HJ_PH

@@ -99,12 +99,19 @@ typedef struct {
 #define HJ_F_NO_TIMING   0x1u /* skip the per-phase CUDA events (buildpart/probejoin stay 0) */
 #define HJ_F_PINNED_HOST 0x2u /* host inputs are already page-locked */
 #define HJ_F_PHASE_TIMES 0x4u /* also time each kernel group (fills hj_result_t.phase) */
+/* Radix joins that count every match (bc, sc, hr, hro; two passes, <= 14 bits) from 2^26 tuples run
+ * in segment mode: pass 1 writes chains of fixed-size segments and counts the histograms itself, so no
+ * histogram pass reads the relations first (if the larger scratch does not fit, the exact-offset
+ * pipeline runs). These flags pick the pipeline regardless of size; results are the same. */
+#define HJ_F_SEGMENTS    0x20u /* segment mode whenever the algorithm allows it */
+#define HJ_F_EXACT       0x40u /* always the histogram pass and exact pass-1 offsets */
 /* Test hook for failure detection: the first partition pass of a radix join withholds one tile load,
  * so a bounded device wait (2 s) expires and the join returns HJ_E_TIMEOUT; the context stays usable. */
 #define HJ_F_TEST_STALL  0x100u
 
 /* hj_result_t.phase[] slots (seconds), filled with HJ_F_PHASE_TIMES. PHJ: histogram, plan, partition
- * pass 1, partition pass 2, shared-memory partition joins, global-memory (large) partition joins.
+ * pass 1, partition pass 2, shared-memory partition joins, global-memory (large) partition joins
+ * (segment mode: no histogram pass, so that slot is 0 and pass 1 includes the counting).
  * NPHJ: build, -, -, -, probe, -. */
 enum { HJ_PH_HIST = 0, HJ_PH_PLAN = 1, HJ_PH_PASS1 = 2, HJ_PH_PASS2 = 3, HJ_PH_JOIN = 4, HJ_PH_LARGE = 5,
        HJ_PH_COUNT = 6 };
