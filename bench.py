@@ -338,6 +338,11 @@ def run_ours(a, rank, world, local_rank):
         achieved = scatter_bytes / pass_s / 1e9
         prof = traffic_profile("scatter_kernel")
         traffic = prof["dram_bytes_per_tuple"] * (nR + nS) if prof else None
+        if seg_mode:
+            # per launch, averaged over the two passes like `achieved`
+            p1 = traffic_profile("seg_pass1_kernel")
+            traffic = ((p1["dram_bytes_per_tuple"] + prof["dram_bytes_per_tuple_pass2"]) / 2 * (nR + nS)
+                       if p1 and prof else None)
         kname = ("seg_pass1_kernel / scatter_kernel (mean of the two radix partition passes)" if seg_mode
                  else "scatter_kernel (one radix partition pass)")
         roofline = {"kernel": kname, "bound": "hbm",
