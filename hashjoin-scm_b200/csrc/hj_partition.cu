@@ -1432,15 +1432,17 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 }
             }
         } else
-        for (uint32_t j0 = tid; j0 < ns; j0 += 4 * kCompactThreads) {
-            tuple_v sv[4];
+        // Eight probe tuples per thread in flight (four left the DRAM queue short: 2.01 -> 1.92 ms
+        // for the headline join phase).
+        for (uint32_t j0 = tid; j0 < ns; j0 += 8 * kCompactThreads) {
+            tuple_v sv[8];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 8; u++) {
                 const uint32_t j = j0 + u * kCompactThreads;
                 sv[u] = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 8; u++) {
                 const uint32_t j = j0 + u * kCompactThreads;
                 if (j >= ns) continue;
                 const uint64_t khi = sv[u].x >> B;
