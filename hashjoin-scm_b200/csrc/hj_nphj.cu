@@ -16,6 +16,12 @@
 // first match; with duplicates sc keeps walking to the empty slot and lp rebuilds the table with the
 // minimum input position per key (atomicMin) and resolves row ids in one gather pass. R tuples whose
 // key equals the EMPTY pattern are kept in a side record instead of the table.
+//
+// Compact slots (nphj_sc): when every build key is below 2^32 - 1 and every build row id below 2^32
+// (a first pass over R finds out), a slot is one 8-byte word (key << 32 | row id), claimed whole by one
+// 64-bit CAS. The table then takes half the bytes (64 MB for |R| = 2^22, where L2 holds it), a build
+// claim needs no second store, and a probe reads 8 bytes. Used when the 16-byte table would exceed
+// 64 MB.
 #include <cstdio>
 
 #include "hj_common.cuh"
@@ -32,7 +38,18 @@ struct NphjSide {
     unsigned long long minpos;   // smallest input position among them
     unsigned int dup;            // the build saw an equal key twice
     unsigned int err;
+    unsigned long long kmax;     // largest build key (compact-slot test)
+    unsigned long long ror;      // OR of all build row ids
 };
+
+constexpr unsigned long long kCompactEmpty = ~0ull;
+constexpr unsigned long long kCompactMinTableBytes = 64ull << 20;
+
+// Every build key below 2^32 - 1 (so no slot can equal the empty pattern) and every row id below 2^32.
+__device__ __forceinline__ bool nphj_compact(const NphjSide *side) {
+    return *reinterpret_cast<const volatile unsigned long long *>(&side->kmax) < 0xffffffffull &&
+           *reinterpret_cast<const volatile unsigned long long *>(&side->ror) < (1ull << 32);
+}
 
 struct NphjArgs {
     const tuple_v *R, *S;
@@ -45,7 +62,55 @@ struct NphjArgs {
     int skip0;  // key 0 never matches (the phj_radix_lp rule)
     unsigned long long *side_pos;  // materialising joins: input positions of the side record's tuples
     MatOut mat;
+    int compact_ok;  // the algorithm may use compact slots (nphj_sc, not materialising)
 };
+
+// Largest build key and OR of build row ids, for the compact-slot test.
+__global__ void nphj_widths(NphjArgs a) {
+    unsigned long long kmax = 0, ror = 0;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    constexpr int U = 4;
+    for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < a.nR;
+         i0 += U * stride) {
+        tuple_v t[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned long long i = i0 + u * stride;
+            t[u] = i < a.nR ? ld_stream(a.R + i) : make_ulonglong2(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            kmax = max(kmax, t[u].x);
+            ror |= t[u].y;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+        ror |= __shfl_xor_sync(0xffffffffu, ror, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&a.side->kmax, kmax);
+        atomicOr(&a.side->ror, ror);
+    }
+}
+
+// Compact build: the CAS writes key and row id together.
+__device__ __forceinline__ void nphj_insert_compact(const NphjArgs &a, unsigned long long *ctab, const tuple_v t,
+                                                    bool &seen_dup) {
+    const unsigned long long v = (t.x << 32) | t.y;
+    unsigned long long h = table_hash(t.x, a.cap);
+    for (unsigned long long steps = 0;;) {
+        const unsigned long long cur = atomicCAS(ctab + h, kCompactEmpty, v);
+        if (cur == kCompactEmpty) return;
+        if ((cur >> 32) == t.x) seen_dup = true;
+        if (++h == a.cap) h = 0;
+        if (++steps >= a.cap) {
+            set_error(&a.acc->error, kErrProbeLimit);
+            return;
+        }
+    }
+}
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
     return *reinterpret_cast<const volatile unsigned long long *>(p);
@@ -83,6 +148,23 @@ __global__ void nphj_build(NphjArgs a) {
     constexpr int U = 4;
     bool seen_dup = false;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    if (a.compact_ok && nphj_compact(a.side)) {
+        unsigned long long *ctab = reinterpret_cast<unsigned long long *>(a.table);
+        for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < a.nR;
+             i0 += U * stride) {
+            tuple_v t[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const unsigned long long i = i0 + u * stride;
+                t[u] = i < a.nR ? ld_stream(a.R + i) : make_ulonglong2(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (i0 + u * stride < a.nR) nphj_insert_compact(a, ctab, t[u], seen_dup);
+        }
+        if (__syncthreads_or(seen_dup) && threadIdx.x == 0) atomicOr(&a.side->dup, 1u);
+        return;
+    }
     for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < a.nR;
          i0 += U * stride) {
         tuple_v t[U];
@@ -147,11 +229,65 @@ __global__ void nphj_lp_resolve(NphjArgs a) {
     }
 }
 
+// Probe of a compact-slot table (see nphj_build); a no-op otherwise. Four probes per thread: the
+// 8-byte slots leave the registers for it.
+__global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
+    __shared__ unsigned long long red[64];
+    if (!(a.compact_ok && nphj_compact(a.side))) return;
+    // Compact slots: no build key is the empty pattern, so there is no side record; a probe key
+    // at or above 2^32 - 1 cannot match.
+    constexpr int V = 4;
+    const unsigned long long *ctab = reinterpret_cast<const unsigned long long *>(a.table);
+    const bool first_only = *reinterpret_cast<volatile unsigned int *>(&a.side->dup) == 0;
+    unsigned long long cnt = 0, sum = 0;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long j0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j0 < a.nS;
+         j0 += V * stride) {
+        tuple_v sv[V];
+        unsigned long long h[V], e[V];
+        bool walk[V];
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            const unsigned long long j = j0 + u * stride;
+            sv[u] = j < a.nS ? ld_stream(a.S + j) : make_ulonglong2(0, 0);
+            walk[u] = j < a.nS && sv[u].x < 0xffffffffull;
+        }
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            if (walk[u]) {
+                h[u] = table_hash(sv[u].x, a.cap);
+                e[u] = ld_slot8(ctab + h[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            if (!walk[u]) continue;
+            unsigned long long hh = h[u], ee = e[u];
+            for (unsigned long long steps = 0;;) {
+                if (ee == kCompactEmpty) break;
+                if ((ee >> 32) == sv[u].x) {
+                    cnt++;
+                    sum += (ee & 0xffffffffull) + sv[u].y;
+                    if (first_only) break;
+                }
+                if (++hh == a.cap) hh = 0;
+                if (++steps >= a.cap) {
+                    set_error(&a.acc->error, kErrProbeLimit);
+                    break;
+                }
+                ee = ld_slot8(ctab + hh);
+            }
+        }
+    }
+    block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
+}
+
 // Two probes per thread at eight 256-thread blocks per SM measured best for tables that sit in L2
 // (more probes per thread cost occupancy through registers).
 __global__ void __launch_bounds__(256, 8) nphj_probe(NphjArgs a) {
     __shared__ unsigned long long red[64];
     constexpr int U = 2;
+    if (a.compact_ok && nphj_compact(a.side)) return;  // nphj_probe_compact probes instead
     ProbeArgs P;
     P.table = a.table;
     P.cap = a.cap;
@@ -310,12 +446,16 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     a.side_pos = mat ? reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(table) + cap * 16 + 256)
                      : nullptr;
     a.mat = mat ? *mat : MatOut{nullptr, 0};
+    // Compact slots pay off once the 16-byte table outgrows a share of L2; below that the extra pass
+    // over R costs more than it saves.
+    a.compact_ok = (!lp && !mat && cap * 16 > kCompactMinTableBytes) ? 1 : 0;
     HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
     HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
     HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));
     const int grid = num_sms * 8;
     // Phase slots: build spans [0, 1], probe spans [4, 5]; the others stay empty.
     if (ph) HJ_CU(cudaEventRecord(ph[0], st));
+    if (a.compact_ok) nphj_widths<<<grid, 256, 0, st>>>(a);
     nphj_build<<<grid, 256, 0, st>>>(a);
     if (lp) {
         nphj_lp_refill<<<grid, 256, 0, st>>>(a);
@@ -327,16 +467,18 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     if (ph) {
         for (int i = 1; i <= 4; i++) HJ_CU(cudaEventRecord(ph[i], st));
     }
-    if (mat)
+    if (mat) {
         nphj_probe_mat<<<grid, 256, 0, st>>>(a);
-    else
+    } else {
         nphj_probe<<<grid, 256, 0, st>>>(a);
+        if (a.compact_ok) nphj_probe_compact<<<grid, 256, 0, st>>>(a);
+    }
     HJ_CU(cudaGetLastError());
     if (ph) {
         HJ_CU(cudaEventRecord(ph[5], st));
         HJ_CU(cudaEventRecord(ph[6], st));
     }
-    if (launches) *launches = lp ? 5u : 2u;
+    if (launches) *launches = lp ? 5u : a.compact_ok ? 4u : 2u;
     return HJ_OK;
 }
 

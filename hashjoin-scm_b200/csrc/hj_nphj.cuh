@@ -15,6 +15,13 @@ __device__ __forceinline__ tuple_v ld_slot(const tuple_v *p) {
     return v;
 }
 
+// Read-only 8-byte load of a compact table slot.
+__device__ __forceinline__ unsigned long long ld_slot8(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+
 struct ProbeArgs {
     const tuple_v *table;
     unsigned long long cap;
