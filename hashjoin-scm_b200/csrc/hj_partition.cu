@@ -578,7 +578,28 @@ struct ItemIter {
     uint32_t seg = 0;   // segment mode: segment of the next tile
 };
 
-__device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item, ItemIter &it) {
+// The next work item, claimed one item ahead (thread 0 only): its id comes from the counter while the
+// current item is processed, and the loads of its description are issued one call later, so that
+// neither the atomic nor the loads stall the CTA at the switch.
+struct ItemAhead {
+    uint32_t item;   // claimed id (stage >= 1)
+    uint32_t stage;  // 0: nothing claimed, 1: claimed, 2: description loaded
+    uint64_t len, off;
+    uint32_t seg;
+};
+
+// Issue the loads that describe `ah.item` (pass 2 units; pass-1 sub-chunks need none).
+__device__ __forceinline__ void item_fetch(const ScatterArgs &a, ItemAhead &ah, uint32_t nitems) {
+    ah.stage = 2;
+    if (a.pass == 0 || ah.item >= nitems) return;
+    ah.len = a.unit_cnt[ah.item];
+    if (a.seg_head)
+        ah.seg = a.seg_head[ah.item];  // read even for an empty unit (then unused): no dependent load
+    else
+        ah.off = a.unit_off[ah.item];
+}
+
+__device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item, const ItemAhead &ah, ItemIter &it) {
     const ChunkGeom &cg = a.cg;
     it.item = item;
     it.done = 0;
@@ -598,31 +619,38 @@ __device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item,
     } else {
         const uint32_t c = item / a.F1;
         const int rel = c < cg.cR ? 0 : 1;
-        it.len = a.unit_cnt[item];
+        it.len = ah.len;
         if (a.seg_head) {
             it.in = a.inR;
-            it.seg = it.len ? a.seg_head[item] : 0u;
+            it.seg = ah.seg;
         } else {
-            it.in = (rel ? a.inS : a.inR) + a.unit_off[item];
+            it.in = (rel ? a.inS : a.inR) + ah.off;
         }
         it.out = rel ? a.outS : a.outR;
         it.out_len = rel ? a.nS : a.nR;
     }
 }
 
-// Claim the next tile (thread 0 only): continue the current item or claim new items until one has
+// Claim the next tile (thread 0 only): continue the current item or take new items until one has
 // tuples. Returns a slot with item == ~0u when the work is exhausted. Segment mode: `pend` carries
 // seg_next of the tile returned last, loaded then so that its latency passes while that tile is
 // processed.
 template <int T>
 __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it, uint32_t nitems,
-                                              uint32_t &pend) {
+                                              uint32_t &pend, ItemAhead &ah) {
     TileSlot s;
     if (a.seg_head && it.item != ~0u && it.done > 0 && it.done < it.len) it.seg = pend;
+    if (ah.stage == 1) item_fetch(a, ah, nitems);
     for (;;) {
         while (it.item == ~0u || it.done >= it.len) {
-            const uint32_t item = atomicAdd(&a.counters[a.ctr_item], 1u);
-            if (item >= nitems) {
+            if (ah.stage == 0) {
+                ah.item = atomicAdd(&a.counters[a.ctr_item], 1u);
+                ah.stage = 1;
+            }
+            if (ah.stage == 1) item_fetch(a, ah, nitems);
+            const ItemAhead cur = ah;
+            ah.stage = 0;
+            if (cur.item >= nitems) {
                 s.item = ~0u;
                 s.in = nullptr;
                 s.out = nullptr;
@@ -635,10 +663,17 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
                 it.done = 0;
                 return s;
             }
-            item_decode(a, item, it);
+            // Pass 2: claim the following item now; its id and description are needed only when this
+            // one is done. (Pass-1 items are long, and an item held back per CTA lengthens the tail
+            // by more than the claim costs.)
+            if (a.pass != 0) {
+                ah.item = atomicAdd(&a.counters[a.ctr_item], 1u);
+                ah.stage = 1;
+            }
+            item_decode(a, cur.item, cur, it);
         }
         if (!a.seg_head) break;
-        if (it.seg < a.max_segs) break;
+        if (it.len == 0 || it.seg < a.max_segs) break;
         // A chain that leaves the segment storage (pass 1 stopped early): drop the rest of the unit.
         set_error(&a.counters[kCtrErr], kErrCapacity);
         it.done = it.len;
@@ -687,6 +722,11 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     const int nbins = 1 << a.bits;
     __shared__ ItemIter it;  // used by thread 0 only
     uint32_t pend = 0;       // thread 0: next segment of the chain (segment mode)
+    ItemAhead ah;            // thread 0: the item claimed ahead
+    ah.item = 0;
+    ah.stage = 0;
+    ah.len = ah.off = 0;
+    ah.seg = 0;
 
     if (!STABLE)
         for (int j = tid; j < 256; j += THREADS) thist[j] = 0;
@@ -696,7 +736,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         if (NBUF == 2) {
-            const TileSlot s0 = next_tile<T>(a, it, nitems, pend);
+            const TileSlot s0 = next_tile<T>(a, it, nitems, pend, ah);
             slots[0] = s0;
             if (s0.item != ~0u && !(a.test_stall && blockIdx.x == 0)) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
         }
@@ -709,7 +749,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             // One buffer: load this tile now (the barrier that ended the previous iteration ordered
             // every read of the buffer before this copy).
             if (tid == 0) {
-                const TileSlot sn = next_tile<T>(a, it, nitems, pend);
+                const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
                 slots[0] = sn;
                 if (sn.item != ~0u && !(a.test_stall && blockIdx.x == 0 && k == 0))
                     tma_load_1d(inbuf, sn.in, sn.cnt * 16u, bar0);
@@ -722,7 +762,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         // Prefetch the next tile into the other buffer; the barrier that ended the previous iteration
         // ordered every read of it before this copy.
         if (NBUF == 2 && tid == 0) {
-            const TileSlot sn = next_tile<T>(a, it, nitems, pend);
+            const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
             slots[cur ^ 1u] = sn;
             if (sn.item != ~0u) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
         }
