@@ -163,3 +163,15 @@ def test_reference_table_names_resolve(hj):
         assert hj.ALGOS[base] == out.value, name
         assert getattr(L, name)  # exported under the reference's name
     assert sum(n.startswith("ptr_") for n in names) == 10
+
+
+def test_python_flag_constants_match_header(hj):
+    # The ctypes binding's flag values are the C header's #defines.
+    import re
+    text = (hj.HERE.parent / "include" / "hjscm.h").read_text()
+    defs = {m.group(1): int(m.group(2), 16) for m in re.finditer(r"#define (HJ_F_\w+)\s+0x([0-9a-fA-F]+)u", text)}
+    assert {"HJ_F_SEGMENTS", "HJ_F_EXACT", "HJ_F_PHASE_TIMES", "HJ_F_TEST_STALL"} <= set(defs)
+    for name, value in defs.items():
+        if hasattr(hj, name):
+            assert getattr(hj, name) == value, name
+    assert len(set(defs.values())) == len(defs)  # no two flags share a bit
