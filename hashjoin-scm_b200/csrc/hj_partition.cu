@@ -1865,9 +1865,12 @@ struct PhjSizes {
     ChunkGeom cg;
 };
 
-// Segment mode from 2^26 tuples: below that the histogram read it saves is small next to the
-// storage of the partly filled segments (2 * CTAs * F1 * kTile tuples).
-constexpr uint64_t kSegMinTuples = 1ull << 26;
+// Segment mode from 2^27 tuples. Its pass 2 has one unit per (pass-1 CTA, relation, digit) and a
+// partial tile per unit whatever the size, and its pass 1 runs at two CTAs per SM. At 2^24 x 2^26
+// (2^26.3 tuples) the joins of both pipelines took the same time; the saved histogram read grows with
+// the size (1.3 ms of 11.8 at 2^27 x 2^29). The partly filled segments also reserve storage
+// (2 * CTAs * F1 * kTile tuples).
+constexpr uint64_t kSegMinTuples = 1ull << 27;
 
 bool phj_seg_applies(const RadixGeom &g, bool lp, size_t nR, size_t nS) {
     return !lp && g.passes == 2 && g.bits <= kSegMaxBits && (uint64_t)nR + nS >= kSegMinTuples;

@@ -99,7 +99,7 @@ typedef struct {
 #define HJ_F_NO_TIMING   0x1u /* skip the per-phase CUDA events (buildpart/probejoin stay 0) */
 #define HJ_F_PINNED_HOST 0x2u /* host inputs are already page-locked */
 #define HJ_F_PHASE_TIMES 0x4u /* also time each kernel group (fills hj_result_t.phase) */
-/* Radix joins that count every match (bc, sc, hr, hro; two passes, <= 14 bits) from 2^26 tuples run
+/* Radix joins that count every match (bc, sc, hr, hro; two passes, <= 14 bits) from 2^27 tuples run
  * in segment mode: pass 1 writes chains of fixed-size segments and counts the histograms itself, so no
  * histogram pass reads the relations first (if the larger scratch does not fit, the exact-offset
  * pipeline runs). These flags pick the pipeline regardless of size; results are the same. */

@@ -115,8 +115,8 @@ def test_segment_mode_materialising(hj, oracle, cuda):
 
 
 def test_segment_mode_by_size(hj, cuda):
-    # From 2^26 tuples segment mode is the default; the exact pipeline gives the same result.
-    nR, nS = 1 << 24, 1 << 26
+    # From 2^27 tuples segment mode is the default; the exact pipeline gives the same result.
+    nR, nS = 1 << 25, 1 << 27
     torch = cuda
     R = torch.empty((nR, 2), dtype=torch.int64, device="cuda")
     S = torch.empty((nS, 2), dtype=torch.int64, device="cuda")
