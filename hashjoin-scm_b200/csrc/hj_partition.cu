@@ -37,6 +37,11 @@
 //   join_large_*       partitions whose R side exceeds shared memory: chains in global memory
 // The join kernels have a materialising variant (MAT) for the ptr_* joins: one (r.row_id, s.row_id)
 // pair per match instead of the sums.
+//
+// Segment mode (joins that count every match, two passes, <= 14 bits, from 2^27 tuples): no histogram
+// pass. seg_pass1_kernel writes pass 1 into per-(CTA, relation, digit) chains of tile-sized segments
+// and counts each CTA's joint histogram itself; colscan/plan/units then treat the pass-1 CTAs as the
+// chunks, and pass 2 (scatter_kernel) walks the chains as its units.
 #include <cstdio>
 
 #include "hj_common.cuh"
