@@ -93,7 +93,8 @@ def workload_config(a, n_gpus):
         "parallelism": f"{n_gpus} independent joins, one per GPU" if n_gpus > 1 else "1 GPU",
         "l2": "inputs (R+S = %.1f GB) larger than L2 (126 MB); no flush between steps"
               % (((1 << a.nr_log) + (1 << a.ns_log)) * 16 / 1e9),
-        "generator": "seeded Feistel permutation on the device (gen_pkfk_uniform distribution)",
+        "generator": "seeded Feistel permutation (gen_pkfk_uniform distribution; the GPU arm generates it on "
+                     "the device, the CPU baseline writes the same bytes to its .bin files)",
     }
 
 
@@ -210,8 +211,12 @@ def host_mem_available_gb() -> float:
     return 0.0
 
 
-def cpu_reference_run(hj, a, trials: int, sample_log: int = 0):
-    """Returns (throughput tuples/s list over timed trials, sample description, threads, kind)."""
+def cpu_reference_run(a, trials: int, warmup: int = 1, sample_log: int = 0):
+    """The reference's own multithreaded join (oracle/_ref) on the host cores, on relations written by
+    the oracle's restatement of the library's generator (the same bytes as the GPU arm's relations, made
+    without loading the library). Runs warmup + trials trials and drops the first `warmup` (the
+    reference drops one, src/main.c:434). Returns (throughput tuples/s per timed trial, sample
+    description, threads, kind)."""
     orc = load_module("hj_oracle", ROOT / "oracle" / "hj_oracle.py")
     nr_log, ns_log = a.nr_log, a.ns_log
     if sample_log:
@@ -227,38 +232,35 @@ def cpu_reference_run(hj, a, trials: int, sample_log: int = 0):
     nR, nS = 1 << nr_log, 1 << ns_log
     threads = os.cpu_count() or 1
     passes = a.passes
+    if not orc.ref_available(passes):
+        raise RuntimeError("oracle/_ref is not built")
     tmpdir = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    warmup = max(1, warmup)
     with tempfile.TemporaryDirectory(dir=tmpdir) as d:
-        R, S = hj.gen_fast_host(nR, nS, seed=12345)
-        R.tofile(os.path.join(d, "r.bin"))
-        S.tofile(os.path.join(d, "s.bin"))
-        del R, S
-        if orc.ref_available(passes):
-            runs = orc.ref_run_files(a.algo.replace("_bw_reg", ""), d, "r.bin", "s.bin", nR, nS, bits=a.bits,
-                                     passes=passes, threads=threads, trials=trials + 1, timeout=1800)
-            kind = "reference"
-        else:
-            raise RuntimeError("oracle/_ref is not built")
-    want = hj.pkfk_closed_form(nR, nS)
+        orc.gen_fast_files(d, "r.bin", "s.bin", nR, nS, seed=12345, threads=threads)
+        runs = orc.ref_run_files(a.algo.replace("_bw_reg", ""), d, "r.bin", "s.bin", nR, nS, bits=a.bits,
+                                 passes=passes, threads=threads, trials=trials + warmup, timeout=1800)
+    want = orc.pkfk_closed_form(nR, nS)
     for r in runs:
         if (r[0], r[1]) != want:
             raise RuntimeError(f"reference result {r[:2]} != closed form {want}")
-    timed = runs[1:]  # the reference drops its first trial as warm-up (src/main.c:434)
+    timed = runs[warmup:]
     thr = [(nR + nS) / r[4] for r in timed]
-    sample = f"{a.algo} R=2^{nr_log} S=2^{ns_log}, {len(timed)} timed trials after 1 warm-up, reference timekeeper total"
-    return thr, sample, threads, kind
+    sample = (f"{a.algo} R=2^{nr_log} S=2^{ns_log}, {len(timed)} timed trials after {warmup} warm-up, "
+              "reference timekeeper total (buildpart + probejoin, src/algo/phj.c:2509-2511)")
+    return thr, sample, threads, "reference"
 
 
 # ---------------------------------------------------------------------------------------------
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return 0
-    hj = load_module("hashjoin_scm_b200", PKG_DIR / "__init__.py")
-    thr, sample, threads, kind = cpu_reference_run(hj, a, trials=max(a.steps, 1), sample_log=a.cpu_sample_log)
+    thr, sample, threads, kind = cpu_reference_run(a, trials=max(a.steps, 1), warmup=a.warmup,
+                                                   sample_log=a.cpu_sample_log)
     value = statistics.mean(thr)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": len(thr),
-        "warmup": 1, "ms_per_step": ((1 << a.nr_log) + (1 << a.ns_log)) / value * 1e3,
+        "warmup": max(1, a.warmup), "ms_per_step": ((1 << a.nr_log) + (1 << a.ns_log)) / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic", "config": workload_config(a, a.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
@@ -397,7 +399,7 @@ def run_ours(a, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
-            thr, sample, threads, kind = cpu_reference_run(hj, a, trials=2, sample_log=a.cpu_sample_log)
+            thr, sample, threads, kind = cpu_reference_run(a, trials=2, sample_log=a.cpu_sample_log)
             cpu = {"value": statistics.mean(thr), "unit": UNIT, "cores": threads, "kind": kind, "sample": sample}
         except Exception as exc:  # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
@@ -408,11 +410,11 @@ def run_ours(a, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": dict(workload_config(a, world),
-                           **({"partition_pipeline": "segment mode: pass 1 writes segment chains and counts "
-                               "the histograms (no histogram pass)" if seg_mode else
-                               "exact offsets: histogram pass, then two scatter passes"}
-                              if a.algo.startswith("phj") else {})),
+            "config": workload_config(a, world),
+            "partition_pipeline": (("segment mode: pass 1 writes segment chains and counts the histograms "
+                                    "(no histogram pass)" if seg_mode else
+                                    "exact offsets: histogram pass, then two scatter passes")
+                                   if a.algo.startswith("phj") else None),
             "roofline": roofline, "pipeline": pipeline, "e2e": e2e, "cpu_baseline": cpu,
             "clocks": clocks, "gpu_launches": launches,
         }

@@ -11,6 +11,8 @@
 // loads the library keeps it until the process exits. All calls share it and it keeps the last call's
 // contents, so each call clears what must start empty (table, side record, result) on its stream, and
 // calls whose work overlaps on the GPU (different streams, or different host threads) race.
+#include <cuda.h>
+
 #include <cstdio>
 #include <mutex>
 
@@ -31,14 +33,42 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[64] = {};
 int g_noalloc_sms[64] = {};
+unsigned long long g_noalloc_ctx[64] = {};
 
-// Device address of the scratch array on the current device, looked up once per device. The name of
-// the array in host code is only a host-side stand-in; kernels must be given this address instead.
+// Process-unique id of the CUDA context current on this thread (0 when none is current yet). The
+// driver's entry points are fetched through the runtime, so the library needs no link to libcuda.
+unsigned long long current_context_id() {
+    using get_current_fn = CUresult (*)(CUcontext *);
+    using get_id_fn = CUresult (*)(CUcontext, unsigned long long *);
+    static get_current_fn get_current = nullptr;
+    static get_id_fn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", reinterpret_cast<void **>(&get_current), cudaEnableDefault,
+                                    &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", reinterpret_cast<void **>(&get_id), cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+        cudaGetLastError();
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the scratch array on the current device. The name of the array in host code is
+// only a host-side stand-in; kernels must be given this address instead. It is looked up on the first
+// call per device and again whenever the device's context changed since (a cudaDeviceReset, or a new
+// primary context, reloads the library's module, and the array may then sit elsewhere).
 int noalloc_setup(int dev, void **ptr, int *sms) {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    unsigned long long ctx = current_context_id();
+    if (!g_noalloc_ptr[dev] || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
         void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // makes the device's context current
         if (e != cudaSuccess || !p) {
             fprintf(stderr, "hj_nphj_join_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
             cudaGetLastError();
@@ -49,6 +79,7 @@ int noalloc_setup(int dev, void **ptr, int *sms) {
         if (e != cudaSuccess) return HJ_E_DEVICE;
         g_noalloc_ptr[dev] = p;
         g_noalloc_sms[dev] = n;
+        g_noalloc_ctx[dev] = current_context_id();
     }
     *ptr = g_noalloc_ptr[dev];
     *sms = g_noalloc_sms[dev];

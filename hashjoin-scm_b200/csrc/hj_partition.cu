@@ -787,12 +787,16 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             running[tid] = off;
         }
         const uint32_t cnt = sl.cnt;
-        const bool ok = mbar_wait(bar0 + 8u * cur, NBUF == 2 ? ((k >> 1) & 1u) : (k & 1u));
+        const uint32_t par = NBUF == 2 ? ((k >> 1) & 1u) : (k & 1u);
+        const bool ok = mbar_wait(bar0 + 8u * cur, par);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 set_error(err, kErrSpinLimit);
-                // Before leaving, let the prefetch into the other buffer land (bounded as well): the
-                // copy must not write into shared memory this CTA no longer owns.
+                // Before leaving, let every copy this CTA issued land (bounded waits as well): no copy
+                // may write into shared memory the CTA no longer owns. The load into this buffer was
+                // issued unless the stall hook withheld it (CTA 0's first tile); the prefetch into the
+                // other buffer was issued if it has a tile.
+                if (!(a.test_stall && blockIdx.x == 0 && k == 0)) mbar_wait(bar0 + 8u * cur, par);
                 if (NBUF == 2 && slots[cur ^ 1u].item != ~0u) mbar_wait(bar0 + 8u * (cur ^ 1u), ((k + 1) >> 1) & 1u);
             }
             break;
@@ -1152,6 +1156,9 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 set_error(err, kErrSpinLimit);
+                // Let the copies this CTA issued land first (bounded): this buffer's, unless the stall
+                // hook withheld it (CTA 0's first tile), and the prefetch into the other one.
+                if (!(a.test_stall && blockIdx.x == 0 && k == 0)) mbar_wait(bar0 + 8u * cur, (k >> 1) & 1u);
                 if (slots[cur ^ 1u].cnt) mbar_wait(bar0 + 8u * (cur ^ 1u), ((k + 1) >> 1) & 1u);
             }
             break;
@@ -1579,6 +1586,8 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
             set_error(err, kErrSpinLimit);
             ok = false;
         }
+        // An expired wait: let the R-tile copy land (bounded) before the CTA leaves its shared memory.
+        if (!ok && tid == 0) mbar_wait(bar, phase);
         phase ^= 1u;
         if (__syncthreads_or(!ok)) break;
         // Build: chain every R tuple (lp_join skips key 0, which reads as an empty slot there).

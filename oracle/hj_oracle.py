@@ -173,6 +173,137 @@ def gen_zipf(nS: int, nR: int, factor: float, seed: int = 12345):
 
 
 # ------------------------------------------------------------------------------------------------
+# The library's parallel PK-FK generator (hj_gen_fast_host / hj_gen_fast_device), restated in numpy
+# so that the CPU-baseline leg of the benchmark can write the same relations without loading the
+# library. The reference draws its permutation with a sequential Knuth shuffle (src/gen.c:161-171);
+# the library replaces that shuffle by a keyed bijection of [0, n): a 6-round unbalanced Feistel
+# network over the smallest power of two >= n (round function: the splitmix64 output mix of Steele,
+# Lea and Flood, 2014), with cycle walking back into [0, n). R tuple i = perm_R(i) + 1 (mod the
+# distinct-key count for the duplicate variant); S tuple j = perm_S(j) mod |distinct| + 1.
+# ------------------------------------------------------------------------------------------------
+_GOLDEN = 0x9E3779B97F4A7C15
+
+
+def _mix64_int(z: int) -> int:
+    z ^= z >> 30
+    z = (z * 0xBF58476D1CE4E5B9) & MASK64
+    z ^= z >> 27
+    z = (z * 0x94D049BB133111EB) & MASK64
+    z ^= z >> 31
+    return z
+
+
+def _mix64_inplace(z: np.ndarray, t: np.ndarray) -> None:
+    np.right_shift(z, np.uint64(30), out=t)
+    z ^= t
+    z *= np.uint64(0xBF58476D1CE4E5B9)
+    np.right_shift(z, np.uint64(27), out=t)
+    z ^= t
+    z *= np.uint64(0x94D049BB133111EB)
+    np.right_shift(z, np.uint64(31), out=t)
+    z ^= t
+
+
+class _Feistel:
+    """Keyed bijection of [0, n): the same network as the library's host/device generators."""
+
+    def __init__(self, n: int, seed: int):
+        k = 2
+        while k < 64 and (1 << k) < n:
+            k += 1
+        self.n = n
+        self.lo_bits, self.hi_bits = k // 2, k - k // 2
+        self.lo_mask = np.uint64((1 << self.lo_bits) - 1)
+        self.hi_mask = np.uint64((1 << self.hi_bits) - 1)
+        s, self.keys = seed & MASK64, []
+        for _ in range(6):
+            s = (s + _GOLDEN) & MASK64
+            self.keys.append(np.uint64(_mix64_int(s)))
+
+    def _pass(self, x: np.ndarray) -> np.ndarray:
+        lo = x & self.lo_mask
+        hi = (x >> np.uint64(self.lo_bits)) & self.hi_mask
+        f, t = np.empty_like(lo), np.empty_like(lo)
+        for r in range(6):
+            src, dst, mask = (lo, hi, self.hi_mask) if r % 2 == 0 else (hi, lo, self.lo_mask)
+            np.bitwise_xor(src, self.keys[r], out=f)
+            _mix64_inplace(f, t)
+            f &= mask
+            dst ^= f
+        hi <<= np.uint64(self.lo_bits)
+        hi |= lo
+        return hi
+
+    def perm(self, idx: np.ndarray) -> np.ndarray:
+        if self.n <= 1:
+            return np.zeros_like(idx)
+        y = self._pass(idx)
+        out = y >= np.uint64(self.n)
+        while out.any():  # cycle walking
+            sel = np.nonzero(out)[0]
+            y[sel] = self._pass(y[sel])
+            out[sel] = y[sel] >= np.uint64(self.n)
+        return y
+
+
+def gen_fast_into(R: np.ndarray, S: np.ndarray, seed: int = 12345, payload: bool = False, dup: int = 1,
+                  threads: int | None = None, chunk: int = 1 << 16) -> None:
+    """Fill R (nR x 2 uint64) and S (nS x 2 uint64) - np.memmap views of .bin files included - with the
+    bytes hj_gen_fast_host writes for (nR, nS, seed, payload, dup). Chunks run on a thread pool (numpy
+    releases the GIL inside its loops)."""
+    import concurrent.futures
+
+    nR, nS = R.shape[0], S.shape[0]
+    dup = max(1, int(dup))
+    distinct = (nR + dup - 1) // dup
+    payload = bool(payload) or dup > 1
+    fr = _Feistel(nR, (seed ^ 0x5245) & MASK64)
+    fs = _Feistel(nS if nS else 1, (seed ^ 0x53 ^ 0x7F4A7C159E3779B9) & MASK64)
+
+    def fill(out, f, lo, hi, side_r):
+        idx = np.arange(lo, hi, dtype=np.uint64)
+        p = f.perm(idx)
+        if side_r and distinct == f.n:
+            key = p + np.uint64(1)
+        else:
+            key = p % np.uint64(distinct) + np.uint64(1)
+        out[lo:hi, 0] = key
+        out[lo:hi, 1] = idx + np.uint64(1) if payload else key
+
+    jobs = [(R, fr, lo, min(nR, lo + chunk), True) for lo in range(0, nR, chunk)]
+    jobs += [(S, fs, lo, min(nS, lo + chunk), False) for lo in range(0, nS, chunk)]
+    with concurrent.futures.ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
+        for fut in [ex.submit(fill, *j) for j in jobs]:
+            fut.result()
+
+
+def gen_fast(nR: int, nS: int, seed: int = 12345, payload: bool = False, dup: int = 1,
+             threads: int | None = None):
+    R = np.empty((nR, 2), dtype=np.uint64)
+    S = np.empty((nS, 2), dtype=np.uint64)
+    gen_fast_into(R, S, seed, payload, dup, threads)
+    return R, S
+
+
+def gen_fast_files(prefix: str, rfile: str, sfile: str, nR: int, nS: int, seed: int = 12345,
+                   threads: int | None = None) -> None:
+    """Write gen_fast's relations (payload = key) straight into two raw .bin files of 16-byte tuples."""
+    R = np.memmap(os.path.join(prefix, rfile), dtype=np.uint64, mode="w+", shape=(nR, 2))
+    S = np.memmap(os.path.join(prefix, sfile), dtype=np.uint64, mode="w+", shape=(nS, 2))
+    gen_fast_into(R, S, seed, threads=threads)
+    R.flush()
+    S.flush()
+    del R, S
+
+
+def pkfk_closed_form(nR: int, nS: int) -> tuple[int, int]:
+    """PK-FK uniform data with row_id = key and nS a multiple of nR: every probe tuple matches once and
+    check_sum = m n (n + 1) mod 2^64 with m = nS / nR (the reference's closed form)."""
+    m = nS // nR
+    return nS, (m * nR * (nR + 1)) & MASK64
+
+
+# ------------------------------------------------------------------------------------------------
 # C oracle
 # ------------------------------------------------------------------------------------------------
 _lib = None
@@ -269,13 +400,22 @@ def phj_literal(bits: int, passes: int, lp: bool, R: np.ndarray, S: np.ndarray) 
 # ------------------------------------------------------------------------------------------------
 # The reference itself (oracle/_ref, built from its sources by oracle/Makefile)
 # ------------------------------------------------------------------------------------------------
-# Where the reference's sources are mounted in the build container (oracle/Makefile's REF); the GPU
-# machines have only the binaries built from them.
-REF_SOURCES = pathlib.Path("/root/reference/src")
+# Where the reference's sources are: $HJ_REFERENCE_ROOT, else the REF default of oracle/Makefile (the
+# recipe that compiles them). Machines that only run the prebuilt binaries have no sources.
+def _reference_root() -> pathlib.Path | None:
+    env = os.environ.get("HJ_REFERENCE_ROOT")
+    if env:
+        return pathlib.Path(env)
+    m = re.search(r"^REF \?= *(\S+)", (HERE / "Makefile").read_text(), re.M)
+    return pathlib.Path(m.group(1)) if m else None
+
+
+_REF_ROOT = _reference_root()
+REF_SOURCES = _REF_ROOT / "src" if _REF_ROOT else None
 
 
 def ref_sources_present() -> bool:
-    return REF_SOURCES.exists()
+    return REF_SOURCES is not None and (REF_SOURCES / "algo" / "phj.c").exists()
 
 
 def ref_available(passes: int = 2) -> bool:
@@ -285,7 +425,10 @@ def ref_available(passes: int = 2) -> bool:
 def ref_build() -> bool:
     if not ref_sources_present():
         return ref_available(1) and ref_available(2)
-    out = subprocess.run(["make", "-C", str(HERE), "ref"], capture_output=True, text=True)
+    env = dict(os.environ)
+    if _REF_ROOT is not None:
+        env["REF"] = str(_REF_ROOT)
+    out = subprocess.run(["make", "-C", str(HERE), "ref"], capture_output=True, text=True, env=env)
     return out.returncode == 0
 
 
