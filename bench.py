@@ -56,7 +56,7 @@ def parse_args():
                          "skew: 2^26 x 2^28 lp joins on Zipf and duplicate-key data; "
                          "mat: the materialising ptr_ join at the headline size; "
                          "stream: R on the device, 2^32 probe tuples streamed from host memory")
-    ap.add_argument("--rates", default="250,500,1000,1500,2000",
+    ap.add_argument("--rates", default="250,1000,2000,3000",
                     help="serve mode: offered request rates (requests/s) to sweep")
     ap.add_argument("--requests", type=int, default=1000, help="serve mode: requests per rate")
     ap.add_argument("--slots", type=int, default=8, help="serve mode: concurrent requests on the GPU")
@@ -104,7 +104,7 @@ def workload_config(a, n_gpus):
 class ClockSampler:
     FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, bus_id: str | None):
         self.bus_id = (bus_id or "").lower()
@@ -151,12 +151,15 @@ class ClockSampler:
             except (ValueError, IndexError):
                 return None
 
-        sm = [num(r[2]) for r in rows if num(r[2]) is not None]
+        # Samples taken while the GPU was busy (utilization >= 50%); all samples when none were.
+        loaded = [r for r in rows if len(r) > 10 and (num(r[10]) or 0) >= 50] or rows
+        sm = [num(r[2]) for r in loaded if num(r[2]) is not None]
         mx = [num(r[3]) for r in rows if num(r[3]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(loaded) if loaded is not rows
+                else 0}
 
 
 def reduce_over_ranks(value: float, dist, device, op: str = "max") -> float:
@@ -176,10 +179,23 @@ def whole_job_rate(units_per_rank: float, world: int, seconds: float) -> float:
     return world * units_per_rank / seconds
 
 
+_MODE_SAMPLER = None  # clock sampler running over a whole non-headline mode (started in main)
+
+
 def emit(rank: int, line: dict) -> None:
-    """Rank 0 prints the one JSON line of the run."""
+    """Rank 0 prints the one JSON line of the run (with the mode's clock record, when one is sampled)."""
+    if _MODE_SAMPLER is not None and "clocks" not in line:
+        line["clocks"] = _MODE_SAMPLER.stop()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def device_bus_id(torch, dev):
+    try:
+        pr = torch.cuda.get_device_properties(dev)
+        return "%02x:%02x.0" % (int(pr.pci_bus_id), int(pr.pci_device_id))
+    except (AttributeError, TypeError, ValueError):
+        return None
 
 
 def measured_peaks():
@@ -301,13 +317,7 @@ def run_ours(a, rank, world, local_rank):
 
     for _ in range(a.warmup):
         step()
-    bus = None
-    try:
-        pr = torch.cuda.get_device_properties(dev)
-        bus = "%02x:%02x.0" % (int(pr.pci_bus_id), int(pr.pci_device_id))
-    except (AttributeError, TypeError, ValueError):
-        pass
-    sampler = ClockSampler(bus)
+    sampler = ClockSampler(device_bus_id(torch, dev))
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -529,7 +539,8 @@ def run_batch_mode(a, rank, world, local_rank):
             "tuner": {"nphj_max_table_bytes": tuner.nphj_max_table_bytes, "calibrated": tuner.calibrated,
                       "phj_fixed_s": tuner.phj_fixed, "calibration": calib},
         }
-        print(json.dumps(line), flush=True)
+    if rank == 0:
+        emit(rank, line)
     ctx.close()
     return 0
 
@@ -561,9 +572,12 @@ def serve_workload(hj, torch, dev, n_small, seed):
 
 
 def run_serve_mode(a, rank, world, local_rank):
-    """Poisson arrivals at each offered rate; 5% of requests are the 2^26 x 2^28 join. The join server
-    (slots, HBM pool budget, per-request autotuned implementation) is compared with a sequential
-    per-join loop (hj_join with the same per-request decision) serving the same arrival times."""
+    """Served joins: 95% of requests sized as the batched joins, 5% 2^26 x 2^28, relations device-resident.
+    (1) Saturation: the whole request sequence submitted at once to the join server (continuous batching:
+    small requests coalesced into waves, large ones on slots), against the plain per-join loop
+    (phj_radix_bc, 14 bits, 2 passes for every request, as a caller of the reference's interface would
+    run them) and the tuned loop (hj_join with the tuner's per-request decision), on the same sequence.
+    (2) Latency: Poisson arrivals at each offered rate, server against the tuned loop."""
     import ctypes
 
     import numpy as np
@@ -576,11 +590,15 @@ def run_serve_mode(a, rank, world, local_rank):
     small, big, buf = serve_workload(hj, torch, dev, 64, 12345 + 1000 * rank)
     rates = [float(x) for x in a.rates.split(",") if x]
     rng = np.random.default_rng(777 + rank)
+
+    def picks_of(n):
+        return [big if rng.random() < 0.05 else small[int(rng.integers(len(small)))] for _ in range(n)]
+
+    sat_picks = picks_of(a.requests)
     streams = []
     for lam in rates:
         arrivals = np.cumsum(rng.exponential(1.0 / lam, a.requests))
-        picks = [big if rng.random() < 0.05 else small[int(rng.integers(len(small)))] for _ in range(a.requests)]
-        streams.append((lam, arrivals, picks))
+        streams.append((lam, arrivals, picks_of(a.requests)))
 
     def pace(t_arr):
         while True:
@@ -598,12 +616,27 @@ def run_serve_mode(a, rank, world, local_rank):
                 "small_p50_ms": float(np.percentile(small_lat, 50) * 1e3),
                 "small_p99_ms": float(np.percentile(small_lat, 99) * 1e3)}
 
-    # 1. the join server
-    srv_out, peak, budget = [], 0.0, 0.0
+    def check(c, want, what):
+        if c.status or (c.matched_cnt, c.checksum) != want:
+            raise RuntimeError(f"{what} result differs from the closed form")
+
+    # 1. the join server: saturation, then the offered-rate sweep
+    srv_out = []
     impl_counts = {0: 0, 1: 0}
     with hj.Server(local_rank, slots=a.slots, hbm_budget_bytes=a.budget_gb * 1e9, large_sm_share=a.large_share) as srv:
         for R, S, _ in small[:8] + [big]:  # warm-up: kernel attributes, first launches
             srv.wait_all([srv.submit("phj_radix_bc", R, S, on_device=True)])
+        st0 = srv.stats()
+        t0 = hj.now()
+        ids = [srv.submit("phj_radix_bc", R, S, on_device=True) for R, S, _ in sat_picks]
+        got = srv.wait_all(ids, timeout_s=600.0)
+        t_last = max(c.done_s for c in got.values())
+        for rid, (R, S, want) in zip(ids, sat_picks):
+            check(got[rid], want, "served join")
+        st1 = srv.stats()
+        sat_server = {"joins_per_s": len(ids) / (t_last - t0), "seconds": t_last - t0,
+                      "waves": st1.waves - st0.waves, "wave_requests": st1.wave_requests - st0.wave_requests,
+                      "max_wave_size": max((c.wave_size for c in got.values()), default=0)}
         for lam, arrivals, picks in streams:
             t0 = hj.now() + 0.02
             ids = []
@@ -614,8 +647,7 @@ def run_serve_mode(a, rank, world, local_rank):
             lat, t_last = [], t0
             for rid, (R, S, want), t in zip(ids, picks, arrivals):
                 c = got[rid]
-                if c.status or (c.matched_cnt, c.checksum) != want:
-                    raise RuntimeError("served join result differs from the closed form")
+                check(c, want, "served join")
                 lat.append(c.done_s - (t0 + t))
                 t_last = max(t_last, c.done_s)
                 impl_counts[c.impl] += 1
@@ -623,7 +655,7 @@ def run_serve_mode(a, rank, world, local_rank):
         st = srv.stats()
         peak, budget = st.peak_in_use_bytes, st.budget_bytes
 
-    # 2. sequential per-join loop on the same arrivals
+    # 2. sequential per-join loops on the same sequences
     loop_out = []
     with hj.Context(local_rank) as ctx:
         def decided(R, S):
@@ -633,16 +665,38 @@ def run_serve_mode(a, rank, world, local_rank):
             return ("nphj_sc", {}) if impl.value == 0 else ("phj_radix_bc", {"bits": bits.value, "passes": passes.value})
 
         plans = {id(p[0]): decided(p[0], p[1]) for p in small + [big]}
+        plain = ("phj_radix_bc", {"bits": 14, "passes": 2})
+
+        def one(R, S, plan):
+            algo, kw = plan
+            return hj.join(algo, R, S, on_device=True, device=local_rank, ctx=ctx, flags=hj.HJ_F_NO_TIMING, **kw)
+
         for R, S, _ in small[:8] + [big]:
-            algo, kw = plans[id(R)]
-            hj.join(algo, R, S, on_device=True, device=local_rank, ctx=ctx, flags=hj.HJ_F_NO_TIMING, **kw)
+            one(R, S, plans[id(R)])
+            one(R, S, plain)
+        sat_loops = {}
+        for name in ("plain", "tuned"):
+            t_small = t_large = 0.0
+            t0 = hj.now()
+            for R, S, want in sat_picks:
+                ta = hj.now()
+                r = one(R, S, plain if name == "plain" else plans[id(R)])
+                tb = hj.now()
+                if (r.matched_cnt, r.checksum) != want:
+                    raise RuntimeError(f"{name} loop result differs from the closed form")
+                if R is big[0]:
+                    t_large += tb - ta
+                else:
+                    t_small += tb - ta
+            el = hj.now() - t0
+            sat_loops[name] = {"joins_per_s": len(sat_picks) / el, "seconds": el, "large_requests_s": t_large,
+                               "small_requests_s": t_small}
         for lam, arrivals, picks in streams:
             t0 = hj.now() + 0.02
             lat, t_last = [], t0
             for (R, S, want), t in zip(picks, arrivals):
                 pace(t0 + t)
-                algo, kw = plans[id(R)]
-                r = hj.join(algo, R, S, on_device=True, device=local_rank, ctx=ctx, flags=hj.HJ_F_NO_TIMING, **kw)
+                r = one(R, S, plans[id(R)])
                 done = hj.now()
                 if (r.matched_cnt, r.checksum) != want:
                     raise RuntimeError("looped join result differs from the closed form")
@@ -650,33 +704,32 @@ def run_serve_mode(a, rank, world, local_rank):
                 t_last = done
             loop_out.append(summarize(lat, picks, t0, t_last, len(picks)))
 
-    # sustained rate: the highest offered rate the server kept up with (completion rate >= 95% offered)
-    best = 0
-    for i, (lam, _, _) in enumerate(streams):
-        if srv_out[i]["joins_per_s"] >= 0.95 * lam:
-            best = i
+    # Amdahl: the server runs the large requests with the same partitioned pipeline as the plain loop, so
+    # its speed-up over that loop is at most (the loop's total time) / (the loop's time on large requests).
+    pl = sat_loops["plain"]
+    bound = pl["seconds"] / pl["large_requests_s"] if pl["large_requests_s"] > 0 else None
     dist = None
     if world > 1:
         import torch.distributed as dist
-    # the slowest rank's sustained rate, times the ranks (each serves its own stream)
-    joins_s = world * reduce_over_ranks(srv_out[best]["joins_per_s"], dist, dev, op="min")
-    if rank == 0:
-        line = {
-            "metric": "served joins/s at p99 latency", "value": joins_s, "unit": "joins/s", "n_gpus": world,
-            "steps": a.requests, "warmup": 9, "ms_per_step": 1e3 / srv_out[best]["joins_per_s"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic",
-            "config": {"workload": "Poisson stream of PK-FK join requests (phj_radix_bc semantics): 95% sized "
-                                   "|R| log-uniform in [2^10, 2^22], |S| = k|R| with k in 1..16, 5% 2^26 x 2^28; "
-                                   "relations device-resident", "requests_per_rate": a.requests,
-                       "slots": a.slots, "hbm_budget_bytes": budget, "peak_pool_bytes": peak},
-            "p50_ms": srv_out[best]["p50_ms"], "p99_ms": srv_out[best]["p99_ms"],
-            "offered_rate": streams[best][0],
-            "sweep": [{"offered_rate": lam, "server": s, "loop": l}
-                      for (lam, _, _), s, l in zip(streams, srv_out, loop_out)],
-            "impl_counts": {"nphj": impl_counts[0], "phj": impl_counts[1]},
-        }
-        print(json.dumps(line), flush=True)
+    joins_s = world * reduce_over_ranks(sat_server["joins_per_s"], dist, dev, op="min")
+    n_big = sum(1 for p in sat_picks if p is big)
+    emit(rank, {
+        "metric": "served joins/s at saturation (continuous batching), p50/p99 latency", "value": joins_s,
+        "unit": "joins/s", "n_gpus": world, "steps": a.requests, "warmup": 9,
+        "ms_per_step": 1e3 / sat_server["joins_per_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": "PK-FK join requests (phj_radix_bc semantics): 95% sized |R| log-uniform in "
+                               "[2^10, 2^22], |S| = k|R| with k in 1..16, 5% 2^26 x 2^28; relations "
+                               "device-resident", "requests": a.requests, "large_requests": n_big,
+                   "slots": a.slots, "hbm_budget_bytes": budget, "peak_pool_bytes": peak},
+        "saturation": {"server": sat_server, "plain_loop": sat_loops["plain"], "tuned_loop": sat_loops["tuned"],
+                       "speedup_vs_plain_loop": sat_server["joins_per_s"] / sat_loops["plain"]["joins_per_s"],
+                       "speedup_vs_tuned_loop": sat_server["joins_per_s"] / sat_loops["tuned"]["joins_per_s"],
+                       "amdahl_bound_vs_plain_loop": bound},
+        "sweep": [{"offered_rate": lam, "server": s_, "tuned_loop": l_}
+                  for (lam, _, _), s_, l_ in zip(streams, srv_out, loop_out)],
+        "impl_counts": {"nphj": impl_counts[0], "phj": impl_counts[1]},
+    })
     del buf
     return 0
 
@@ -723,17 +776,27 @@ def run_skew_mode(a, rank, world, local_rank):
     ctx = hj.Context(local_rank)
     cases = []
     total_tuples, total_s = 0, 0.0
-    data = [("zipf 0.5", 0.5, 1), ("zipf 1.0", 1.0, 1), ("zipf 1.5", 1.5, 1), ("dup x4", None, 4)]
+    data = [("zipf 0.5", 0.5, 1), ("zipf 1.0", 1.0, 1), ("zipf 1.5", 1.5, 1), ("dup x4", None, 4),
+            ("build hot key", None, 0)]
     for name, theta, dup in data:
         seed = 12345 + 1000 * rank
-        if theta is None:
+        algos = ("phj_radix_lp", "nphj_lp")
+        if name == "build hot key":
+            # Build-side skew: a quarter of R (2^24 tuples) carries one key, so its radix partition holds
+            # 2^24 build tuples; 1% of the probes carry that key (each matches 2^24 build tuples).
+            # Non-partitioned tables cluster equal keys (quadratic build), so only the radix joins run.
+            hj.gen_fast_device(nR, nS, R.data_ptr(), S.data_ptr(), seed=seed, stream=stream.cuda_stream)
+            R[: nR // 4, 0] = 5
+            S[::100, 0] = 5
+            algos = ("phj_radix_bc", "phj_radix_lp")
+        elif theta is None:
             hj.gen_fast_device(nR, nS, R.data_ptr(), S.data_ptr(), seed=seed, dup=dup, stream=stream.cuda_stream)
         else:
             hj.gen_fast_device(nR, 0, R.data_ptr(), S.data_ptr(), seed=seed, stream=stream.cuda_stream)
             hj.gen_zipf_device(nS, nR, theta, S.data_ptr(), seed=seed, stream=stream.cuda_stream)
         torch.cuda.synchronize(dev)
-        for algo in ("phj_radix_lp", "nphj_lp"):
-            want = dense_expected(torch, R, S, lp=True)
+        for algo in algos:
+            want = dense_expected(torch, R, S, lp=algo.endswith("_lp"))
             torch.cuda.synchronize(dev)
 
             def step():
@@ -767,8 +830,10 @@ def run_skew_mode(a, rank, world, local_rank):
         "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": total_s / len(cases) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": "R=2^26, S=2^28 16-B tuples: Zipf FK theta 0.5/1.0/1.5 over unique R keys, and "
-                               "R of 2^24 keys x4 with uniform S; phj_radix_lp (14 bits, 2 passes) and nphj_lp",
+        "config": {"workload": "R=2^26, S=2^28 16-B tuples: Zipf FK theta 0.5/1.0/1.5 over unique R keys, "
+                               "R of 2^24 keys x4 with uniform S (phj_radix_lp, 14 bits / 2 passes, and nphj_lp); "
+                               "and build-side skew: 2^24 of R's tuples on one key, 1% of probes on it "
+                               "(phj_radix_bc and phj_radix_lp)",
                    "value": "all cases' tuples over all cases' time"},
         "cases": cases,
     })
@@ -892,6 +957,12 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
+    if a.mode != "join":
+        global _MODE_SAMPLER
+        import torch
+
+        _MODE_SAMPLER = ClockSampler(device_bus_id(torch, torch.device("cuda", local_rank)))
+        _MODE_SAMPLER.start()
     try:
         if a.mode == "batch":
             return run_batch_mode(a, rank, world, local_rank)

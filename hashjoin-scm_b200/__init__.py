@@ -514,19 +514,21 @@ class Batch:
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double),
                 ("autotune", ctypes.c_int), ("tuner", Tuner), ("small_request_tuples", ctypes.c_double),
-                ("large_sm_share", ctypes.c_double)]
+                ("large_sm_share", ctypes.c_double), ("waves", ctypes.c_int), ("wave_max_requests", ctypes.c_int)]
 
 
 class Completion(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint64), ("matched_cnt", ctypes.c_uint64), ("checksum", ctypes.c_uint64),
                 ("status", ctypes.c_int), ("impl", ctypes.c_int), ("submit_s", ctypes.c_double),
-                ("start_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+                ("start_s", ctypes.c_double), ("done_s", ctypes.c_double), ("wave", ctypes.c_uint64),
+                ("wave_size", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("admitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
                 ("budget_bytes", ctypes.c_double), ("in_use_bytes", ctypes.c_double),
-                ("peak_in_use_bytes", ctypes.c_double), ("queued", ctypes.c_int), ("inflight", ctypes.c_int)]
+                ("peak_in_use_bytes", ctypes.c_double), ("queued", ctypes.c_int), ("inflight", ctypes.c_int),
+                ("waves", ctypes.c_uint64), ("wave_requests", ctypes.c_uint64)]
 
 
 def _bind_server():
@@ -560,11 +562,15 @@ class Server:
     server keeps a reference to them until their completion has been polled."""
 
     def __init__(self, device: int = 0, slots: int = 8, hbm_budget_bytes: float = 150e9, autotune: bool = True,
-                 tuner: dict | None = None, large_sm_share: float | None = None):
+                 tuner: dict | None = None, large_sm_share: float | None = None, waves: bool = True,
+                 wave_max_requests: int | None = None):
         L = _bind_server()
         cfg = ServerConfig()
         L.hj_server_config_init(ctypes.byref(cfg))
         cfg.device, cfg.slots, cfg.hbm_budget_bytes, cfg.autotune = device, slots, hbm_budget_bytes, int(autotune)
+        cfg.waves = int(waves)
+        if wave_max_requests is not None:
+            cfg.wave_max_requests = wave_max_requests
         for k, v in (tuner or {}).items():
             setattr(cfg.tuner, k, v)
         if large_sm_share is not None:

@@ -30,27 +30,11 @@
 #include "hj_ctx.h"
 #include "hj_internal.h"
 #include "hj_nphj.cuh"
+#include "hj_wave.cuh"
 
 namespace hj {
 
 constexpr unsigned long long kMjEmpty = ~0ull;
-
-struct MSide {
-    unsigned long long cnt, sum;  // build tuples whose key is the empty pattern: count, row-id sum
-    unsigned long long notpos;    // max of ~position over them (0 = none), i.e. ~(smallest position)
-    unsigned int dup;             // an equal key was inserted twice
-    unsigned int pad;
-};
-
-struct MJob {
-    const tuple_v *R, *S;
-    unsigned long long nR, nS;
-    tuple_v *table;
-    unsigned long long cap;
-    MSide *side;
-    JoinAccum *acc;
-    unsigned int lp, skip0;
-};
 
 // Largest j with flat[j] <= g (flat[0] = 0, non-decreasing; empty jobs are skipped over).
 __device__ __forceinline__ int mj_find(const unsigned long long *flat, int njobs, unsigned long long g) {
@@ -74,14 +58,6 @@ __device__ __forceinline__ void mj_range(unsigned long long total, unsigned long
     *lo = blockIdx.x * chunk;
     *hi = *lo + chunk < total ? *lo + chunk : total;
 }
-
-// A piece of one job's build or probe side: the multi-join kernels take these as work items, so a
-// block always works on a single job.
-struct MChunk {
-    unsigned int job;
-    unsigned int len;
-    unsigned long long begin;
-};
 
 __device__ __forceinline__ void mj_insert(const MJob &J, const tuple_v t, unsigned long long i) {
     if (J.skip0 && t.x == 0) return;
@@ -254,6 +230,31 @@ __global__ void __launch_bounds__(256, 8) mj_probe(const MJob *__restrict__ jobs
     }
 }
 
+int mj_launch_wave(const WaveDev &w, int num_sms, cudaStream_t st, uint32_t *launches) {
+    if (w.count <= 0) return HJ_OK;
+    if (w.total_t && cudaMemsetAsync(w.tables, 0xff, w.total_t * 16, st) != cudaSuccess) return HJ_E_DEVICE;
+    if (cudaMemsetAsync(w.sides, 0, sizeof(MSide) * w.count, st) != cudaSuccess) return HJ_E_DEVICE;
+    const size_t sm = sizeof(unsigned long long) * (w.count + 1);
+    const int grid = num_sms * 8;
+    uint32_t l = 0;
+    if (w.n_r_chunks) {
+        mj_build<<<w.n_r_chunks < grid ? w.n_r_chunks : grid, 256, 0, st>>>(w.jobs, w.r_chunks, w.n_r_chunks);
+        l++;
+    }
+    if (w.any_lp && w.total_r) {
+        mj_lp_refill<<<grid, 256, sm, st>>>(w.jobs, w.count, w.t_flat, w.total_t);
+        mj_lp_dedup<<<grid, 256, sm, st>>>(w.jobs, w.count, w.r_flat, w.total_r);
+        mj_lp_resolve<<<grid, 256, sm, st>>>(w.jobs, w.count, w.t_flat, w.total_t);
+        l += 3;
+    }
+    if (w.n_s_chunks) {
+        mj_probe<<<w.n_s_chunks < grid ? w.n_s_chunks : grid, 256, 0, st>>>(w.jobs, w.s_chunks, w.n_s_chunks);
+        l++;
+    }
+    if (launches) *launches += l;
+    return cudaGetLastError() == cudaSuccess ? HJ_OK : HJ_E_DEVICE;
+}
+
 }  // namespace hj
 
 using hj::JoinAccum;
@@ -277,7 +278,8 @@ struct Wave {
     bool any_lp;
 };
 
-constexpr unsigned kBuildChunk = 8192, kProbeChunkMJ = 16384;
+using hj::kBuildChunk;
+using hj::kProbeChunkMJ;
 
 void make_chunks(std::vector<hj::MChunk> &out, unsigned job, unsigned long long n, unsigned piece) {
     for (unsigned long long b = 0; b < n; b += piece) {
@@ -294,7 +296,7 @@ size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 bool sem_lp(hj_algo_t a) { return hj::algo_lp(a); }
 bool sem_skip0(hj_algo_t a) { return hj::algo_skip0(a); }
 
-unsigned long long nphj_slots(size_t nR) { return (unsigned long long)((double)nR / 0.5) + 2; }
+unsigned long long nphj_slots(size_t nR) { return hj::mj_slots(nR); }
 
 }  // namespace
 
@@ -387,25 +389,22 @@ int enqueue_batch(hj_batch *b) {
     }
     for (const Wave &w : b->waves) {
         if (w.total_r == 0 && w.total_s == 0) continue;
-        BCU(cudaMemsetAsync(w.tables, 0xff, w.total_t * 16, st));
-        BCU(cudaMemsetAsync(w.sides, 0, sizeof(hj::MSide) * w.count, st));
-        const size_t sm = sizeof(unsigned long long) * (w.count + 1);
-        const int grid = sms * 8;
-        if (w.n_r_chunks) {
-            hj::mj_build<<<std::min(grid, w.n_r_chunks), 256, 0, st>>>(w.jobs_dev, w.r_chunks, w.n_r_chunks);
-            launches++;
-        }
-        if (w.any_lp && w.total_r) {
-            hj::mj_lp_refill<<<grid, 256, sm, st>>>(w.jobs_dev, w.count, w.t_flat, w.total_t);
-            hj::mj_lp_dedup<<<grid, 256, sm, st>>>(w.jobs_dev, w.count, w.r_flat, w.total_r);
-            hj::mj_lp_resolve<<<grid, 256, sm, st>>>(w.jobs_dev, w.count, w.t_flat, w.total_t);
-            launches += 3;
-        }
-        if (w.n_s_chunks) {
-            hj::mj_probe<<<std::min(grid, w.n_s_chunks), 256, 0, st>>>(w.jobs_dev, w.s_chunks, w.n_s_chunks);
-            launches++;
-        }
-        BCU(cudaGetLastError());
+        hj::WaveDev wd;
+        wd.jobs = w.jobs_dev;
+        wd.count = w.count;
+        wd.r_chunks = w.r_chunks;
+        wd.s_chunks = w.s_chunks;
+        wd.n_r_chunks = w.n_r_chunks;
+        wd.n_s_chunks = w.n_s_chunks;
+        wd.r_flat = w.r_flat;
+        wd.t_flat = w.t_flat;
+        wd.total_r = w.total_r;
+        wd.total_t = w.total_t;
+        wd.any_lp = w.any_lp;
+        wd.tables = w.tables;
+        wd.sides = w.sides;
+        const int rc = hj::mj_launch_wave(wd, sms, st, &launches);
+        if (rc) return rc;
     }
     for (int j : b->phj_jobs) {
         const hj_batch_job_t &J = b->jobs[j];

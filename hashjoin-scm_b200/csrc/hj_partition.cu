@@ -76,6 +76,7 @@ enum : int {
     kCtrNItemsA = 2,     // join items whose build side fits the compact shared-memory table (listed first)
     kCtrItemA = 3,       // compact join work-item counter
     kCtrSegAlloc = 4,    // segment mode: segment ids handed out
+    kCtrLargeAgg = 5,    // 1: large partitions use key-aggregated tables (see join_large_build)
     kCtrNItems = 6,
     kCtrNLarge = 7,
     kCtrItem = 8,        // join work-item counter
@@ -335,12 +336,21 @@ struct PlanArgs {
     LargePart *large;
     uint64_t max_large;
     uint64_t large_table_words;
+    int agg_ok;  // joins that need no per-match output may use key-aggregated large-partition tables
 };
 
 __device__ __forceinline__ uint32_t part_to_value(int f, int passes, int b1, int F2) {
     if (passes == 1) return (uint32_t)f;
     const uint32_t d1 = (uint32_t)f / (uint32_t)F2, d2 = (uint32_t)f % (uint32_t)F2;
     return d1 | (d2 << b1);
+}
+
+// u32 words of one large partition's table. Chains: head[nb] then next[r_len]. Key-aggregated:
+// sum[r_len] (u64), head[nb], next[r_len], cnt[r_len], negpos[r_len], rounded to an even count so the
+// next table's sums stay 8-byte aligned.
+__device__ __forceinline__ uint64_t large_words_chain(const LargePart &L) { return (1ull << L.nb_log) + L.r_len; }
+__device__ __forceinline__ uint64_t large_words_agg(const LargePart &L) {
+    return ((1ull << L.nb_log) + 5 * L.r_len + 1) & ~1ull;
 }
 
 // Dynamic shared memory: the relation totals ([2][2^B] u32) when they fit (B <= 14), so that the
@@ -453,13 +463,19 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
     __syncthreads();
     if (tid == 0) {
         const uint64_t nl = large_run < a.max_large ? large_run : a.max_large;
+        // Key-aggregated tables (large_words_agg) when the join allows them and they fit the table
+        // area, else plain chains (large_words_chain).
+        uint64_t need_agg = 0;
+        for (uint64_t l = 0; l < nl; l++) need_agg += large_words_agg(a.large[l]);
+        const bool agg = a.agg_ok && need_agg <= a.large_table_words;
+        a.counters[kCtrLargeAgg] = agg ? 1u : 0u;
         uint64_t off = 0, rf = 0, sf = 0;
         for (uint64_t l = 0; l < nl; l++) {
             LargePart &lp = a.large[l];
             lp.table_off = off;
             lp.r_flat = rf;
             lp.s_flat = sf;
-            off += (1ull << lp.nb_log) + lp.r_len;
+            off += agg ? large_words_agg(lp) : large_words_chain(lp);
             rf += lp.r_len;
             sf += lp.s_len;
         }
@@ -1709,9 +1725,103 @@ __global__ void join_large_clear(JoinArgs a) {
         a.large_table[i] = 0;
 }
 
+// Key-aggregated table of one large partition (see large_words_agg): one chain node per distinct build
+// key, holding the count of its build tuples, the wrapping sum of their row ids and the smallest
+// position among them (as the maximum of ~position). A probe then costs one lookup however many build
+// tuples share its key, where a chain of every build tuple costs a walk over all of them (a hot build
+// key makes that quadratic).
+struct LargeAgg {
+    unsigned long long *sum;
+    uint32_t *head, *next, *cnt, *negpos;
+};
+
+__device__ __forceinline__ LargeAgg large_agg(uint32_t *table, const LargePart &L) {
+    LargeAgg t;
+    uint32_t *base = table + L.table_off;
+    t.sum = reinterpret_cast<unsigned long long *>(base);
+    t.head = base + 2 * L.r_len;
+    t.next = t.head + (1ull << L.nb_log);
+    t.cnt = t.next + L.r_len;
+    t.negpos = t.cnt + L.r_len;
+    return t;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t *p) {
+    return *reinterpret_cast<const volatile uint32_t *>(p);
+}
+
+// The node (index + 1) of key k in bucket h, inserting build tuple i as its node when the key is absent.
+// Lock-free: a node is published by a CAS on the bucket head after its next link is written; a failed
+// CAS means another insert succeeded, and only the nodes it added (above the old head) are re-checked.
+// Returns 0 (and sets the error word) if the walk exceeds the partition's size.
+__device__ __forceinline__ uint32_t large_agg_find_or_insert(const LargeAgg &t, const tuple_v *rr, uint64_t r_len,
+                                                             uint64_t h, uint64_t k, uint32_t i, uint32_t *err) {
+    uint32_t stop = 0;
+    uint32_t e = ld_volatile_u32(&t.head[h]);
+    uint64_t steps = 0;
+    for (;;) {
+        for (uint32_t x = e; x && x != stop; x = ld_volatile_u32(&t.next[x - 1])) {
+            if (rr[x - 1].x == k) return x;
+            if (++steps > r_len) {
+                set_error(err, kErrProbeLimit);
+                return 0;
+            }
+        }
+        *reinterpret_cast<volatile uint32_t *>(&t.next[i]) = e;
+        __threadfence();
+        const uint32_t old = atomicCAS(&t.head[h], e, i + 1);
+        if (old == e) return i + 1;
+        stop = e;
+        e = old;
+        if (++steps > r_len) {
+            set_error(err, kErrProbeLimit);
+            return 0;
+        }
+    }
+}
+
 __global__ void join_large_build(JoinArgs a) {
     const int nl = (int)a.counters[kCtrNLarge];
     const uint64_t total = ld_u64_pair(&a.counters[kCtrLargeR]);
+    if (a.counters[kCtrLargeAgg]) {
+        // Warp-uniform rounds: lanes holding equal keys (equal keys always share a partition) combine
+        // their count, row-id sum and smallest position first, so a hot key costs one update per warp.
+        const unsigned lane = threadIdx.x & 31;
+        for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); g0 < total;
+             g0 += (uint64_t)gridDim.x * blockDim.x) {
+            const uint64_t g = g0 + lane;
+            bool act = g < total;
+            int l = 0;
+            uint64_t i = 0;
+            tuple_v r = make_ulonglong2(0, 0);
+            if (act) {
+                l = find_large(a.large, nl, g, true);
+                i = g - a.large[l].r_flat;
+                r = a.finR[a.large[l].r_begin + i];
+                act = !(a.skip0 && r.x == 0);
+            }
+            const unsigned act_mask = __ballot_sync(0xffffffffu, act);
+            if (!act) continue;
+            const unsigned peers = __match_any_sync(act_mask, r.x);
+            // Row-id sum of the group in three pieces of at most 24 bits (32 addends cannot overflow them).
+            const unsigned s0 = __reduce_add_sync(peers, (unsigned)(r.y & 0xffffffu));
+            const unsigned s1 = __reduce_add_sync(peers, (unsigned)((r.y >> 24) & 0xffffffu));
+            const unsigned s2 = __reduce_add_sync(peers, (unsigned)(r.y >> 48));
+            const unsigned minpos = __reduce_min_sync(peers, (unsigned)i);
+            if ((int)lane != __ffs(peers) - 1) continue;
+            const LargePart &L = a.large[l];
+            const LargeAgg t = large_agg(a.large_table, L);
+            const uint64_t h = (r.x >> a.bits) & ((1ull << L.nb_log) - 1);
+            const uint32_t node = large_agg_find_or_insert(t, a.finR + L.r_begin, L.r_len, h, r.x, (uint32_t)i,
+                                                           &a.counters[kCtrErr]);
+            if (!node) continue;
+            atomicAdd(&t.cnt[node - 1], (uint32_t)__popc(peers));
+            atomicAdd(&t.sum[node - 1], (unsigned long long)s0 + ((unsigned long long)s1 << 24) +
+                                            ((unsigned long long)s2 << 48));
+            atomicMax(&t.negpos[node - 1], ~minpos);
+        }
+        return;
+    }
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const int l = find_large(a.large, nl, g, true);
@@ -1775,6 +1885,38 @@ __global__ void join_large_probe(JoinArgs a) {
                     for (uint32_t e = e0; e && steps++ <= Lp->r_len; e = nxt[e - 1])
                         if (rr[e - 1].x == s.x) mat_put(a.mat, o++, rr[e - 1].y, s.y, err);
                 }
+            }
+        }
+    } else if (a.counters[kCtrLargeAgg]) {
+        for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
+             g += (uint64_t)gridDim.x * blockDim.x) {
+            const int l = find_large(a.large, nl, g, false);
+            const LargePart &L = a.large[l];
+            const tuple_v s = ld_stream(a.finS + L.s_begin + (g - L.s_flat));
+            const LargeAgg t = large_agg(a.large_table, L);
+            const tuple_v *rr = a.finR + L.r_begin;
+            uint32_t e = t.head[(s.x >> a.bits) & ((1ull << L.nb_log) - 1)];
+            uint64_t steps = 0;
+            while (e && rr[e - 1].x != s.x) {
+                e = t.next[e - 1];
+                if (++steps > L.r_len) {
+                    set_error(&a.counters[kCtrErr], kErrProbeLimit);
+                    e = 0;
+                }
+            }
+            if (!e) continue;
+            if (a.lp) {
+                const uint32_t first = ~t.negpos[e - 1];
+                if (first < L.r_len) {
+                    cnt++;
+                    sum += rr[first].y + s.y;
+                } else {
+                    set_error(&a.counters[kCtrErr], kErrBounds);
+                }
+            } else {
+                const unsigned long long c = t.cnt[e - 1];
+                cnt += c;
+                sum += t.sum[e - 1] + c * s.y;
             }
         }
     } else
@@ -1932,9 +2074,10 @@ static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms,
     z.tmp2 = g.passes == 2 ? align_up((nR + nS) * 16, 256) : 0;
     z.seg_head = seg ? align_up((size_t)2 * z.seg_grid * g.F1 * 4, 256) : 0;
     z.seg_next = seg ? align_up((size_t)z.max_segs * 4, 256) : 0;
-    // Large-partition chains: head <= 2*|R_p| words, next = |R_p| words. With two passes they reuse
-    // the pass-1 buffer, which is dead once pass 2 has run.
-    z.large_table_words = 3 * nR + 2;
+    // Large-partition tables: chains take head <= 2*|R_p| words and next = |R_p| words; key-aggregated
+    // tables another 4*|R_p| words plus one word of alignment each. With two passes they reuse the
+    // pass-1 buffer, which is dead once pass 2 has run (tables that do not fit it fall back to chains).
+    z.large_table_words = 7 * nR + 2 * z.max_large + 2;
     z.large_table = g.passes == 2 ? 0 : align_up(z.large_table_words * 4, 256);
     return z;
 }
@@ -2118,6 +2261,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     pa.large = reinterpret_cast<LargePart *>(s.large);
     pa.max_large = s.max_large;
     pa.large_table_words = s.large_table_words;
+    pa.agg_ok = mat ? 0 : 1;
     plan_kernel<<<1, 1024, g.bits <= kPlanStageBits ? (size_t)2 * np * 4 : 0, st>>>(pa);
     {
         const int ut = F1 < 32 ? 32 : F1;

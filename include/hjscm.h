@@ -352,6 +352,12 @@ int hj_nphj_join_noalloc(hj_algo_t algo, const hj_tuple_t *R_dev, size_t nR, con
  *   - Each request runs the implementation the autotuner picks for its sizes (or, with autotune = 0,
  *     the named algorithm at 14 radix bits / 2 passes) with the named algorithm's result semantics, so
  *     its result is the same as hj_join's, alone or in any mix.
+ *   - Continuous batching (waves = 1, the default): requests that run as non-partitioned joins are not
+ *     given slots of their own. At each dispatch, the ones queued (up to wave_max_requests, their
+ *     tables within the tuner's wave_table_bytes) are coalesced into one wave - one multi-join build
+ *     and one multi-join probe launch over all of them, on a high-priority stream - whose memory is one
+ *     block of the pool. Two waves can be on the GPU at once; requests that arrive while they run form
+ *     the next wave. Partitioned (large) requests keep their slots and overlap the waves.
  * -------------------------------------------------------------------------------------------- */
 typedef struct {
     int device;
@@ -362,6 +368,9 @@ typedef struct {
     double small_request_tuples; /* requests with |R| + |S| <= this run on high-priority streams */
     double large_sm_share;       /* larger requests launch their kernels sized for this share of the SMs
                                     (0..1], leaving room for small requests' blocks; 1 = all SMs */
+    int waves;                   /* 1: coalesce non-partitioned requests into waves (default); 0: one slot
+                                    per request */
+    int wave_max_requests;       /* requests per wave (1..1024; default 512) */
 } hj_server_config_t;
 
 typedef struct {
@@ -371,12 +380,16 @@ typedef struct {
     int status;                  /* HJ_OK or an HJ_E_* code */
     int impl;                    /* 0 = non-partitioned table, 1 = radix-partitioned */
     double submit_s, start_s, done_s; /* hj_now() clock: submission, admission, completion seen */
+    uint64_t wave;               /* 0: ran on a slot of its own; else the id (1, 2, ...) of its wave */
+    int wave_size;               /* requests in that wave */
+    int reserved;
 } hj_server_completion_t;
 
 typedef struct {
     uint64_t submitted, admitted, completed;
     double budget_bytes, in_use_bytes, peak_in_use_bytes;
-    int queued, inflight;
+    int queued, inflight;        /* inflight: requests on slots and in waves */
+    uint64_t waves, wave_requests; /* waves launched and the requests they carried */
 } hj_server_stats_t;
 
 typedef struct hj_server hj_server_t;
@@ -384,7 +397,7 @@ typedef struct hj_server hj_server_t;
 /* Monotonic clock in seconds, the one completions are stamped with. */
 double hj_now(void);
 /* Defaults: device 0, 8 slots, 150e9 bytes, autotune, small requests up to 2^25 tuples, large requests
- * on 0.75 of the SMs. */
+ * on 0.75 of the SMs, waves of up to 512 requests. */
 int hj_server_config_init(hj_server_config_t *cfg);
 int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out);
 int hj_server_submit(hj_server_t *srv, hj_algo_t algo, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,

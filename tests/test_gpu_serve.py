@@ -30,14 +30,18 @@ def _requests(seed, n, max_log=18):
     return out
 
 
-@pytest.mark.parametrize("slots,tuner", [(8, None), (3, {"nphj_max_table_bytes": 1e6, "partition_target": 512,
-                                                          "wave_table_bytes": 64e6}), (1, None)])
-def test_server_mix_matches_alone(hj, oracle, cuda, slots, tuner):
+@pytest.mark.parametrize("slots,tuner,waves", [
+    (8, None, True),
+    (3, {"nphj_max_table_bytes": 1e6, "partition_target": 512, "wave_table_bytes": 64e6}, True),
+    (1, None, True),
+    (8, None, False),
+    (2, {"nphj_max_table_bytes": 1e6, "partition_target": 512, "wave_table_bytes": 4e6}, True)])
+def test_server_mix_matches_alone(hj, oracle, cuda, slots, tuner, waves):
     reqs = _requests(11 + slots, 48)
     alone = [hj.join(a, R, S) for a, R, S in reqs]
     dev = [(cuda.from_numpy(R.view(np.int64)).cuda(), cuda.from_numpy(S.view(np.int64)).cuda())
            for _, R, S in reqs]
-    with hj.Server(0, slots=slots, hbm_budget_bytes=2e9, tuner=tuner) as srv:
+    with hj.Server(0, slots=slots, hbm_budget_bytes=2e9, tuner=tuner, waves=waves) as srv:
         ids = {}
         for rep in range(2):
             for i, (a, R, S) in enumerate(reqs):
@@ -56,11 +60,57 @@ def test_server_mix_matches_alone(hj, oracle, cuda, slots, tuner):
             assert (c.matched_cnt, c.checksum) == oracle.join(a, R, S)
             assert c.submit_s <= c.start_s <= c.done_s
             impls.add(c.impl)
+            if waves and c.impl == 0 and R.shape[0] and S.shape[0]:
+                assert c.wave > 0 and c.wave_size >= 1  # non-partitioned requests run in waves
+            else:
+                assert c.wave == 0
         st = srv.stats()
         assert st.completed == st.submitted == 2 * len(reqs)
         assert st.in_use_bytes == 0 and st.queued == 0 and st.inflight == 0
+        if waves:
+            assert st.waves > 0 and st.wave_requests == sum(1 for c in got.values() if c.wave)
     if tuner:
         assert impls == {0, 1}
+
+
+def test_server_waves_coalesce_a_burst(hj, oracle, cuda):
+    """A burst of small requests submitted at once is served in a few waves of many requests each, and
+    every result equals the same join alone and the oracle, whichever wave carried it."""
+    reqs = _requests(97, 300, max_log=12)
+    dev = [(cuda.from_numpy(R.view(np.int64)).cuda(), cuda.from_numpy(S.view(np.int64)).cuda())
+           for _, R, S in reqs]
+    with hj.Server(0, slots=4, hbm_budget_bytes=4e9, wave_max_requests=128) as srv:
+        ids = {srv.submit(a, dev[i][0], dev[i][1], on_device=True): i for i, (a, R, S) in enumerate(reqs)}
+        got = srv.wait_all(ids.keys())
+        sizes = {}
+        for rid, c in got.items():
+            a, R, S = reqs[ids[rid]]
+            assert c.status == 0
+            assert (c.matched_cnt, c.checksum) == oracle.join(a, R, S), (a, R.shape, S.shape, c.wave)
+            if c.wave:
+                sizes[c.wave] = c.wave_size
+        st = srv.stats()
+    assert max(sizes.values()) > 1                      # requests were coalesced
+    assert max(sizes.values()) <= 128                   # within the configured wave size
+    assert st.waves == len(sizes) < st.wave_requests    # fewer waves than requests
+    assert st.in_use_bytes == 0
+
+
+def test_server_wave_shrinks_under_memory_pressure(hj, cuda):
+    """With a pool that holds only a few requests' tables, waves shrink to what fits and every request
+    is still served exactly (no wave waits forever for a block larger than the pool)."""
+    nR, nS = 1 << 16, 1 << 18
+    R, S = hj.gen_fast_host(nR, nS, seed=9)
+    Rd = cuda.from_numpy(R.view(np.int64)).cuda()
+    Sd = cuda.from_numpy(S.view(np.int64)).cuda()
+    want = hj.pkfk_closed_form(nR, nS)
+    with hj.Server(0, slots=2, hbm_budget_bytes=8e6) as srv:  # ~2.1 MB per request's table
+        ids = [srv.submit("nphj_sc", Rd, Sd, on_device=True) for _ in range(40)]
+        got = srv.wait_all(ids)
+        assert all((c.status, c.matched_cnt, c.checksum) == (0, *want) for c in got.values())
+        st = srv.stats()
+        assert 0 < st.peak_in_use_bytes <= st.budget_bytes
+        assert st.wave_requests == 40 and st.in_use_bytes == 0
 
 
 def test_server_budget_admission(hj, cuda):
