@@ -124,6 +124,9 @@ inline bool phj_phase_span(bool seg_mode, int i, int *from, int *to) {
 // Non-partitioned joins on a global open-addressing table.
 // mat: as for phj_enqueue; a materialising join needs nphj_scratch_bytes(nR, load, true).
 size_t nphj_scratch_bytes(size_t nR, double load, bool mat = false);
+// Shared-memory attributes of the non-partitioned join's kernels on the current device (idempotent;
+// call before capturing nphj_enqueue in a graph).
+int nphj_prepare_device();
 int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                  int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr);

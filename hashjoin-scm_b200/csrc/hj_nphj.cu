@@ -18,11 +18,21 @@
 // key equals the EMPTY pattern are kept in a side record instead of the table.
 //
 // Compact slots (nphj_sc): when every build key is below 2^32 - 1 and every build row id below 2^32
-// (a first pass over R finds out), a slot is one 8-byte word (key << 32 | row id), claimed whole by one
-// 64-bit CAS. The table then takes half the bytes (64 MB for |R| = 2^22, where L2 holds it), a build
-// claim needs no second store, and a probe reads 8 bytes. Used when the 16-byte table would exceed
-// 64 MB.
+// (a first pass over R finds out), a slot is one 8-byte word (key << 32 | row id). The table then takes
+// half the bytes (64 MB for |R| = 2^22, where L2 holds it) and a probe reads 8 bytes. Used when the
+// 16-byte table would exceed 64 MB.
+//
+// Sliced build of a compact table: the table is cut into slices of kSliceSlots slots and a key's
+// probe sequence wraps around inside its slice. The first pass over R also counts the build tuples of
+// every slice per block of R; a column scan turns the counts into each block's output offsets; the
+// build tuples are scattered by slice into a staging array as compact words; then one CTA per slice
+// builds that slice's table in shared memory (shared-memory CAS) and writes it out whole. The build then
+// makes no global atomics: claiming random global slots one CAS at a time is bound by the L2 atomic
+// rate (about 20 G claims per second here), well below the bandwidth of the passes that replace it. If
+// any slice would be filled above 7/8, the table is built by global CAS instead (the probe follows the
+// mode the build used).
 #include <cstdio>
+#include <mutex>
 
 #include "hj_common.cuh"
 #include "hj_internal.h"
@@ -40,10 +50,18 @@ struct NphjSide {
     unsigned int err;
     unsigned long long kmax;     // largest build key (compact-slot test)
     unsigned long long ror;      // OR of all build row ids
+    unsigned int sliced;         // the compact table is built (and probed) slice by slice
+    unsigned int pad;
 };
 
 constexpr unsigned long long kCompactEmpty = ~0ull;
 constexpr unsigned long long kCompactMinTableBytes = 64ull << 20;
+
+constexpr int kSliceLog = 13;
+constexpr unsigned kSliceSlots = 1u << kSliceLog;        // 64 KB of compact slots per slice
+constexpr unsigned kSliceMaxFill = kSliceSlots / 8 * 7;  // fuller slices: global-CAS build instead
+constexpr unsigned kSliceMaxCount = 40960;              // slices the per-block histograms hold in shared memory
+constexpr int kSliceThreads = 512;
 
 // Every build key below 2^32 - 1 (so no slot can equal the empty pattern) and every row id below 2^32.
 __device__ __forceinline__ bool nphj_compact(const NphjSide *side) {
@@ -63,25 +81,62 @@ struct NphjArgs {
     unsigned long long *side_pos;  // materialising joins: input positions of the side record's tuples
     MatOut mat;
     int compact_ok;  // the algorithm may use compact slots (nphj_sc, not materialising)
+    // Compact tables: capacity (a multiple of kSliceSlots) and the sliced build's buffers.
+    unsigned long long ccap;
+    unsigned int nslices;      // ccap / kSliceSlots; 0: no sliced build
+    unsigned int hist_blocks;  // blocks of the counting and scatter passes (each a contiguous range of R)
+    unsigned long long *stage; // [nR] build tuples as compact words, ordered by slice
+    uint32_t *slice_hist;      // [hist_blocks][nslices] build tuples per (block, slice)
+    uint32_t *slice_off;       // [hist_blocks][nslices] the block's offset inside the slice
+    uint32_t *slice_start;     // [nslices + 1] first staging index of each slice
 };
 
-// Largest build key and OR of build row ids, for the compact-slot test.
-__global__ void nphj_widths(NphjArgs a) {
+__device__ __forceinline__ bool compact_sliced(const NphjSide *side) {
+    return *reinterpret_cast<const volatile unsigned int *>(&side->sliced) != 0;
+}
+
+__device__ __forceinline__ unsigned slice_of(unsigned long long key, unsigned long long ccap) {
+    return (unsigned)(table_hash(key, ccap) >> kSliceLog);
+}
+
+// Next slot of a compact table's probe sequence: inside the slice when the table was built by slices.
+__device__ __forceinline__ unsigned long long compact_next(unsigned long long h, bool sliced, unsigned long long ccap) {
+    if (sliced) return (h & ~(unsigned long long)(kSliceSlots - 1)) | ((h + 1) & (kSliceSlots - 1));
+    return h + 1 == ccap ? 0 : h + 1;
+}
+
+__device__ __forceinline__ void block_range(unsigned long long n, unsigned long long *lo, unsigned long long *hi) {
+    const unsigned long long per = (n + gridDim.x - 1) / gridDim.x;
+    *lo = blockIdx.x * per < n ? blockIdx.x * per : n;
+    *hi = *lo + per < n ? *lo + per : n;
+}
+
+// Largest build key and OR of build row ids (the compact-slot test) and, when the table may be built
+// by slices, the build tuples of every slice in this block's contiguous range of R.
+__global__ void __launch_bounds__(kSliceThreads) nphj_widths(NphjArgs a) {
+    extern __shared__ uint32_t sh_cnt[];  // [nslices]
+    const bool count = a.nslices != 0;
+    if (count) {
+        for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) sh_cnt[j] = 0;
+        __syncthreads();
+    }
+    unsigned long long lo, hi;
+    block_range(a.nR, &lo, &hi);
     unsigned long long kmax = 0, ror = 0;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     constexpr int U = 4;
-    for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < a.nR;
-         i0 += U * stride) {
+    for (unsigned long long i0 = lo + threadIdx.x; i0 < hi; i0 += U * blockDim.x) {
         tuple_v t[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const unsigned long long i = i0 + u * stride;
-            t[u] = i < a.nR ? ld_stream(a.R + i) : make_ulonglong2(0, 0);
+            const unsigned long long i = i0 + u * blockDim.x;
+            t[u] = i < hi ? ld_stream(a.R + i) : make_ulonglong2(0, 0);
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
             kmax = max(kmax, t[u].x);
             ror |= t[u].y;
+            if (count && i0 + u * blockDim.x < hi && t[u].x < 0xffffffffull)
+                atomicAdd(&sh_cnt[slice_of(t[u].x, a.ccap)], 1u);
         }
     }
 #pragma unroll
@@ -93,19 +148,182 @@ __global__ void nphj_widths(NphjArgs a) {
         atomicMax(&a.side->kmax, kmax);
         atomicOr(&a.side->ror, ror);
     }
+    if (count) {
+        __syncthreads();
+        uint32_t *row = a.slice_hist + (size_t)blockIdx.x * a.nslices;
+        for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) row[j] = sh_cnt[j];
+    }
 }
 
-// Compact build: the CAS writes key and row id together.
+// Per slice, the offset of every block's tuples inside the slice (an exclusive scan down the column
+// of the histogram) and the slice's total. 32 slices per CTA; warp w sums a contiguous run of rows.
+__global__ void __launch_bounds__(1024) nphj_slice_colscan(NphjArgs a, uint32_t *total) {
+    __shared__ uint32_t part[32][33];
+    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned sidx = blockIdx.x * 32 + lane;
+    const bool valid = sidx < a.nslices;
+    const unsigned rpw = (a.hist_blocks + 31) / 32;
+    const unsigned r0 = w * rpw, r1 = min(a.hist_blocks, r0 + rpw);
+    uint32_t sum = 0;
+    for (unsigned r = r0; r < r1 && valid; r++) sum += a.slice_hist[(size_t)r * a.nslices + sidx];
+    part[w][lane] = sum;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t run = 0;
+        for (int q = 0; q < 32; q++) {
+            const uint32_t v = part[q][lane];
+            part[q][lane] = run;
+            run += v;
+        }
+        if (valid) total[sidx] = run;
+    }
+    __syncthreads();
+    uint32_t run = part[w][lane];
+    for (unsigned r = r0; r < r1 && valid; r++) {
+        const size_t q = (size_t)r * a.nslices + sidx;
+        const uint32_t v = a.slice_hist[q];
+        a.slice_off[q] = run;
+        run += v;
+    }
+}
+
+// One CTA: the first staging index of every slice, and the mode of the build: sliced when the table
+// is compact and no slice is filled above kSliceMaxFill.
+__global__ void __launch_bounds__(1024) nphj_slice_plan(NphjArgs a, const uint32_t *total) {
+    __shared__ uint32_t scan_tmp[32];
+    __shared__ uint32_t s_max;
+    const unsigned n = a.nslices;
+    const unsigned per = (n + blockDim.x - 1) / blockDim.x;
+    const unsigned j0 = min(n, threadIdx.x * per), j1 = min(n, j0 + per);
+    uint32_t sum = 0, mx = 0;
+    for (unsigned j = j0; j < j1; j++) {
+        sum += total[j];
+        mx = max(mx, total[j]);
+    }
+    if (threadIdx.x == 0) s_max = 0;
+    __syncthreads();
+    atomicMax(&s_max, mx);
+    // Block-wide exclusive scan of the per-thread sums.
+    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += v;
+    }
+    if (lane == 31) scan_tmp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t v = lane < blockDim.x / 32 ? scan_tmp[lane] : 0;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= (unsigned)o) x += y;
+        }
+        scan_tmp[lane] = x - v;
+    }
+    __syncthreads();
+    uint32_t run = scan_tmp[w] + incl - sum;
+    for (unsigned j = j0; j < j1; j++) {
+        a.slice_start[j] = run;
+        run += total[j];
+    }
+    if (threadIdx.x == blockDim.x - 1) a.slice_start[n] = run;
+    if (threadIdx.x == 0) {
+        const bool compact = nphj_compact(a.side);
+        a.side->sliced = (compact && s_max <= kSliceMaxFill) ? 1u : 0u;
+    }
+}
+
+// Empties the table the build will claim slots in: the 16-byte table when the keys or row ids are too
+// wide for compact slots, the compact table when it is built by global CAS. A table built by slices
+// is written whole by nphj_slice_build.
+__global__ void nphj_clear_table(NphjArgs a) {
+    const bool compact = nphj_compact(a.side);
+    if (compact && compact_sliced(a.side)) return;
+    const unsigned long long words16 = compact ? a.ccap / 2 : a.cap;  // 16-byte units
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < words16;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        a.table[i] = make_ulonglong2(kEmpty, kEmpty);
+}
+
+// Build tuples in slice order as compact words (key << 32 | row id); block b writes its tuples of
+// slice s from start[s] + off[b][s] on, ranked by shared-memory counters.
+__global__ void __launch_bounds__(kSliceThreads) nphj_slice_scatter(NphjArgs a) {
+    extern __shared__ uint32_t sh_pos[];  // [nslices]
+    if (!compact_sliced(a.side)) return;
+    const uint32_t *off = a.slice_off + (size_t)blockIdx.x * a.nslices;
+    for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) sh_pos[j] = a.slice_start[j] + off[j];
+    __syncthreads();
+    unsigned long long lo, hi;
+    block_range(a.nR, &lo, &hi);
+    constexpr int U = 4;
+    for (unsigned long long i0 = lo + threadIdx.x; i0 < hi; i0 += U * blockDim.x) {
+        tuple_v t[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned long long i = i0 + u * blockDim.x;
+            t[u] = i < hi ? ld_stream(a.R + i) : make_ulonglong2(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (i0 + u * blockDim.x >= hi) continue;
+            const uint32_t pos = atomicAdd(&sh_pos[slice_of(t[u].x, a.ccap)], 1u);
+            if (pos < a.nR)
+                a.stage[pos] = (t[u].x << 32) | t[u].y;
+            else
+                set_error(&a.acc->error, kErrBounds);
+        }
+    }
+}
+
+// One slice at a time per CTA: its build tuples claim slots of a shared-memory table by CAS, probing
+// inside the slice; then the whole slice, empty slots included, is written to the global table.
+__global__ void __launch_bounds__(kSliceThreads) nphj_slice_build(NphjArgs a) {
+    extern __shared__ unsigned long long tab[];  // [kSliceSlots]
+    if (!compact_sliced(a.side)) return;
+    bool seen_dup = false;
+    unsigned long long *ctab = reinterpret_cast<unsigned long long *>(a.table);
+    for (unsigned sl = blockIdx.x; sl < a.nslices; sl += gridDim.x) {
+        for (unsigned j = threadIdx.x; j < kSliceSlots; j += blockDim.x) tab[j] = kCompactEmpty;
+        __syncthreads();
+        const uint32_t lo = a.slice_start[sl], n = a.slice_start[sl + 1] - lo;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long v = a.stage[lo + i];
+            const unsigned long long k = v >> 32;
+            unsigned h = (unsigned)table_hash(k, a.ccap) & (kSliceSlots - 1);
+            for (unsigned steps = 0;;) {
+                const unsigned long long cur = atomicCAS(&tab[h], kCompactEmpty, v);
+                if (cur == kCompactEmpty) break;
+                if ((cur >> 32) == k) seen_dup = true;
+                h = (h + 1) & (kSliceSlots - 1);
+                if (++steps >= kSliceSlots) {
+                    set_error(&a.acc->error, kErrProbeLimit);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(ctab + (size_t)sl * kSliceSlots);
+        const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(tab);
+        for (unsigned j = threadIdx.x; j < kSliceSlots / 2; j += blockDim.x) dst[j] = src[j];
+        __syncthreads();
+    }
+    if (__syncthreads_or(seen_dup) && threadIdx.x == 0) atomicOr(&a.side->dup, 1u);
+}
+
+// Compact build by global CAS (the table was not built by slices): the CAS writes key and row id together.
 __device__ __forceinline__ void nphj_insert_compact(const NphjArgs &a, unsigned long long *ctab, const tuple_v t,
                                                     bool &seen_dup) {
     const unsigned long long v = (t.x << 32) | t.y;
-    unsigned long long h = table_hash(t.x, a.cap);
+    unsigned long long h = table_hash(t.x, a.ccap);
     for (unsigned long long steps = 0;;) {
         const unsigned long long cur = atomicCAS(ctab + h, kCompactEmpty, v);
         if (cur == kCompactEmpty) return;
         if ((cur >> 32) == t.x) seen_dup = true;
-        if (++h == a.cap) h = 0;
-        if (++steps >= a.cap) {
+        if (++h == a.ccap) h = 0;
+        if (++steps >= a.ccap) {
             set_error(&a.acc->error, kErrProbeLimit);
             return;
         }
@@ -149,6 +367,7 @@ __global__ void nphj_build(NphjArgs a) {
     bool seen_dup = false;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     if (a.compact_ok && nphj_compact(a.side)) {
+        if (compact_sliced(a.side)) return;  // nphj_slice_build built the table
         unsigned long long *ctab = reinterpret_cast<unsigned long long *>(a.table);
         for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < a.nR;
              i0 += U * stride) {
@@ -239,6 +458,8 @@ __global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
     constexpr int V = 4;
     const unsigned long long *ctab = reinterpret_cast<const unsigned long long *>(a.table);
     const bool first_only = *reinterpret_cast<volatile unsigned int *>(&a.side->dup) == 0;
+    const bool sliced = compact_sliced(a.side);
+    const unsigned long long max_steps = sliced ? kSliceSlots : a.ccap;
     unsigned long long cnt = 0, sum = 0;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     for (unsigned long long j0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j0 < a.nS;
@@ -255,7 +476,7 @@ __global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
 #pragma unroll
         for (int u = 0; u < V; u++) {
             if (walk[u]) {
-                h[u] = table_hash(sv[u].x, a.cap);
+                h[u] = table_hash(sv[u].x, a.ccap);
                 e[u] = ld_slot8(ctab + h[u]);
             }
         }
@@ -270,8 +491,8 @@ __global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
                     sum += (ee & 0xffffffffull) + sv[u].y;
                     if (first_only) break;
                 }
-                if (++hh == a.cap) hh = 0;
-                if (++steps >= a.cap) {
+                hh = compact_next(hh, sliced, a.ccap);
+                if (++steps >= max_steps) {
                     set_error(&a.acc->error, kErrProbeLimit);
                     break;
                 }
@@ -427,6 +648,24 @@ size_t nphj_scratch_bytes(size_t nR, double load, bool mat) {
         }                                                                             \
     } while (0)
 
+static std::mutex g_nphj_attr_mu;
+static bool g_nphj_attr_done[64];
+
+// Shared-memory limits of the sliced build's kernels, once per device.
+int nphj_prepare_device() {
+    int dev = 0;
+    HJ_CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return HJ_E_INVAL;
+    std::lock_guard<std::mutex> lk(g_nphj_attr_mu);
+    if (g_nphj_attr_done[dev]) return HJ_OK;
+    HJ_CU(cudaFuncSetAttribute(nphj_widths, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kSliceMaxCount * 4)));
+    HJ_CU(cudaFuncSetAttribute(nphj_slice_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(kSliceMaxCount * 4)));
+    HJ_CU(cudaFuncSetAttribute(nphj_slice_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kSliceSlots * 8)));
+    g_nphj_attr_done[dev] = true;
+    return HJ_OK;
+}
+
 int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                  int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat) {
@@ -449,14 +688,61 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     // Compact slots pay off once the 16-byte table outgrows a share of L2; below that the extra pass
     // over R costs more than it saves.
     a.compact_ok = (!lp && !mat && cap * 16 > kCompactMinTableBytes) ? 1 : 0;
-    HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
+    // Compact table: capacity rounded up to whole slices; behind it (inside the 16-byte table's bytes)
+    // the sliced build's staging array, histograms and slice starts.
+    a.ccap = (cap + kSliceSlots - 1) / kSliceSlots * kSliceSlots;
+    a.nslices = 0;
+    a.hist_blocks = (unsigned)num_sms * 2;
+    a.stage = nullptr;
+    a.slice_hist = a.slice_off = a.slice_start = nullptr;
+    uint32_t *slice_total = nullptr;
+    if (a.compact_ok) {
+        const unsigned long long ns = a.ccap / kSliceSlots;
+        char *p = reinterpret_cast<char *>(table) + ((a.ccap * 8 + 255) & ~255ull);
+        char *const end = reinterpret_cast<char *>(table) + cap * 16;
+        char *q = p + ((nR * 8 + 255) & ~255ull);
+        const size_t hist_bytes = ((size_t)a.hist_blocks * ns * 4 + 255) & ~(size_t)255;
+        char *q_end = q + 2 * hist_bytes + 2 * (((ns + 1) * 4 + 255) & ~(size_t)255);
+        if (ns <= kSliceMaxCount && q_end <= end) {
+            a.nslices = (unsigned)ns;
+            a.stage = reinterpret_cast<unsigned long long *>(p);
+            a.slice_hist = reinterpret_cast<uint32_t *>(q);
+            a.slice_off = reinterpret_cast<uint32_t *>(q + hist_bytes);
+            a.slice_start = reinterpret_cast<uint32_t *>(q + 2 * hist_bytes);
+            slice_total = reinterpret_cast<uint32_t *>(q + 2 * hist_bytes + (((ns + 1) * 4 + 255) & ~(size_t)255));
+        }
+    }
+    if (a.compact_ok) {
+        const int rc = nphj_prepare_device();
+        if (rc) return rc;
+    }
+    if (!a.compact_ok) HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
     HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
     HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));
     const int grid = num_sms * 8;
+    uint32_t nl = 0;
     // Phase slots: build spans [0, 1], probe spans [4, 5]; the others stay empty.
     if (ph) HJ_CU(cudaEventRecord(ph[0], st));
-    if (a.compact_ok) nphj_widths<<<grid, 256, 0, st>>>(a);
+    if (a.compact_ok) {
+        const size_t hist_smem = (size_t)a.nslices * 4;
+        nphj_widths<<<a.hist_blocks, kSliceThreads, hist_smem, st>>>(a);
+        nl++;
+        if (a.nslices) {
+            nphj_slice_colscan<<<(a.nslices + 31) / 32, 1024, 0, st>>>(a, slice_total);
+            nphj_slice_plan<<<1, 1024, 0, st>>>(a, slice_total);
+            nl += 2;
+        }
+        nphj_clear_table<<<grid, 256, 0, st>>>(a);
+        nl++;
+        if (a.nslices) {
+            nphj_slice_scatter<<<a.hist_blocks, kSliceThreads, hist_smem, st>>>(a);
+            const unsigned bgrid = a.nslices < (unsigned)num_sms * 3 ? a.nslices : (unsigned)num_sms * 3;
+            nphj_slice_build<<<bgrid, kSliceThreads, kSliceSlots * 8, st>>>(a);
+            nl += 2;
+        }
+    }
     nphj_build<<<grid, 256, 0, st>>>(a);
+    nl++;
     if (lp) {
         nphj_lp_refill<<<grid, 256, 0, st>>>(a);
         nphj_lp_dedup_build<<<grid, 256, 0, st>>>(a);
@@ -478,7 +764,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         HJ_CU(cudaEventRecord(ph[5], st));
         HJ_CU(cudaEventRecord(ph[6], st));
     }
-    if (launches) *launches = lp ? 5u : a.compact_ok ? 4u : 2u;
+    if (launches) *launches = lp ? 5u : nl + (a.compact_ok ? 2u : 1u);
     return HJ_OK;
 }
 

@@ -86,7 +86,9 @@ enum : int {
     kCtrErr = 15,
     kCtrMaxKey = 16,     // u64: OR of all R keys (words 16-17)
     kCtrMaxRid = 18,     // u64: OR of all R row ids (words 18-19)
-    kNumCounters = 20
+    kCtrItem1S = 20,     // first-match joins: pass-1 work-item counter of the probe relation's items
+    kCtrItem2S = 21,     // first-match joins: pass-2 work-item counter of the probe relation's items
+    kNumCounters = 22
 };
 
 // Build partitions up to this size whose keys (above the radix bits) and row ids fit 32 bits are
@@ -577,6 +579,9 @@ struct ScatterArgs {
     int test_stall;             // test hook: CTA 0 withholds its first tile load (its wait must expire)
     uint32_t *counters;
     int ctr_item;
+    // Work items of this launch: [item_base, item_end) of the pass's items (R's first, then S's), claimed
+    // through counters[ctr_item]; item_end 0 = all of them.
+    uint32_t item_base, item_end;
 };
 
 // A tile claimed for processing: its source, length, output region and owning work item.
@@ -665,7 +670,7 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
     for (;;) {
         while (it.item == ~0u || it.done >= it.len) {
             if (ah.stage == 0) {
-                ah.item = atomicAdd(&a.counters[a.ctr_item], 1u);
+                ah.item = a.item_base + atomicAdd(&a.counters[a.ctr_item], 1u);
                 ah.stage = 1;
             }
             if (ah.stage == 1) item_fetch(a, ah, nitems);
@@ -688,7 +693,7 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
             // one is done. (Pass-1 items are long, and an item held back per CTA lengthens the tail
             // by more than the claim costs.)
             if (a.pass != 0) {
-                ah.item = atomicAdd(&a.counters[a.ctr_item], 1u);
+                ah.item = a.item_base + atomicAdd(&a.counters[a.ctr_item], 1u);
                 ah.stage = 1;
             }
             item_decode(a, cur.item, cur, it);
@@ -736,7 +741,8 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     const int F = a.F;
     const uint64_t dmask = (uint64_t)F - 1;
     const uint32_t nchunks = a.cg.cR + a.cg.cS;
-    const uint32_t nitems = a.pass == 0 ? nchunks * a.cg.spc : nchunks * (uint32_t)a.F1;
+    const uint32_t nitems =
+        a.item_end ? a.item_end : (a.pass == 0 ? nchunks * a.cg.spc : nchunks * (uint32_t)a.F1);
     unsigned int *err = &a.counters[kCtrErr];
     const unsigned ltmask = lanemask_lt();
     const uint32_t bar0 = smem_addr(&bars[0]);
@@ -2171,7 +2177,7 @@ int phj_prepare_device() {
     HJ_CU(cudaFuncSetAttribute(join_compact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kCompactSmem));
     g_attr_done[cur_dev] = true;
-    return HJ_OK;
+    return nphj_prepare_device();
 }
 
 int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
@@ -2303,12 +2309,31 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.test_stall = (pass == 0 && (test_flags & 1)) ? 1 : 0;
         sa.counters = s.counters;
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
-        if (lp)
-            scatter_kernel<kScatterThreads, kScatterItems, true, kScatterBufs, kScatterCtasPerSm>
-                <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
-        else
+        sa.item_base = sa.item_end = 0;
+        if (lp) {
+            // First-match joins need each final build partition in input order (the join keeps the
+            // lowest position among equal keys), so the build relation's items take the stable rank.
+            // The probe relation's order inside a partition changes nothing (each probe tuple finds its
+            // first match on its own), so its items take the cheaper atomic rank, in a second launch.
+            const uint32_t per_chunk = pass == 0 ? cg.spc : (uint32_t)F1;
+            const uint32_t r_items = cg.cR * per_chunk, all_items = (cg.cR + cg.cS) * per_chunk;
+            sa.item_end = r_items;
+            if (r_items) {
+                scatter_kernel<kScatterThreads, kScatterItems, true, kScatterBufs, kScatterCtasPerSm>
+                    <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+                nlaunch++;
+            }
+            sa.item_base = r_items;
+            sa.item_end = all_items;
+            sa.ctr_item = pass == 0 ? kCtrItem1S : kCtrItem2S;
+            sa.test_stall = 0;
+            if (all_items > r_items)
+                scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
+                    <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+        } else {
             scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
                 <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+        }
         HJ_CU(cudaGetLastError());
         nlaunch++;
         HJ_PH(segm ? 3 : 3 + pass);

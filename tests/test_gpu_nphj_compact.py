@@ -78,3 +78,25 @@ def test_compact_slots_pkfk_sizes(hj, cuda):
         cuda.cuda.synchronize()
         r = hj.join("nphj_sc", R, S, on_device=True)
         assert (r.matched_cnt, r.checksum) == hj.pkfk_closed_form(nR, nS)
+
+
+def test_sliced_build_and_its_fallback(hj, oracle, cuda):
+    """Compact tables are built slice by slice in shared memory (8192 slots per slice, probes wrap
+    inside the slice) unless some slice would be filled above 7/8: then the build claims global slots by
+    CAS instead. Both modes give the oracle's result: uniform keys (sliced), one key repeated 9000 times
+    (its slice overfills: fallback), and a key repeated 2500 times (its slice holds ~6600 of 8192 slots:
+    sliced, with a long cluster)."""
+    rng = np.random.default_rng(23)
+    nR = (1 << 21) + 4099
+    base = rng.integers(1, 2**32 - 2, nR, dtype=np.uint64)
+    rids = rng.integers(0, 2**32, nR, dtype=np.uint64)
+    for hot in (0, 9000, 2500):
+        k = base.copy()
+        if hot:
+            k[rng.choice(nR, hot, replace=False)] = np.uint64(123456789)
+        nS = 3 << 20
+        probe = k[rng.integers(0, nR, nS)]
+        probe[::13] = rng.integers(1, 2**33, probe[::13].size, dtype=np.uint64)
+        probe[::101] = np.uint64(123456789)
+        S = rel(probe, rng.integers(0, 2**64 - 1, nS, dtype=np.uint64))
+        check(hj, oracle, cuda, rel(k, rids), S)
