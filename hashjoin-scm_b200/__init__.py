@@ -634,3 +634,81 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ------------------------------------------------------------------------------------------------
+# Sharded joins: one join over the GPUs of a torch.distributed process group
+# ------------------------------------------------------------------------------------------------
+def shard_route(T, nshards: int, stream: int | None = None):
+    """Group the tuples of a CUDA tensor T (n, 2) int64 by owner rank (hj_shard_route, stable: input
+    order kept within each owner's range). Returns (routed tensor, counts) with counts an int64 CUDA
+    tensor of nshards entries."""
+    import torch
+
+    L = lib()
+    if not getattr(L, "_shard_bound", False):
+        L.hj_shard_route_scratch_bytes.argtypes = [ctypes.c_size_t, ctypes.c_int]
+        L.hj_shard_route_scratch_bytes.restype = ctypes.c_size_t
+        L.hj_shard_route.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        L.hj_shard_route.restype = ctypes.c_int
+        L._shard_bound = True
+    if not T.is_cuda:
+        raise ValueError("shard_route takes a CUDA tensor")
+    n = T.shape[0]
+    out = torch.empty_like(T)
+    counts = torch.empty(nshards, dtype=torch.int64, device=T.device)
+    sb = L.hj_shard_route_scratch_bytes(n, nshards)
+    scratch = torch.empty(sb, dtype=torch.uint8, device=T.device)
+    st = stream if stream is not None else torch.cuda.current_stream(T.device).cuda_stream
+    rc = L.hj_shard_route(T.data_ptr() if n else None, n, nshards, out.data_ptr() if n else None, counts.data_ptr(),
+                          scratch.data_ptr(), sb, st)
+    if rc:
+        raise JoinError(rc, "hj_shard_route")
+    return out, counts
+
+
+def sharded_join(algo: str, R, S, *, group=None, bits: int = 14, passes: int = 2, ctx: "Context | None" = None,
+                 route=None, local_join=None) -> tuple[int, int]:
+    """One join of the relations spread over the ranks of a torch.distributed process group: rank r
+    holds R_r and S_r (CUDA tensors (n, 2) int64), and the join is that of R = R_0 ++ R_1 ++ ... and
+    S = S_0 ++ S_1 ++ ... (first-match joins take the first build tuple in that order). Every rank
+    routes its tuples to their owner ranks (hj_shard_route), one all-to-all moves them (counts first),
+    each rank joins what it owns on its GPU, and an all-reduce adds the (matched_cnt, check_sum) pairs
+    modulo 2^64. Returns the same pair on every rank. Every rank must call it with the same arguments.
+
+    route(T, nshards) -> (routed, counts) and local_join(algo, R, S) -> (matched, checksum) replace the
+    GPU routing kernel and the GPU join (defaults); tests of the exchange on CPU-only process groups
+    pass host implementations of both."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    if route is None:
+        route = shard_route
+    if local_join is None:
+        def local_join(a, r, s):
+            res = join(a, r, s, on_device=True, bits=bits, passes=passes, device=r.device.index or 0, ctx=ctx)
+            return res.matched_cnt, res.checksum
+
+    def exchange(T):
+        routed, counts = route(T, world)
+        counts = counts.to(torch.int64)
+        recv_counts = torch.empty_like(counts)
+        dist.all_to_all_single(recv_counts, counts, group=group)
+        send, recv = counts.tolist(), recv_counts.tolist()
+        out = torch.empty((sum(recv), 2), dtype=T.dtype, device=T.device)
+        dist.all_to_all_single(out, routed, output_split_sizes=recv, input_split_sizes=send, group=group)
+        return out
+
+    Rx, Sx = exchange(R), exchange(S)
+    matched, checksum = local_join(algo, Rx, Sx)
+
+    def signed(x):
+        x &= (1 << 64) - 1
+        return x - (1 << 64) if x >= 1 << 63 else x
+
+    t = torch.tensor([signed(matched), signed(checksum)], dtype=torch.int64, device=R.device)
+    dist.all_reduce(t, group=group)  # two's-complement sums wrap exactly as the u64 sums do
+    m, c = t.tolist()
+    return m & ((1 << 64) - 1), c & ((1 << 64) - 1)

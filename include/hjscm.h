@@ -338,6 +338,21 @@ int hj_nphj_join_noalloc(hj_algo_t algo, const hj_tuple_t *R_dev, size_t nR, con
                          size_t nS, hj_device_result_t *out_dev, void *stream);
 
 /* ----------------------------------------------------------------------------------------------
+ * Sharded joins over several GPUs (one process per GPU). The reference runs on one machine's threads
+ * and has no counterpart; its co-partitions are independent (src/algo/phj.c:1257-1311), so a join
+ * shards by key with one exchange step. hj_shard_route groups the n tuples of in_dev (device) by owner
+ * rank, owner = mulhi(mix64(key ^ 0x5ca1ab1e5eed0001), nshards) with mix64 the splitmix64 output mix,
+ * into out_dev (n tuples, device), stably (input order kept within each owner's range), and writes
+ * the owners' tuple counts to counts_dev (nshards u64, device). All work is enqueued on `stream`;
+ * scratch_dev (device) holds hj_shard_route_scratch_bytes(n, nshards) bytes. nshards: 1..32.
+ * The exchange itself (all-to-all of counts, then of tuples) and the sum of the local results are
+ * collective calls of the caller's communication library (the Python layer uses torch.distributed).
+ * -------------------------------------------------------------------------------------------- */
+size_t hj_shard_route_scratch_bytes(size_t n, int nshards);
+int hj_shard_route(const hj_tuple_t *in_dev, size_t n, int nshards, hj_tuple_t *out_dev, uint64_t *counts_dev,
+                   void *scratch_dev, size_t scratch_bytes, void *stream);
+
+/* ----------------------------------------------------------------------------------------------
  * Join server: requests arrive at any time and are served concurrently under an HBM budget. The
  * reference runs one join per process (src/main.c:429-448); this layer has no counterpart there.
  *   - hj_server_create allocates one device pool of hbm_budget_bytes (capped at 92% of the free device

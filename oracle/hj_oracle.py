@@ -477,3 +477,23 @@ def ref_join(algo: str, R: np.ndarray, S: np.ndarray, bits: int = 14, passes: in
         runs = ref_run_files(algo, d, "r.bin", "s.bin", R.shape[0], S.shape[0], bits, passes, threads,
                              bits1=bits1)
         return runs[0][0], runs[0][1]
+
+
+# ------------------------------------------------------------------------------------------------
+# Sharded joins: the owner of a key (the library's hj_shard_route) and a host routing of a relation
+# ------------------------------------------------------------------------------------------------
+def shard_of(keys: np.ndarray, nshards: int) -> np.ndarray:
+    """owner = mulhi(mix64(key ^ 0x5ca1ab1e5eed0001), nshards), mix64 = splitmix64's output mix."""
+    z = np.asarray(keys, dtype=np.uint64) ^ np.uint64(0x5CA1AB1E5EED0001)
+    t = np.empty_like(z)
+    _mix64_inplace(z, t)
+    hi, lo = z >> np.uint64(32), z & np.uint64(0xFFFFFFFF)
+    n = np.uint64(nshards)
+    return ((hi * n + ((lo * n) >> np.uint64(32))) >> np.uint64(32)).astype(np.int64)
+
+
+def shard_route(T: np.ndarray, nshards: int):
+    """Stable grouping of the tuples of T (n x 2) by owner: (routed tuples, tuples per owner)."""
+    own = shard_of(T[:, 0], nshards)
+    order = np.argsort(own, kind="stable")
+    return T[order], np.bincount(own, minlength=nshards).astype(np.int64)
