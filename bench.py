@@ -339,39 +339,49 @@ def run_ours(a, rank, world, local_rank):
     seg_mode = a.algo.startswith("phj") and phases["hist"] == 0.0
 
     # Roofline of the dominant kernel. Radix joins: a partition pass reads and writes every tuple once
-    # (32 B); the pipeline with P materialised passes moves 16 (2P + 1) B per tuple. Non-partitioned
-    # joins: build and probe read every tuple and touch one 16-byte table slot each (32 B per tuple).
+    # (32 B); when the last pass stores compact final partitions (8-byte words, HJ_RES_COMPACT_PARTITIONS)
+    # it writes 8 B per tuple (24 B) and the join reads 8 B per tuple instead of 16. The pipeline with P
+    # passes moves 16 (2P + 1) B per tuple, 64 B with compact final partitions at P = 2.
+    # Non-partitioned joins: build and probe read every tuple and touch one 16-byte slot each (32 B).
     peak, peak_kind = measured_peaks()
     step_s = ms / 1e3 / a.steps
+    compact = bool(results[-1].flags & hj.HJ_RES_COMPACT_PARTITIONS)
     if a.algo.startswith("phj"):
         P = results[-1].physical_passes
-        pass_s = statistics.mean([phases["pass1"], phases["pass2"]]) if P == 2 else phases["pass1"]
-        scatter_bytes = 32 * (nR + nS)
+        last_b = 24 if compact else 32
+        pass_b = [32, last_b] if P == 2 else [last_b]
+        pass_t = [phases["pass1"], phases["pass2"]] if P == 2 else [phases["pass1"]]
+        scatter_bytes = sum(pass_b) / len(pass_b) * (nR + nS)  # per launch, averaged like the times
+        pass_s = statistics.mean(pass_t)
         achieved = scatter_bytes / pass_s / 1e9
         prof = traffic_profile("scatter_kernel")
         traffic = prof["dram_bytes_per_tuple"] * (nR + nS) if prof else None
         if seg_mode:
             # per launch, averaged over the two passes like `achieved`
             p1 = traffic_profile("seg_pass1_kernel")
-            traffic = ((p1["dram_bytes_per_tuple"] + prof["dram_bytes_per_tuple_pass2"]) / 2 * (nR + nS)
-                       if p1 and prof else None)
+            key2 = "dram_bytes_per_tuple_pass2_compact" if compact else "dram_bytes_per_tuple_pass2"
+            traffic = ((p1["dram_bytes_per_tuple"] + prof[key2]) / 2 * (nR + nS)
+                       if p1 and prof and key2 in prof else None)
         kname = ("seg_pass1_kernel / scatter_kernel (mean of the two radix partition passes)" if seg_mode
-                 else "scatter_kernel (one radix partition pass)")
+                 else "scatter_kernel (radix partition passes, mean per launch)")
         roofline = {"kernel": kname, "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": peak_kind, "traffic": traffic,
-                    "algorithmic_bytes_per_launch": scatter_bytes, "launch_ms": pass_s * 1e3}
-        per_tuple = 16 * (2 * P + 1)
+                    "algorithmic_bytes_per_launch": scatter_bytes, "launch_ms": pass_s * 1e3,
+                    "per_pass": [{"bytes_per_tuple": b, "ms": t * 1e3, "gbs": b * (nR + nS) / t / 1e9,
+                                  "frac": b * (nR + nS) / t / 1e9 / peak} for b, t in zip(pass_b, pass_t)]}
+        per_tuple = sum(pass_b) + (8 if compact else 16)
     else:
         per_tuple = 32
         join_bytes = per_tuple * (nR + nS)
         achieved = join_bytes / step_s / 1e9
-        roofline = {"kernel": "nphj_build + nphj_probe (the whole join)", "bound": "hbm",
+        roofline = {"kernel": "non-partitioned build + probe (the whole join)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": peak_kind, "traffic": None,
                     "algorithmic_bytes_per_launch": join_bytes, "launch_ms": step_s * 1e3}
     pipe_bytes = per_tuple * (nR + nS)
     pipeline = {"algorithmic_bytes_per_tuple": per_tuple, "bytes_per_step": pipe_bytes,
+                "compact_final_partitions": compact,
                 "achieved_gbs": pipe_bytes / step_s / 1e9, "frac": pipe_bytes / step_s / 1e9 / peak,
                 "phase_ms": {k: v * 1e3 for k, v in phases.items()}}
 

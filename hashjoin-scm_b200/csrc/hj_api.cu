@@ -337,6 +337,7 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     out->matched_cnt = c->acc_host->matched;
     out->checksum = c->acc_host->checksum;
     out->large_partitions = c->acc_host->large_parts;
+    out->flags = (uint32_t)c->acc_host->flags;
     if (timing) {
         float a = 0, b = 0, h = 0;
         cudaEventElapsedTime(&a, c->ev_start, c->ev_mid);
@@ -456,6 +457,7 @@ static int join_mat(hj_ctx *c, hj_algo_t algo, const hj_params_t &p, const hj_tu
     out->matched_cnt = n;
     out->checksum = c->acc_host->checksum;
     out->large_partitions = c->acc_host->large_parts;
+    out->flags = (uint32_t)c->acc_host->flags;
     if (timing) {
         float a = 0, b = 0, r = 0, h = 0;
         cudaEventElapsedTime(&a, c->ev_start, c->ev_mid);

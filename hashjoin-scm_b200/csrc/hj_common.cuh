@@ -31,7 +31,8 @@ struct JoinAccum {
     unsigned int dup_flag;      // set by NPHJ builds that saw an equal key twice
     unsigned long long large_parts;
     unsigned long long pairs;   // materialising joins: output slots reserved so far
-    unsigned long long pad[3];
+    unsigned long long flags;   // HJ_RES_* bits of hj_result_t.flags
+    unsigned long long pad[2];
 };
 
 __device__ __forceinline__ void set_error(unsigned int *err, uint32_t bit) { atomicOr(err, bit); }
@@ -56,6 +57,19 @@ __device__ __forceinline__ tuple_v ld_stream(const tuple_v *p) {
 // Streaming store: the partition output is re-read only by the next pass, after the whole pass.
 __device__ __forceinline__ void st_stream(tuple_v *p, tuple_v v) {
     asm volatile("st.global.cs.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(v.x), "l"(v.y) : "memory");
+}
+
+// 8-byte variants for partitions stored as compact words (key bits above the radix bits << 32 | row id).
+__device__ __forceinline__ unsigned long long ld_stream8(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u64 %0, [%1], %2;"
+                 : "=l"(v)
+                 : "l"(p), "l"(policy_evict_first()));
+    return v;
+}
+
+__device__ __forceinline__ void st_stream8(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.global.cs.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

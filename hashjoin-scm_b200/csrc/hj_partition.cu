@@ -86,10 +86,28 @@ enum : int {
     kCtrErr = 15,
     kCtrMaxKey = 16,     // u64: OR of all R keys (words 16-17)
     kCtrMaxRid = 18,     // u64: OR of all R row ids (words 18-19)
-    kCtrItem1S = 20,     // first-match joins: pass-1 work-item counter of the probe relation's items
-    kCtrItem2S = 21,     // first-match joins: pass-2 work-item counter of the probe relation's items
-    kNumCounters = 22
+    kCtrOrRidS = 20,     // u64: OR of all S row ids (words 20-21)
+    kCtrItem1S = 22,     // first-match joins: pass-1 work-item counter of the probe relation's items
+    kCtrItem2S = 23,     // first-match joins: pass-2 work-item counter of the probe relation's items
+    kNumCounters = 24
 };
+
+// Compact final partitions. When every build key shifted right by the radix bits is below 2^31 and
+// every row id (build and probe) below 2^32, the last partition pass stores each tuple as one 8-byte
+// word, (key >> bits) << 32 | row id, and the joins read 8 bytes per tuple instead of 16. Inside a
+// final partition the low `bits` key bits are equal, so comparing key >> bits compares keys. A probe
+// key whose high part does not fit is stored as 0xffffffff: no build key has that high part. The
+// widths are ORed together by the pass that reads the relations first (hist_chunk_kernel or
+// seg_pass1_kernel), so the choice is made on the device, before the last pass.
+__device__ __forceinline__ bool ci_applies(const uint32_t *counters, int bits) {
+    const unsigned long long *mx = reinterpret_cast<const unsigned long long *>(counters + kCtrMaxKey);
+    return (mx[0] >> bits) < (1ull << 31) && mx[1] < (1ull << 32) && mx[2] < (1ull << 32);
+}
+
+__device__ __forceinline__ unsigned long long ci_word(unsigned long long key, unsigned long long rid, int bits) {
+    const unsigned long long hi = key >> bits;
+    return ((hi < 0xffffffffull ? hi : 0xffffffffull) << 32) | (rid & 0xffffffffull);
+}
 
 // Build partitions up to this size whose keys (above the radix bits) and row ids fit 32 bits are
 // joined with a 4-byte-per-field shared-memory table, two CTAs per SM.
@@ -173,9 +191,9 @@ __device__ __forceinline__ void tma_load_1d(void *dst_smem, const void *src, uin
 }
 
 // Count the tuples [lo, hi) of `in`, read by one warp (four 512-byte loads in flight), into the joint
-// histogram and into the warp's histogram of the pass-1 digit. BUILD: also OR together all keys and row
-// ids; their widths decide whether the compact join table applies (a value fits 32 bits iff the OR of
-// all values does).
+// histogram and into the warp's histogram of the pass-1 digit, ORing together all row ids and (BUILD)
+// all keys: their widths decide whether the compact join table and the compact final partitions apply
+// (a value fits k bits iff the OR of all values does).
 template <bool BUILD>
 __device__ __forceinline__ void hist_range_warp(const tuple_v *__restrict__ in, uint64_t lo, uint64_t hi,
                                                 uint32_t *sh_hist, uint32_t *wsub, uint64_t mask, uint32_t m1,
@@ -192,19 +210,15 @@ __device__ __forceinline__ void hist_range_warp(const tuple_v *__restrict__ in, 
         atomicAdd(&wsub[(uint32_t)t1.x & m1], 1u);
         atomicAdd(&wsub[(uint32_t)t2.x & m1], 1u);
         atomicAdd(&wsub[(uint32_t)t3.x & m1], 1u);
-        if (BUILD) {
-            kor |= t0.x | t1.x | t2.x | t3.x;
-            ror |= t0.y | t1.y | t2.y | t3.y;
-        }
+        if (BUILD) kor |= t0.x | t1.x | t2.x | t3.x;
+        ror |= t0.y | t1.y | t2.y | t3.y;
     }
     for (; i < hi; i += 32) {
         const tuple_v t = ld_stream(in + i);
         atomicAdd(&sh_hist[t.x & mask], 1u);
         atomicAdd(&wsub[(uint32_t)t.x & m1], 1u);
-        if (BUILD) {
-            kor |= t.x;
-            ror |= t.y;
-        }
+        if (BUILD) kor |= t.x;
+        ror |= t.y;
     }
 }
 
@@ -250,15 +264,18 @@ __global__ void __launch_bounds__(512) hist_chunk_kernel(const tuple_v *__restri
         }
         __syncwarp();
     }
-    if (rel == 0) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            kor |= __shfl_xor_sync(0xffffffffu, kor, o);
-            ror |= __shfl_xor_sync(0xffffffffu, ror, o);
-        }
-        if (lane == 0) {
-            atomicOr(reinterpret_cast<unsigned long long *>(maxima), kor);
-            atomicOr(reinterpret_cast<unsigned long long *>(maxima) + 1, ror);
+    for (int o = 16; o > 0; o >>= 1) {
+        kor |= __shfl_xor_sync(0xffffffffu, kor, o);
+        ror |= __shfl_xor_sync(0xffffffffu, ror, o);
+    }
+    if (lane == 0) {
+        unsigned long long *mx = reinterpret_cast<unsigned long long *>(maxima);
+        if (rel == 0) {
+            if (kor) atomicOr(mx, kor);
+            if (ror) atomicOr(mx + 1, ror);
+        } else if (ror) {
+            atomicOr(mx + 2, ror);
         }
     }
     __syncthreads();
@@ -339,6 +356,7 @@ struct PlanArgs {
     uint64_t max_large;
     uint64_t large_table_words;
     int agg_ok;  // joins that need no per-match output may use key-aggregated large-partition tables
+    int ci_ok;   // the join may read compact final partitions (see ci_applies)
 };
 
 __device__ __forceinline__ uint32_t part_to_value(int f, int passes, int b1, int F2) {
@@ -395,13 +413,16 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
     // Join work items (partitions with both sides non-empty, src/algo/phj.c:459-491) and large
     // partitions. Partition sizes come from the totals, starts from the running sums above.
     const uint32_t *totR = tot_all, *totS = tot_all + nparts;
+    // With compact final partitions only the compact shared-memory join and the large-partition join
+    // read them: partitions above the compact table's capacity are large.
+    const uint64_t small_cap = (a.ci_ok && ci_applies(a.counters, a.bits)) ? (uint64_t)kCompactCap : (uint64_t)kSmemCap;
     uint32_t asum = 0, bsum = 0, lsum = 0;  // items with |R_p| <= compact cap, other small items, large
     for (int f = f0; f < f1; f++) {
         const uint32_t v = part_to_value(f, a.passes, a.b1, a.F2);
         const uint64_t nr = totR[v], ns = totS[v];
         if (nr > 0 && ns > 0) {
             if (nr <= (uint64_t)kCompactCap) asum += ceil_div_u64(ns, kProbeChunk);
-            else if (nr <= (uint64_t)kSmemCap) bsum += ceil_div_u64(ns, kProbeChunk);
+            else if (nr <= small_cap) bsum += ceil_div_u64(ns, kProbeChunk);
             else lsum++;
         }
     }
@@ -418,7 +439,7 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
         rR += nr;
         rS += ns;
         if (!(nr > 0 && ns > 0)) continue;
-        if (nr <= (uint64_t)kSmemCap) {
+        if (nr <= small_cap) {
             uint64_t &item_idx = nr <= (uint64_t)kCompactCap ? a_idx : b_idx;
             const uint32_t k = ceil_div_u64(ns, kProbeChunk);
             for (uint32_t q = 0; q < k; q++, item_idx++) {
@@ -582,6 +603,10 @@ struct ScatterArgs {
     // Work items of this launch: [item_base, item_end) of the pass's items (R's first, then S's), claimed
     // through counters[ctr_item]; item_end 0 = all of them.
     uint32_t item_base, item_end;
+    // Last pass of a join that may read compact final partitions: when ci_applies holds, the output is
+    // 8-byte words (ci_word) at outR8 / outS8 instead of tuples at outR / outS.
+    int ci_out;
+    unsigned long long *outR8, *outS8;
 };
 
 // A tile claimed for processing: its source, length, output region and owning work item.
@@ -747,6 +772,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     const unsigned ltmask = lanemask_lt();
     const uint32_t bar0 = smem_addr(&bars[0]);
     const int nbins = 1 << a.bits;
+    const bool ci = a.ci_out && ci_applies(a.counters, a.bits);
     __shared__ ItemIter it;  // used by thread 0 only
     uint32_t pend = 0;       // thread 0: next segment of the chain (segment mode)
     ItemAhead ah;            // thread 0: the item claimed ahead
@@ -931,8 +957,10 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             }
         }
         __syncthreads();
-        // Write each digit run: consecutive threads write consecutive 16-byte tuples. Full tiles load
-        // their staged tuples in two halves so that the stores issue back to back.
+        // Write each digit run: consecutive threads write consecutive 16-byte tuples (8-byte words for
+        // compact final partitions). Full tiles load their staged tuples in two halves so that the stores
+        // issue back to back.
+        unsigned long long *out8 = sl.out == a.outS ? a.outS8 : a.outR8;
         if (cnt == (uint32_t)T) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
@@ -946,10 +974,14 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
                              (long long)(tid + (hh * ITEMS / 2 + i) * THREADS);
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) {
-                    if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len)
-                        st_stream(sl.out + dst[i], t[i]);
-                    else
+                    if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len) {
+                        if (ci)
+                            st_stream8(out8 + dst[i], ci_word(t[i].x, t[i].y, a.bits));
+                        else
+                            st_stream(sl.out + dst[i], t[i]);
+                    } else {
                         set_error(err, kErrBounds);
+                    }
                 }
             }
         } else
@@ -957,10 +989,14 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             const tuple_v t = buf[j];
             const uint32_t dd = (uint32_t)((t.x >> a.shift) & dmask);
             const long long dst = gbase[dd] + (long long)j;
-            if (dst >= 0 && (uint64_t)dst < sl.out_len)
-                st_stream(sl.out + dst, t);
-            else
+            if (dst >= 0 && (uint64_t)dst < sl.out_len) {
+                if (ci)
+                    st_stream8(out8 + dst, ci_word(t.x, t.y, a.bits));
+                else
+                    st_stream(sl.out + dst, t);
+            } else {
                 set_error(err, kErrBounds);
+            }
         }
         __syncthreads();
     }
@@ -1116,7 +1152,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
 
     int phase_rel = 0;           // relation whose tuples the counters and segment state hold
     uint32_t since = 0;          // upper bound of every counter (uniform)
-    unsigned long long kor = 0, ror = 0;
+    unsigned long long kor = 0, ror = 0, rors = 0;
     __shared__ uint32_t s_max[THREADS / 32];
 
     for (uint32_t k = 0;; k++) {
@@ -1200,6 +1236,8 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 if (sl.rel == 0) {
                     kor |= v[i].x;
                     ror |= v[i].y;
+                } else {
+                    rors |= v[i].y;
                 }
             }
         }
@@ -1349,11 +1387,13 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
     for (int o = 16; o > 0; o >>= 1) {
         kor |= __shfl_xor_sync(0xffffffffu, kor, o);
         ror |= __shfl_xor_sync(0xffffffffu, ror, o);
+        rors |= __shfl_xor_sync(0xffffffffu, rors, o);
     }
-    if (lane == 0 && (kor | ror)) {
+    if (lane == 0 && (kor | ror | rors)) {
         unsigned long long *mx = reinterpret_cast<unsigned long long *>(a.counters + kCtrMaxKey);
-        atomicOr(mx, kor);
-        atomicOr(mx + 1, ror);
+        if (kor) atomicOr(mx, kor);
+        if (ror) atomicOr(mx + 1, ror);
+        if (rors) atomicOr(mx + 2, rors);
     }
 }
 
@@ -1386,7 +1426,27 @@ struct JoinArgs {
     int skip0;  // build tuples with key 0 never match (key 0 marks an empty slot in lp_join)
     JoinAccum *acc;
     MatOut mat; // materialising joins (MAT kernels): where the (r.row_id, s.row_id) pairs go
+    int ci;     // the final partitions may be compact words (when ci_applies holds) at finR8 / finS8
+    const unsigned long long *finR8, *finS8;
 };
+
+// A tuple of a final partition: the stored tuple, or for compact partitions {key >> bits, row id}.
+// Joins compare x for equality and hash x >> shift with shift = bits (tuples) or 0 (compact words).
+__device__ __forceinline__ tuple_v ld_fin(const tuple_v *p16, const unsigned long long *p8, uint64_t i, bool ci) {
+    if (ci) {
+        const unsigned long long w = ld_stream8(p8 + i);
+        return make_ulonglong2(w >> 32, w & 0xffffffffull);
+    }
+    return ld_stream(p16 + i);
+}
+
+__device__ __forceinline__ tuple_v fin_r(const JoinArgs &a, bool ci, uint64_t i) {
+    if (ci) {
+        const unsigned long long w = a.finR8[i];
+        return make_ulonglong2(w >> 32, w & 0xffffffffull);
+    }
+    return a.finR[i];
+}
 
 constexpr int kHeadMax = 16384;  // next_pow_2(kSmemCap)
 constexpr size_t kJoinSmem = (size_t)kSmemCap * 16 + kHeadMax * 2 + (size_t)kSmemCap * 2;
@@ -1420,7 +1480,8 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
     const int tid = threadIdx.x;
     unsigned int *err = &a.counters[kCtrErr];
     const uint32_t nA = a.counters[kCtrNItemsA];
-    const int B = a.bits;
+    const bool ci = !MAT && a.ci && ci_applies(a.counters, a.bits);
+    const int B = ci ? 0 : a.bits;  // shift from a stored x to the key's bits above the radix bits
     const bool lp = a.lp != 0;
     const bool skip0 = a.skip0 != 0;
     unsigned long long cnt = 0, sum = 0;
@@ -1436,14 +1497,16 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
         uint32_t *head32 = reinterpret_cast<uint32_t *>(head);
         for (uint32_t q = tid; q < (nb + 1) / 2; q += kCompactThreads) head32[q] = 0;
         __syncthreads();
-        // Load and chain the build side; lp_join skips key 0, which reads as an empty slot there.
+        // Load and chain the build side; lp_join skips key 0, which reads as an empty slot there (compact
+        // final partitions are never used by joins with that rule).
         const tuple_v *R = a.finR + item.r_begin;
+        const unsigned long long *R8 = a.finR8 + item.r_begin;
         for (uint32_t i0 = tid; i0 < nr; i0 += 4 * kCompactThreads) {
             tuple_v t[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const uint32_t i = i0 + u * kCompactThreads;
-                t[u] = i < nr ? ld_stream(R + i) : make_ulonglong2(0, 0);
+                t[u] = i < nr ? ld_fin(R, R8, i, ci) : make_ulonglong2(0, 0);
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
@@ -1457,6 +1520,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
         }
         __syncthreads();
         const tuple_v *S = a.finS + item.s_begin;
+        const unsigned long long *S8 = a.finS8 + item.s_begin;
         const uint32_t ns = item.s_len;
         if constexpr (MAT) {
             constexpr int U = 4;  // probe tuples per thread and round: loads in flight, fewer rounds
@@ -1513,7 +1577,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const uint32_t j = j0 + u * kCompactThreads;
-                sv[u] = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
+                sv[u] = j < ns ? ld_fin(S, S8, j, ci) : make_ulonglong2(0, 0);
             }
 #pragma unroll
             for (int u = 0; u < 8; u++) {
@@ -1760,14 +1824,15 @@ __device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t *p) {
 // Lock-free: a node is published by a CAS on the bucket head after its next link is written; a failed
 // CAS means another insert succeeded, and only the nodes it added (above the old head) are re-checked.
 // Returns 0 (and sets the error word) if the walk exceeds the partition's size.
-__device__ __forceinline__ uint32_t large_agg_find_or_insert(const LargeAgg &t, const tuple_v *rr, uint64_t r_len,
-                                                             uint64_t h, uint64_t k, uint32_t i, uint32_t *err) {
+__device__ __forceinline__ uint32_t large_agg_find_or_insert(const LargeAgg &t, const JoinArgs &a, bool ci,
+                                                             uint64_t r_begin, uint64_t r_len, uint64_t h,
+                                                             uint64_t k, uint32_t i, uint32_t *err) {
     uint32_t stop = 0;
     uint32_t e = ld_volatile_u32(&t.head[h]);
     uint64_t steps = 0;
     for (;;) {
         for (uint32_t x = e; x && x != stop; x = ld_volatile_u32(&t.next[x - 1])) {
-            if (rr[x - 1].x == k) return x;
+            if (fin_r(a, ci, r_begin + x - 1).x == k) return x;
             if (++steps > r_len) {
                 set_error(err, kErrProbeLimit);
                 return 0;
@@ -1789,6 +1854,8 @@ __device__ __forceinline__ uint32_t large_agg_find_or_insert(const LargeAgg &t, 
 __global__ void join_large_build(JoinArgs a) {
     const int nl = (int)a.counters[kCtrNLarge];
     const uint64_t total = ld_u64_pair(&a.counters[kCtrLargeR]);
+    const bool ci = a.ci && ci_applies(a.counters, a.bits);
+    const int bshift = ci ? 0 : a.bits;
     if (a.counters[kCtrLargeAgg]) {
         // Warp-uniform rounds: lanes holding equal keys (equal keys always share a partition) combine
         // their count, row-id sum and smallest position first, so a hot key costs one update per warp.
@@ -1803,7 +1870,7 @@ __global__ void join_large_build(JoinArgs a) {
             if (act) {
                 l = find_large(a.large, nl, g, true);
                 i = g - a.large[l].r_flat;
-                r = a.finR[a.large[l].r_begin + i];
+                r = fin_r(a, ci, a.large[l].r_begin + i);
                 act = !(a.skip0 && r.x == 0);
             }
             const unsigned act_mask = __ballot_sync(0xffffffffu, act);
@@ -1817,8 +1884,8 @@ __global__ void join_large_build(JoinArgs a) {
             if ((int)lane != __ffs(peers) - 1) continue;
             const LargePart &L = a.large[l];
             const LargeAgg t = large_agg(a.large_table, L);
-            const uint64_t h = (r.x >> a.bits) & ((1ull << L.nb_log) - 1);
-            const uint32_t node = large_agg_find_or_insert(t, a.finR + L.r_begin, L.r_len, h, r.x, (uint32_t)i,
+            const uint64_t h = (r.x >> bshift) & ((1ull << L.nb_log) - 1);
+            const uint32_t node = large_agg_find_or_insert(t, a, ci, L.r_begin, L.r_len, h, r.x, (uint32_t)i,
                                                            &a.counters[kCtrErr]);
             if (!node) continue;
             atomicAdd(&t.cnt[node - 1], (uint32_t)__popc(peers));
@@ -1833,11 +1900,11 @@ __global__ void join_large_build(JoinArgs a) {
         const int l = find_large(a.large, nl, g, true);
         const LargePart &L = a.large[l];
         const uint64_t i = g - L.r_flat;
-        const uint64_t k = a.finR[L.r_begin + i].x;
+        const uint64_t k = fin_r(a, ci, L.r_begin + i).x;
         if (a.skip0 && k == 0) continue;
         uint32_t *head = a.large_table + L.table_off;
         uint32_t *nxt = head + (1ull << L.nb_log);
-        const uint64_t h = (k >> a.bits) & ((1ull << L.nb_log) - 1);
+        const uint64_t h = (k >> bshift) & ((1ull << L.nb_log) - 1);
         nxt[i] = atomicExch(&head[h], (uint32_t)(i + 1));
     }
 }
@@ -1850,6 +1917,8 @@ __global__ void join_large_probe(JoinArgs a) {
     const int nl = (int)a.counters[kCtrNLarge];
     const uint64_t total = ld_u64_pair(&a.counters[kCtrLargeS]);
     unsigned long long cnt = 0, sum = 0;
+    const bool ci = !MAT && a.ci && ci_applies(a.counters, a.bits);
+    const int bshift = ci ? 0 : a.bits;
     if constexpr (MAT) {
         unsigned int *err = &a.counters[kCtrErr];
         // Block-uniform rounds over the flattened probe tuples of all large partitions.
@@ -1898,12 +1967,11 @@ __global__ void join_large_probe(JoinArgs a) {
              g += (uint64_t)gridDim.x * blockDim.x) {
             const int l = find_large(a.large, nl, g, false);
             const LargePart &L = a.large[l];
-            const tuple_v s = ld_stream(a.finS + L.s_begin + (g - L.s_flat));
+            const tuple_v s = ld_fin(a.finS, a.finS8, L.s_begin + (g - L.s_flat), ci);
             const LargeAgg t = large_agg(a.large_table, L);
-            const tuple_v *rr = a.finR + L.r_begin;
-            uint32_t e = t.head[(s.x >> a.bits) & ((1ull << L.nb_log) - 1)];
+            uint32_t e = t.head[(s.x >> bshift) & ((1ull << L.nb_log) - 1)];
             uint64_t steps = 0;
-            while (e && rr[e - 1].x != s.x) {
+            while (e && fin_r(a, ci, L.r_begin + e - 1).x != s.x) {
                 e = t.next[e - 1];
                 if (++steps > L.r_len) {
                     set_error(&a.counters[kCtrErr], kErrProbeLimit);
@@ -1915,7 +1983,7 @@ __global__ void join_large_probe(JoinArgs a) {
                 const uint32_t first = ~t.negpos[e - 1];
                 if (first < L.r_len) {
                     cnt++;
-                    sum += rr[first].y + s.y;
+                    sum += fin_r(a, ci, L.r_begin + first).y + s.y;
                 } else {
                     set_error(&a.counters[kCtrErr], kErrBounds);
                 }
@@ -1930,15 +1998,14 @@ __global__ void join_large_probe(JoinArgs a) {
          g += (uint64_t)gridDim.x * blockDim.x) {
         const int l = find_large(a.large, nl, g, false);
         const LargePart &L = a.large[l];
-        const tuple_v s = ld_stream(a.finS + L.s_begin + (g - L.s_flat));
+        const tuple_v s = ld_fin(a.finS, a.finS8, L.s_begin + (g - L.s_flat), ci);
         const uint32_t *head = a.large_table + L.table_off;
         const uint32_t *nxt = head + (1ull << L.nb_log);
-        const tuple_v *rr = a.finR + L.r_begin;
-        uint32_t e = head[(s.x >> a.bits) & ((1ull << L.nb_log) - 1)];
+        uint32_t e = head[(s.x >> bshift) & ((1ull << L.nb_log) - 1)];
         uint32_t best = 0;
         uint64_t steps = 0;
         while (e) {
-            const tuple_v r = rr[e - 1];
+            const tuple_v r = fin_r(a, ci, L.r_begin + e - 1);
             if (r.x == s.x) {
                 if (a.lp) {
                     if (best == 0 || e < best) best = e;
@@ -1955,11 +2022,14 @@ __global__ void join_large_probe(JoinArgs a) {
         }
         if (a.lp && best) {
             cnt++;
-            sum += rr[best - 1].y + s.y;
+            sum += fin_r(a, ci, L.r_begin + best - 1).y + s.y;
         }
     }
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
-    if (blockIdx.x == 0 && threadIdx.x == 0 && nl) atomicAdd(&a.acc->large_parts, (unsigned long long)nl);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (nl) atomicAdd(&a.acc->large_parts, (unsigned long long)nl);
+        if (ci) atomicOr(&a.acc->flags, (unsigned long long)HJ_RES_COMPACT_PARTITIONS);
+    }
 }
 
 __global__ void copy_error(const uint32_t *counters, JoinAccum *acc) {
@@ -2268,6 +2338,10 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     pa.max_large = s.max_large;
     pa.large_table_words = s.large_table_words;
     pa.agg_ok = mat ? 0 : 1;
+    // Compact final partitions: joins without per-match output whose key 0 may match (every join but
+    // the materialising ones and phj_radix_lp), when the widths allow (decided on the device).
+    const int ci_ok = (!mat && !skip0) ? 1 : 0;
+    pa.ci_ok = ci_ok;
     plan_kernel<<<1, 1024, g.bits <= kPlanStageBits ? (size_t)2 * np * 4 : 0, st>>>(pa);
     {
         const int ut = F1 < 32 ? 32 : F1;
@@ -2310,6 +2384,9 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.counters = s.counters;
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
         sa.item_base = sa.item_end = 0;
+        sa.ci_out = (pass == g.passes - 1) ? ci_ok : 0;
+        sa.outR8 = reinterpret_cast<unsigned long long *>(out);
+        sa.outS8 = sa.outR8 + nR;
         if (lp) {
             // First-match joins need each final build partition in input order (the join keeps the
             // lowest position among equal keys), so the build relation's items take the stable rank.
@@ -2354,6 +2431,9 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     ja.skip0 = skip0 ? 1 : 0;
     ja.acc = acc;
     ja.mat = mat ? *mat : MatOut{nullptr, 0};
+    ja.ci = ci_ok;
+    ja.finR8 = reinterpret_cast<const unsigned long long *>(s.tmp2);
+    ja.finS8 = ja.finR8 + nR;
     if (mat) {
         join_compact_kernel<true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
         join_small_kernel<true><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);

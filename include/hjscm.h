@@ -132,9 +132,14 @@ typedef struct {
     uint64_t large_partitions; /* partitions joined through the global-memory path (PHJ only) */
     double phase[HJ_PH_COUNT]; /* per-kernel-group seconds (HJ_F_PHASE_TIMES) */
     uint32_t kernel_launches;  /* kernels this join launched */
-    uint32_t pad;
+    uint32_t flags;            /* HJ_RES_* bits */
     double retrieve;           /* materialising joins: seconds of the retrieve phase (included in total) */
 } hj_result_t;
+
+/* hj_result_t.flags: the last partition pass stored the final partitions as 8-byte words
+ * (key >> radix bits) << 32 | row id, which the joins read (radix joins without per-match output and
+ * without the key-0 rule, when every build key >> radix bits is below 2^31 and every row id below 2^32). */
+#define HJ_RES_COMPACT_PARTITIONS 0x1u
 
 typedef struct hj_ctx hj_ctx_t;
 

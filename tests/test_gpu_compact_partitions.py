@@ -1,0 +1,104 @@
+"""Compact final partitions on the B200: when every build key shifted right by the radix bits is below
+2^31 and every row id (build and probe) below 2^32, the last partition pass stores 8-byte words
+(key >> bits) << 32 | row id and the joins read those (hj_result_t.flags has HJ_RES_COMPACT_PARTITIONS).
+Results equal the oracle's on both sides of every limit, through both pipelines and the large-partition
+path; joins with per-match output or the key-0 rule never use them."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+BITS = 14
+
+
+def dev(cuda, a):
+    return cuda.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+
+
+def rels(seed, nR=1 << 18, nS=1 << 20, kmax=1 << 24):
+    rng = np.random.default_rng(seed)
+    R = np.empty((nR, 2), dtype=np.uint64)
+    R[:, 0] = rng.integers(1, kmax, nR, dtype=np.uint64)
+    R[:, 1] = rng.integers(0, 1 << 32, nR, dtype=np.uint64)
+    S = np.empty((nS, 2), dtype=np.uint64)
+    S[:, 0] = R[rng.integers(0, nR, nS), 0]
+    S[::7, 0] = rng.integers(1, kmax, S[::7].shape[0], dtype=np.uint64)
+    S[:, 1] = rng.integers(0, 1 << 32, nS, dtype=np.uint64)
+    return R, S
+
+
+def run(hj, oracle, cuda, algo, R, S, flags=0, bits=BITS, passes=2):
+    r = hj.join(algo, dev(cuda, R), dev(cuda, S), on_device=True, bits=bits, passes=passes, flags=flags)
+    assert (r.matched_cnt, r.checksum) == oracle.join(algo, R, S), (algo, flags, bits, passes)
+    return bool(r.flags & hj.HJ_RES_COMPACT_PARTITIONS)
+
+
+@pytest.mark.parametrize("pipeline", ["exact", "segments"])
+def test_flag_and_results_at_the_limits(hj, oracle, cuda, pipeline):
+    flags = hj.HJ_F_SEGMENTS if pipeline == "segments" else hj.HJ_F_EXACT
+    R, S = rels(1)
+    assert run(hj, oracle, cuda, "phj_radix_bc", R, S, flags)
+    # largest build key that fits: (2^31 - 1) << 14 | digits
+    R2 = R.copy()
+    R2[5, 0] = np.uint64(((1 << 31) - 1) << BITS | 77)
+    S2 = S.copy()
+    S2[3, 0] = R2[5, 0]
+    assert run(hj, oracle, cuda, "phj_radix_bc", R2, S2, flags)
+    # one build key past it: wide partitions
+    R3 = R2.copy()
+    R3[6, 0] = np.uint64((1 << 31) << BITS | 78)
+    S3 = S2.copy()
+    S3[4, 0] = R3[6, 0]
+    assert not run(hj, oracle, cuda, "phj_radix_bc", R3, S3, flags)
+    # a build row id of 2^32, or a probe row id of 2^32: wide
+    R4 = R.copy()
+    R4[9, 1] = np.uint64(1 << 32)
+    assert not run(hj, oracle, cuda, "phj_radix_bc", R4, S, flags)
+    S4 = S.copy()
+    S4[9, 1] = np.uint64(1 << 32)
+    assert not run(hj, oracle, cuda, "phj_radix_bc", R, S4, flags)
+    # probe keys far beyond every build key (including all ones) stay compact and never match
+    S5 = S.copy()
+    S5[::5, 0] = np.uint64(2**64 - 1)
+    S5[1::5, 0] = np.uint64((1 << 40) << BITS | 5)
+    S5[2::5, 0] = np.uint64(((1 << 31) + 3) << BITS | 9)
+    assert run(hj, oracle, cuda, "phj_radix_bc", R, S5, flags)
+
+
+def test_semantics_that_keep_tuples(hj, oracle, cuda):
+    R, S = rels(2)
+    R[::50, 0] = 0  # key 0: ignored by phj_radix_lp
+    for algo in ("phj_radix_sc", "phj_radix_hr", "phj_asymm_radix_bc", "phj_radix_bw_reg_bc"):
+        assert run(hj, oracle, cuda, algo, R, S)
+    assert not run(hj, oracle, cuda, "phj_radix_lp", R, S)
+    # one pass (8 bits) and two passes with an uneven split
+    assert run(hj, oracle, cuda, "phj_radix_bc", R, S, bits=8, passes=1)
+    assert run(hj, oracle, cuda, "phj_radix_bc", R, S, bits=11, passes=2)
+
+
+def test_large_partitions_read_compact_words(hj, oracle, cuda):
+    """Partitions above the compact shared-memory table (8192 build tuples) go to the global-memory
+    join when the final partitions are compact, with duplicate keys and a hot key."""
+    rng = np.random.default_rng(3)
+    n = 1 << 20
+    R = np.empty((n, 2), dtype=np.uint64)
+    part = rng.integers(0, 64, n, dtype=np.uint64)  # 64 partitions of ~16K build tuples
+    R[:, 0] = (rng.integers(0, 5000, n, dtype=np.uint64) << np.uint64(BITS)) | part
+    R[: n // 8, 0] = np.uint64((7 << BITS) | 3)  # a hot key
+    R[:, 1] = rng.integers(0, 1 << 32, n, dtype=np.uint64)
+    S = R[rng.integers(0, n, 2 * n)].copy()
+    S[:, 1] = rng.integers(0, 1 << 32, S.shape[0], dtype=np.uint64)
+    S[::9, 0] += np.uint64(1 << 30)
+    for flags in (hj.HJ_F_EXACT, hj.HJ_F_SEGMENTS):
+        assert run(hj, oracle, cuda, "phj_radix_bc", R, S, flags)
+
+
+def test_headline_shape_uses_compact_partitions(hj, cuda):
+    nR, nS = 1 << 22, 1 << 24
+    R = cuda.empty((nR, 2), dtype=cuda.int64, device="cuda")
+    S = cuda.empty((nS, 2), dtype=cuda.int64, device="cuda")
+    hj.gen_fast_device(nR, nS, R.data_ptr(), S.data_ptr(), seed=3)
+    cuda.cuda.synchronize()
+    for flags in (0, hj.HJ_F_SEGMENTS, hj.HJ_F_EXACT):
+        r = hj.join("phj_radix_bc", R, S, on_device=True, flags=flags)
+        assert (r.matched_cnt, r.checksum) == hj.pkfk_closed_form(nR, nS)
+        assert r.flags & hj.HJ_RES_COMPACT_PARTITIONS
