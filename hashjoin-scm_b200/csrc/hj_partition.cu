@@ -356,7 +356,6 @@ struct PlanArgs {
     uint64_t max_large;
     uint64_t large_table_words;
     int agg_ok;  // joins that need no per-match output may use key-aggregated large-partition tables
-    int ci_ok;   // the join may read compact final partitions (see ci_applies)
 };
 
 __device__ __forceinline__ uint32_t part_to_value(int f, int passes, int b1, int F2) {
@@ -413,9 +412,7 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
     // Join work items (partitions with both sides non-empty, src/algo/phj.c:459-491) and large
     // partitions. Partition sizes come from the totals, starts from the running sums above.
     const uint32_t *totR = tot_all, *totS = tot_all + nparts;
-    // With compact final partitions only the compact shared-memory join and the large-partition join
-    // read them: partitions above the compact table's capacity are large.
-    const uint64_t small_cap = (a.ci_ok && ci_applies(a.counters, a.bits)) ? (uint64_t)kCompactCap : (uint64_t)kSmemCap;
+    const uint64_t small_cap = (uint64_t)kSmemCap;
     uint32_t asum = 0, bsum = 0, lsum = 0;  // items with |R_p| <= compact cap, other small items, large
     for (int f = f0; f < f1; f++) {
         const uint32_t v = part_to_value(f, a.passes, a.b1, a.F2);
@@ -1632,7 +1629,8 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
     }
     __syncthreads();
     const uint32_t nitems = a.counters[kCtrNItems];
-    const int B = a.bits;
+    const bool ci = !MAT && a.ci && ci_applies(a.counters, a.bits);
+    const int B = ci ? 0 : a.bits;  // shift from a stored x to the key's bits above the radix bits
     const bool lp = a.lp != 0;
     const bool skip0 = a.skip0 != 0;
     // Items [0, nA) went to the compact kernel if the build side's keys and row ids fit it.
@@ -1649,7 +1647,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
         const uint32_t nr = item.r_len;
         const uint32_t nb = next_pow2_u32(nr);
         const uint64_t hmask = nb - 1;
-        if (tid == 0) {
+        if (!ci && tid == 0) {
             // Order earlier generic-proxy accesses to rt before the async-proxy writes.
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             const uint32_t bytes = nr * 16u;
@@ -1668,13 +1666,19 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
         }
         uint32_t *head32 = reinterpret_cast<uint32_t *>(head);
         for (uint32_t q = tid; q < (nb + 1) / 2; q += kJoinThreads) head32[q] = 0;
-        if (!mbar_wait(bar, phase)) {
-            set_error(err, kErrSpinLimit);
-            ok = false;
+        if (ci) {
+            // Compact final partitions: expand the build side's words into {key >> bits, row id}.
+            for (uint32_t i = tid; i < nr; i += kJoinThreads)
+                rt[i] = ld_fin(a.finR + item.r_begin, a.finR8 + item.r_begin, i, true);
+        } else {
+            if (!mbar_wait(bar, phase)) {
+                set_error(err, kErrSpinLimit);
+                ok = false;
+            }
+            // An expired wait: let the R-tile copy land (bounded) before the CTA leaves its shared memory.
+            if (!ok && tid == 0) mbar_wait(bar, phase);
+            phase ^= 1u;
         }
-        // An expired wait: let the R-tile copy land (bounded) before the CTA leaves its shared memory.
-        if (!ok && tid == 0) mbar_wait(bar, phase);
-        phase ^= 1u;
         if (__syncthreads_or(!ok)) break;
         // Build: chain every R tuple (lp_join skips key 0, which reads as an empty slot there).
         for (uint32_t i = tid; i < nr; i += kJoinThreads) {
@@ -1740,7 +1744,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const uint32_t j = j0 + u * kJoinThreads;
-                s[u] = j < ns ? ld_stream(S + j) : make_ulonglong2(0, 0);
+                s[u] = j < ns ? ld_fin(S, a.finS8 + item.s_begin, j, ci) : make_ulonglong2(0, 0);
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
@@ -2341,7 +2345,6 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     // Compact final partitions: joins without per-match output whose key 0 may match (every join but
     // the materialising ones and phj_radix_lp), when the widths allow (decided on the device).
     const int ci_ok = (!mat && !skip0) ? 1 : 0;
-    pa.ci_ok = ci_ok;
     plan_kernel<<<1, 1024, g.bits <= kPlanStageBits ? (size_t)2 * np * 4 : 0, st>>>(pa);
     {
         const int ut = F1 < 32 ? 32 : F1;

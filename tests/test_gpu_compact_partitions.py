@@ -75,15 +75,18 @@ def test_semantics_that_keep_tuples(hj, oracle, cuda):
     assert run(hj, oracle, cuda, "phj_radix_bc", R, S, bits=11, passes=2)
 
 
-def test_large_partitions_read_compact_words(hj, oracle, cuda):
-    """Partitions above the compact shared-memory table (8192 build tuples) go to the global-memory
-    join when the final partitions are compact, with duplicate keys and a hot key."""
+def test_mid_and_large_partitions_read_compact_words(hj, oracle, cuda):
+    """Partitions above the compact shared-memory table (8192 build tuples) read compact words too:
+    up to 10240 build tuples in the 16-byte shared-memory join, beyond that in the global-memory join,
+    with duplicate keys and a hot key."""
     rng = np.random.default_rng(3)
-    n = 1 << 20
+    n_mid, n_big = 32 * 9000, 32 * 16000
+    part = np.concatenate([rng.integers(0, 32, n_mid, dtype=np.uint64),      # ~9000 per partition
+                           rng.integers(32, 64, n_big, dtype=np.uint64)])   # ~16000 per partition
+    n = part.size
     R = np.empty((n, 2), dtype=np.uint64)
-    part = rng.integers(0, 64, n, dtype=np.uint64)  # 64 partitions of ~16K build tuples
     R[:, 0] = (rng.integers(0, 5000, n, dtype=np.uint64) << np.uint64(BITS)) | part
-    R[: n // 8, 0] = np.uint64((7 << BITS) | 3)  # a hot key
+    R[n_mid: n_mid + n_big // 8, 0] = np.uint64((7 << BITS) | 40)  # a hot key in a large partition
     R[:, 1] = rng.integers(0, 1 << 32, n, dtype=np.uint64)
     S = R[rng.integers(0, n, 2 * n)].copy()
     S[:, 1] = rng.integers(0, 1 << 32, S.shape[0], dtype=np.uint64)
