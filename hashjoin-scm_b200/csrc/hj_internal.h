@@ -127,9 +127,13 @@ size_t nphj_scratch_bytes(size_t nR, double load, bool mat = false);
 // Shared-memory attributes of the non-partitioned join's kernels on the current device (idempotent;
 // call before capturing nphj_enqueue in a graph).
 int nphj_prepare_device();
+// phases: kNphjBuild and/or kNphjProbe. A probe-only call probes the table an earlier build-only call
+// on the same table memory (same R, nR, table, table_bytes, load) left there; its results add to acc.
+constexpr int kNphjBuild = 1, kNphjProbe = 2;
 int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr);
+                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr,
+                 int phases = kNphjBuild | kNphjProbe);
 
 // Checksum of materialised pairs as the reference's retrieve phase computes it: the wrapping sum of
 // R[r_row_id - 1].row_id + S[s_row_id - 1].row_id over the first n pairs (into acc->checksum).

@@ -668,7 +668,8 @@ int nphj_prepare_device() {
 
 int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S, size_t nS, void *table,
                  size_t table_bytes, double load, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat) {
+                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat, int phases) {
+    const bool do_build = (phases & kNphjBuild) != 0, do_probe = (phases & kNphjProbe) != 0;
     const unsigned long long cap = nphj_cap(nR, load);
     if (cap * 16 + 256 + (mat ? (unsigned long long)nR * 8 : 0ull) > table_bytes) return HJ_E_INVAL;
     NphjArgs a;
@@ -716,11 +717,12 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         const int rc = nphj_prepare_device();
         if (rc) return rc;
     }
+    const int grid = num_sms * 8;
+    uint32_t nl = 0;
+    if (do_build) {
     if (!a.compact_ok) HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
     HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
     HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));
-    const int grid = num_sms * 8;
-    uint32_t nl = 0;
     // Phase slots: build spans [0, 1], probe spans [4, 5]; the others stay empty.
     if (ph) HJ_CU(cudaEventRecord(ph[0], st));
     if (a.compact_ok) {
@@ -747,24 +749,32 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         nphj_lp_refill<<<grid, 256, 0, st>>>(a);
         nphj_lp_dedup_build<<<grid, 256, 0, st>>>(a);
         nphj_lp_resolve<<<grid, 256, 0, st>>>(a);
+        nl += 3;
     }
     HJ_CU(cudaGetLastError());
+    }  // do_build
+    if (!do_probe) {
+        if (launches) *launches = nl;
+        return HJ_OK;
+    }
     if (ev_mid) HJ_CU(cudaEventRecord(ev_mid, st));
     if (ph) {
         for (int i = 1; i <= 4; i++) HJ_CU(cudaEventRecord(ph[i], st));
     }
-    if (mat) {
-        nphj_probe_mat<<<grid, 256, 0, st>>>(a);
-    } else {
-        nphj_probe<<<grid, 256, 0, st>>>(a);
-        if (a.compact_ok) nphj_probe_compact<<<grid, 256, 0, st>>>(a);
+    if (nS) {
+        if (mat) {
+            nphj_probe_mat<<<grid, 256, 0, st>>>(a);
+        } else {
+            nphj_probe<<<grid, 256, 0, st>>>(a);
+            if (a.compact_ok) nphj_probe_compact<<<grid, 256, 0, st>>>(a);
+        }
     }
     HJ_CU(cudaGetLastError());
     if (ph) {
         HJ_CU(cudaEventRecord(ph[5], st));
         HJ_CU(cudaEventRecord(ph[6], st));
     }
-    if (launches) *launches = lp ? 5u : nl + (a.compact_ok ? 2u : 1u);
+    if (launches) *launches = nl + (nS ? (mat || !a.compact_ok ? 1u : 2u) : 0u);
     return HJ_OK;
 }
 

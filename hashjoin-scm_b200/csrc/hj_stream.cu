@@ -7,7 +7,13 @@
 // device buffers: the copy of chunk k+1 (its own stream) overlaps the join of chunk k. Every chunk is
 // joined with all of R by the ordinary pipeline and the counts and checksums add up, so the result is
 // hj_join's: every-match joins sum over chunks, and first-match joins pick per probe tuple the first R
-// tuple in input order, which does not depend on how S is cut.
+// tuple in input order, which does not depend on how S is cut. Non-partitioned joins build their table
+// from R once and only probe it per chunk.
+//
+// The overlap needs S in pinned (page-locked) host memory: cudaHostAlloc'd, or registered once by the
+// caller with cudaHostRegister. From pageable memory the driver stages each chunk's copy through its own
+// pinned buffers and the copies no longer run beside the joins (the result is the same). The join does
+// not register S itself: pinning tens of GB takes longer than the copies it would speed up.
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -134,6 +140,15 @@ extern "C" int hj_join_streamed(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *
     cudaEventRecord(consumed[1], st);
     const size_t nchunks = (nS + chunk - 1) / chunk;
     uint32_t launches = 0;
+    const bool nphj = !hj::algo_is_phj(algo);
+    const size_t table_bytes = c->arena_bytes - (size_t)(scratch - c->arena);
+    if (nphj) {
+        // The table is built once, from R alone, while the first chunk is copied.
+        uint32_t l = 0;
+        rc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, nullptr, 0, scratch, table_bytes, p.table_load, acc,
+                              st, nullptr, c->num_sms, nullptr, &l, nullptr, hj::kNphjBuild);
+        launches += l;
+    }
     for (size_t k = 0; k < nchunks && !rc; k++) {
         const int b = (int)(k & 1);
         const size_t lo = k * chunk, len = nS - lo < chunk ? nS - lo : chunk;
@@ -156,9 +171,8 @@ extern "C" int hj_join_streamed(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *
             rc = hj::phj_enqueue(g, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, buf[b], len, s, acc, st,
                                  nullptr, c->num_sms, nullptr, &l);
         } else {
-            rc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, buf[b], len, scratch,
-                                  c->arena_bytes - (size_t)(scratch - c->arena), p.table_load, acc, st, nullptr,
-                                  c->num_sms, nullptr, &l);
+            rc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, buf[b], len, scratch, table_bytes, p.table_load,
+                                  acc, st, nullptr, c->num_sms, nullptr, &l, nullptr, hj::kNphjProbe);
         }
         launches += l;
         if (!rc && cudaEventRecord(consumed[b], st) != cudaSuccess) rc = HJ_E_DEVICE;
