@@ -80,7 +80,7 @@ struct NphjArgs {
     int skip0;  // key 0 never matches (the phj_radix_lp rule)
     unsigned long long *side_pos;  // materialising joins: input positions of the side record's tuples
     MatOut mat;
-    int compact_ok;  // the algorithm may use compact slots (nphj_sc, not materialising)
+    int compact_ok;  // the join may use compact slots (not materialising; key 0 may match)
     // Compact tables: capacity (a multiple of kSliceSlots) and the sliced build's buffers.
     unsigned long long ccap;
     unsigned int nslices;      // ccap / kSliceSlots; 0: no sliced build
@@ -93,6 +93,13 @@ struct NphjArgs {
 
 __device__ __forceinline__ bool compact_sliced(const NphjSide *side) {
     return *reinterpret_cast<const volatile unsigned int *>(&side->sliced) != 0;
+}
+
+// The join runs on the compact table: allowed, the widths fit, and for first-match joins the table is
+// built by slices (the sliced build keeps one slot per key, with the first build tuple in input order;
+// otherwise a first-match join uses the 16-byte table and its duplicate rebuild).
+__device__ __forceinline__ bool use_compact(const NphjArgs &a) {
+    return a.compact_ok && nphj_compact(a.side) && (!a.lp || compact_sliced(a.side));
 }
 
 __device__ __forceinline__ unsigned slice_of(unsigned long long key, unsigned long long ccap) {
@@ -240,7 +247,7 @@ __global__ void __launch_bounds__(1024) nphj_slice_plan(NphjArgs a, const uint32
 // wide for compact slots, the compact table when it is built by global CAS. A table built by slices
 // is written whole by nphj_slice_build.
 __global__ void nphj_clear_table(NphjArgs a) {
-    const bool compact = nphj_compact(a.side);
+    const bool compact = use_compact(a);
     if (compact && compact_sliced(a.side)) return;
     const unsigned long long words16 = compact ? a.ccap / 2 : a.cap;  // 16-byte units
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < words16;
@@ -270,8 +277,10 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_slice_scatter(NphjArgs a) 
         for (int u = 0; u < U; u++) {
             if (i0 + u * blockDim.x >= hi) continue;
             const uint32_t pos = atomicAdd(&sh_pos[slice_of(t[u].x, a.ccap)], 1u);
+            // Every match: key and row id. First match: key and input position (the slice build keeps
+            // the smallest position per key, then looks its row id up).
             if (pos < a.nR)
-                a.stage[pos] = (t[u].x << 32) | t[u].y;
+                a.stage[pos] = (t[u].x << 32) | (a.lp ? i0 + u * blockDim.x : t[u].y);
             else
                 set_error(&a.acc->error, kErrBounds);
         }
@@ -280,6 +289,9 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_slice_scatter(NphjArgs a) 
 
 // One slice at a time per CTA: its build tuples claim slots of a shared-memory table by CAS, probing
 // inside the slice; then the whole slice, empty slots included, is written to the global table.
+// First-match joins: a tuple whose key already has a slot lowers the slot's position (64-bit min on
+// key << 32 | position), and before the write-out each slot's position is replaced by the row id of
+// that build tuple.
 __global__ void __launch_bounds__(kSliceThreads) nphj_slice_build(NphjArgs a) {
     extern __shared__ unsigned long long tab[];  // [kSliceSlots]
     if (!compact_sliced(a.side)) return;
@@ -296,7 +308,13 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_slice_build(NphjArgs a) {
             for (unsigned steps = 0;;) {
                 const unsigned long long cur = atomicCAS(&tab[h], kCompactEmpty, v);
                 if (cur == kCompactEmpty) break;
-                if ((cur >> 32) == k) seen_dup = true;
+                if ((cur >> 32) == k) {
+                    seen_dup = true;
+                    if (a.lp) {
+                        atomicMin(&tab[h], v);
+                        break;
+                    }
+                }
                 h = (h + 1) & (kSliceSlots - 1);
                 if (++steps >= kSliceSlots) {
                     set_error(&a.acc->error, kErrProbeLimit);
@@ -305,6 +323,28 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_slice_build(NphjArgs a) {
             }
         }
         __syncthreads();
+        if (a.lp) {
+            // Positions -> row ids; eight gathers in flight per thread.
+            constexpr int G = 8;
+            for (unsigned j0 = threadIdx.x; j0 < kSliceSlots; j0 += G * blockDim.x) {
+                unsigned long long w[G], rid[G];
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const unsigned j = j0 + g * blockDim.x;
+                    w[g] = j < kSliceSlots ? tab[j] : kCompactEmpty;
+                    const unsigned long long p = w[g] & 0xffffffffull;
+                    rid[g] = (w[g] != kCompactEmpty && p < a.nR) ? a.R[p].y : 0ull;
+                }
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const unsigned j = j0 + g * blockDim.x;
+                    if (j >= kSliceSlots || w[g] == kCompactEmpty) continue;
+                    if ((w[g] & 0xffffffffull) >= a.nR) set_error(&a.acc->error, kErrBounds);
+                    tab[j] = (w[g] & ~0xffffffffull) | rid[g];
+                }
+            }
+            __syncthreads();
+        }
         ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(ctab + (size_t)sl * kSliceSlots);
         const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(tab);
         for (unsigned j = threadIdx.x; j < kSliceSlots / 2; j += blockDim.x) dst[j] = src[j];
@@ -366,7 +406,7 @@ __global__ void nphj_build(NphjArgs a) {
     constexpr int U = 4;
     bool seen_dup = false;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    if (a.compact_ok && nphj_compact(a.side)) {
+    if (use_compact(a)) {
         if (compact_sliced(a.side)) return;  // nphj_slice_build built the table
         unsigned long long *ctab = reinterpret_cast<unsigned long long *>(a.table);
         for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < a.nR;
@@ -403,14 +443,14 @@ __global__ void nphj_build(NphjArgs a) {
 
 // Duplicate-key rebuild for nphj_lp: one slot per distinct key holding the minimum input position.
 __global__ void nphj_lp_refill(NphjArgs a) {
-    if (!(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
+    if (use_compact(a) || !(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.cap;
          i += (unsigned long long)gridDim.x * blockDim.x)
         a.table[i] = make_ulonglong2(kEmpty, kEmpty);
 }
 
 __global__ void nphj_lp_dedup_build(NphjArgs a) {
-    if (!(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
+    if (use_compact(a) || !(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.nR;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const unsigned long long k = a.R[i].x;
@@ -435,7 +475,7 @@ __global__ void nphj_lp_dedup_build(NphjArgs a) {
 }
 
 __global__ void nphj_lp_resolve(NphjArgs a) {
-    if (!(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
+    if (use_compact(a) || !(*reinterpret_cast<volatile unsigned int *>(&a.side->dup))) return;
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < a.cap;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         tuple_v s = a.table[i];
@@ -452,12 +492,12 @@ __global__ void nphj_lp_resolve(NphjArgs a) {
 // 8-byte slots leave the registers for it.
 __global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
     __shared__ unsigned long long red[64];
-    if (!(a.compact_ok && nphj_compact(a.side))) return;
+    if (!use_compact(a)) return;
     // Compact slots: no build key is the empty pattern, so there is no side record; a probe key
     // at or above 2^32 - 1 cannot match.
     constexpr int V = 4;
     const unsigned long long *ctab = reinterpret_cast<const unsigned long long *>(a.table);
-    const bool first_only = *reinterpret_cast<volatile unsigned int *>(&a.side->dup) == 0;
+    const bool first_only = a.lp || *reinterpret_cast<volatile unsigned int *>(&a.side->dup) == 0;
     const bool sliced = compact_sliced(a.side);
     const unsigned long long max_steps = sliced ? kSliceSlots : a.ccap;
     unsigned long long cnt = 0, sum = 0;
@@ -508,7 +548,7 @@ __global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
 __global__ void __launch_bounds__(256, 8) nphj_probe(NphjArgs a) {
     __shared__ unsigned long long red[64];
     constexpr int U = 2;
-    if (a.compact_ok && nphj_compact(a.side)) return;  // nphj_probe_compact probes instead
+    if (use_compact(a)) return;  // nphj_probe_compact probes instead
     ProbeArgs P;
     P.table = a.table;
     P.cap = a.cap;
@@ -688,7 +728,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     a.mat = mat ? *mat : MatOut{nullptr, 0};
     // Compact slots pay off once the 16-byte table outgrows a share of L2; below that the extra pass
     // over R costs more than it saves.
-    a.compact_ok = (!lp && !mat && cap * 16 > kCompactMinTableBytes) ? 1 : 0;
+    a.compact_ok = (!mat && !skip0 && cap * 16 > kCompactMinTableBytes) ? 1 : 0;
     // Compact table: capacity rounded up to whole slices; behind it (inside the 16-byte table's bytes)
     // the sliced build's staging array, histograms and slice starts.
     a.ccap = (cap + kSliceSlots - 1) / kSliceSlots * kSliceSlots;

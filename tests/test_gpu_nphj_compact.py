@@ -1,6 +1,6 @@
 """GPU parity of the non-partitioned join's two slot layouts. When its 16-byte table would exceed 64 MB
-(over 2^21 build tuples), nphj_sc packs a build tuple into one 8-byte slot if every build key is below
-2^32 - 1 and every build row id below 2^32, and uses 16-byte slots otherwise; both must give the
+(over 2^21 build tuples), nphj_sc and nphj_lp pack a build tuple into one 8-byte slot if every build key
+is below 2^32 - 1 and every build row id below 2^32, and use 16-byte slots otherwise; both must give the
 oracle's result bit for bit, at and around the limits."""
 import numpy as np
 import pytest
@@ -62,7 +62,7 @@ def test_compact_slots_duplicates(hj, oracle, cuda):
     R = rel(rng.integers(0, 1 << 20, nR), rng.integers(0, 2**32, nR))
     S = rel(rng.integers(0, 5 << 18, 1 << 20), rng.integers(0, 2**64 - 1, 1 << 20, dtype=np.uint64))
     check(hj, oracle, cuda, R, S)
-    # nphj_lp keeps the 16-byte layout (first match in input order)
+    # nphj_lp: compact slots built by slices, one slot per key holding the first build tuple in input order
     check(hj, oracle, cuda, R, S, "nphj_lp")
 
 
@@ -100,3 +100,6 @@ def test_sliced_build_and_its_fallback(hj, oracle, cuda):
         probe[::101] = np.uint64(123456789)
         S = rel(probe, rng.integers(0, 2**64 - 1, nS, dtype=np.uint64))
         check(hj, oracle, cuda, rel(k, rids), S)
+        # first match: the sliced build keeps the first build tuple per key; the fallback is the 16-byte
+        # table with its duplicate rebuild
+        check(hj, oracle, cuda, rel(k, rids), S, "nphj_lp")

@@ -2,7 +2,8 @@
 nphj_widths, nphj_slice_colscan, nphj_slice_plan, nphj_slice_scatter, nphj_slice_build and the probe's
 slice wrap), run before the kernels ever touch a GPU: every staging write lands inside [0, |R|) exactly
 once, each slice holds only its own keys, no slice overflows its slots, and probing inside slices gives
-the oracle's result."""
+the oracle's result, for every-match joins (staged key and row id) and first-match joins (staged key and
+input position, smallest position kept per key, then its row id)."""
 import numpy as np
 import pytest
 
@@ -20,7 +21,7 @@ def table_hash(key, cap):
     return (h * cap) >> 64
 
 
-def sliced_join(R, S, hist_blocks):
+def sliced_join(R, S, hist_blocks, lp=False):
     nR = R.shape[0]
     cap = int(nR / 0.5) + 2
     ccap = (cap + SLICE - 1) // SLICE * SLICE
@@ -50,7 +51,7 @@ def sliced_join(R, S, hist_blocks):
             p = int(pos[sl[i]])
             pos[sl[i]] += 1
             assert 0 <= p < nR and stage[p] is None
-            stage[p] = (keys[i] << 32) | rids[i]
+            stage[p] = (keys[i] << 32) | (i if lp else rids[i])
     assert all(v is not None for v in stage)
     # nphj_slice_build: per slice, linear probing inside the slice
     table = [None] * ccap
@@ -60,12 +61,18 @@ def sliced_join(R, S, hist_blocks):
             assert table_hash(k, ccap) >> SLICE_LOG == s
             h = table_hash(k, ccap) & (SLICE - 1)
             for _ in range(SLICE):
-                if table[s * SLICE + h] is None:
+                cur = table[s * SLICE + h]
+                if cur is None:
                     table[s * SLICE + h] = v
+                    break
+                if lp and cur >> 32 == k:  # first match: the smallest position per key
+                    table[s * SLICE + h] = min(cur, v)
                     break
                 h = (h + 1) & (SLICE - 1)
             else:
                 raise AssertionError("slice overflow")
+    if lp:  # positions -> row ids
+        table = [None if e is None else (e & ~0xFFFFFFFF) | rids[e & 0xFFFFFFFF] for e in table]
     # probe with the slice wrap (every match: nphj_sc)
     cnt = csum = 0
     for k, r in zip(S[:, 0], S[:, 1]):
@@ -80,13 +87,16 @@ def sliced_join(R, S, hist_blocks):
             if e >> 32 == k:
                 cnt += 1
                 csum = (csum + (e & 0xFFFFFFFF) + r) & M64
+                if lp:
+                    break
             h = (h & ~(SLICE - 1)) | ((h + 1) & (SLICE - 1))
     return cnt, csum
 
 
+@pytest.mark.parametrize("lp", [False, True])
 @pytest.mark.parametrize("nR,nS,hist_blocks,dups", [(20_000, 50_000, 7, False), (30_001, 40_000, 296, True),
                                                     (8_192, 20_000, 1, True)])
-def test_sliced_build_index_arithmetic(oracle, nR, nS, hist_blocks, dups):
+def test_sliced_build_index_arithmetic(oracle, nR, nS, hist_blocks, dups, lp):
     rng = np.random.default_rng(nR)
     R = np.empty((nR, 2), dtype=np.uint64)
     R[:, 0] = rng.integers(1, nR // 3 if dups else 1 << 31, nR, dtype=np.uint64)
@@ -95,4 +105,4 @@ def test_sliced_build_index_arithmetic(oracle, nR, nS, hist_blocks, dups):
     S[:, 0] = R[rng.integers(0, nR, nS), 0]
     S[::9, 0] = rng.integers(1, 1 << 33, S[::9].shape[0], dtype=np.uint64)
     S[:, 1] = rng.integers(0, 1 << 40, nS, dtype=np.uint64)
-    assert sliced_join(R, S, hist_blocks) == oracle.join("nphj_sc", R, S)
+    assert sliced_join(R, S, hist_blocks, lp) == oracle.join("nphj_lp" if lp else "nphj_sc", R, S)
