@@ -64,6 +64,7 @@ HJ_RES_COMPACT_PARTITIONS = 0x1
 HJ_F_PHASE_TIMES = 0x4
 HJ_F_SEGMENTS = 0x20  # radix joins counting every match: segment mode at any size
 HJ_F_EXACT = 0x40     # radix joins: always the histogram pass and exact pass-1 offsets
+HJ_F_WIDE = 0x80      # radix joins: 16-byte tuples in every partition pass (no 8-byte words)
 PHASES = ("hist", "plan", "pass1", "pass2", "join", "large")
 
 

@@ -36,6 +36,7 @@ constexpr int kScatterThreads = 256;
 constexpr int kScatterItems = 8;
 constexpr int kScatterBufs = 2;       // tile buffers per CTA (2: double-buffered TMA loads)
 constexpr int kScatterCtasPerSm = 3;  // resident scatter CTAs per SM (registers and shared memory)
+constexpr int kScatterWordCtasPerSm = 2;  // pass 2 over 8-byte words: 16 words per thread, up to 128 registers
 constexpr int kTile = kScatterThreads * kScatterItems;  // tuples per partition tile
 constexpr int kJoinThreads = 1024;
 constexpr int kSmemCap = 10240;        // largest build partition joined in shared memory

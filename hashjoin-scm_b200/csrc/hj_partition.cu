@@ -104,6 +104,22 @@ __device__ __forceinline__ bool ci_applies(const uint32_t *counters, int bits) {
     return (mx[0] >> bits) < (1ull << 31) && mx[1] < (1ull << 32) && mx[2] < (1ull << 32);
 }
 
+// Segment mode can go further: pass 1 stores (key >> b1) << 32 | row id (w8_word) in segments of 4096
+// words (the same 32 KB as 2048 tuples) when every build key >> b1 is below 2^31 and every row id below
+// 2^32; pass 2 then reads 8-byte words in tiles of 4096 and writes compact final partitions. A probe
+// key whose key >> b1 does not fit keeps its low 31 bits and gets bit 31 set: its pass-2 digit stays
+// right, and after pass 2's shift its high part is still above every build key's.
+__device__ __forceinline__ bool w8_fits(const uint32_t *counters, int b1) {
+    const unsigned long long *mx = reinterpret_cast<const unsigned long long *>(counters + kCtrMaxKey);
+    return (mx[0] >> b1) < (1ull << 31) && mx[1] < (1ull << 32) && mx[2] < (1ull << 32);
+}
+
+__device__ __forceinline__ unsigned long long w8_word(unsigned long long key, unsigned long long rid, int b1) {
+    const unsigned long long hi = key >> b1;
+    const unsigned long long h32 = hi < (1ull << 31) ? hi : (0x80000000ull | (hi & 0x7fffffffull));
+    return (h32 << 32) | (rid & 0xffffffffull);
+}
+
 __device__ __forceinline__ unsigned long long ci_word(unsigned long long key, unsigned long long rid, int bits) {
     const unsigned long long hi = key >> bits;
     return ((hi < 0xffffffffull ? hi : 0xffffffffull) << 32) | (rid & 0xffffffffull);
@@ -604,6 +620,9 @@ struct ScatterArgs {
     // 8-byte words (ci_word) at outR8 / outS8 instead of tuples at outR / outS.
     int ci_out;
     unsigned long long *outR8, *outS8;
+    // Segment mode after a pass 1 that may have written 8-byte words: 1 = this launch reads words (runs
+    // when w8_fits holds), 2 = this launch reads tuples (runs when it does not); 0 = no such pass 1.
+    int w8;
 };
 
 // A tile claimed for processing: its source, length, output region and owning work item.
@@ -727,7 +746,8 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
         it.done = it.len;
     }
     s.item = it.item;
-    s.in = a.seg_head ? it.in + (uint64_t)it.seg * T : it.in + it.done;
+    // A segment is kTile tuples (32 KB) in either layout; T counts the launch's elements per tile.
+    s.in = a.seg_head ? it.in + (uint64_t)it.seg * kTile : it.in + it.done;
     s.out = it.out;
     s.out_len = it.out_len;
     s.cnt = (uint32_t)(it.len - it.done < (uint64_t)T ? it.len - it.done : (uint64_t)T);
@@ -744,12 +764,46 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
 // and the joins that count every match do not depend on their order.
 // NBUF = 2: the next tile streams into a second buffer while this one is processed; NBUF = 1: one
 // buffer per CTA, the CTAs of an SM overlap each other's loads instead.
-template <int THREADS, int ITEMS, bool STABLE, int NBUF, int MINB>
+// Store one element of the last pass: a tuple, its compact final word (ci), or - from an 8-byte word of
+// a segment-mode pass 1, which holds key >> b1 - the final word with key >> bits.
+__device__ __forceinline__ void store_elem(const tuple_v &t, tuple_v *out, unsigned long long *out8, long long dst,
+                                           bool ci, int bits, int) {
+    if (ci)
+        st_stream8(out8 + dst, ci_word(t.x, t.y, bits));
+    else
+        st_stream(out + dst, t);
+}
+__device__ __forceinline__ void store_elem(unsigned long long w, tuple_v *, unsigned long long *out8, long long dst,
+                                           bool, int, int b2) {
+    st_stream8(out8 + dst, (((w >> 32) >> b2) << 32) | (w & 0xffffffffull));
+}
+
+// Elements of a tile: 16-byte tuples, or (WIN) the 8-byte words of a segment-mode pass 1 (w8_word).
+template <bool WIN>
+struct ScatterElem {
+    using type = tuple_v;
+};
+template <>
+struct ScatterElem<true> {
+    using type = unsigned long long;
+};
+
+// Digit of an element in this pass: (key >> shift) & mask; a word holds key >> b1, which is pass 2's shift.
+__device__ __forceinline__ uint32_t elem_digit(const tuple_v &v, int shift, uint64_t dmask) {
+    return (uint32_t)((v.x >> shift) & dmask);
+}
+__device__ __forceinline__ uint32_t elem_digit(unsigned long long v, int, uint64_t dmask) {
+    return (uint32_t)((v >> 32) & dmask);
+}
+
+template <int THREADS, int ITEMS, bool STABLE, int NBUF, int MINB, bool WIN = false>
 __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
+    static_assert(!(WIN && STABLE), "8-byte-word tiles only for joins that count every match");
+    using E = typename ScatterElem<WIN>::type;
     constexpr int T = THREADS * ITEMS;
     constexpr int NW = THREADS / 32;
     extern __shared__ __align__(128) unsigned char smem[];
-    tuple_v *inbuf = reinterpret_cast<tuple_v *>(smem);                // [NBUF][T]
+    E *inbuf = reinterpret_cast<E *>(smem);                              // [NBUF][T]
     long long *gbase = reinterpret_cast<long long *>(inbuf + NBUF * T);  // [256]
     long long *running = gbase + 256;                                   // [256]
     uint32_t *tdstart = reinterpret_cast<uint32_t *>(running + 256);    // [256]
@@ -770,6 +824,8 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     const uint32_t bar0 = smem_addr(&bars[0]);
     const int nbins = 1 << a.bits;
     const bool ci = a.ci_out && ci_applies(a.counters, a.bits);
+    const int b2 = a.bits - a.b1;
+    if (a.w8 && (a.w8 == 1) != w8_fits(a.counters, a.b1)) return;  // the other layout's launch runs
     __shared__ ItemIter it;  // used by thread 0 only
     uint32_t pend = 0;       // thread 0: next segment of the chain (segment mode)
     ItemAhead ah;            // thread 0: the item claimed ahead
@@ -788,7 +844,8 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         if (NBUF == 2) {
             const TileSlot s0 = next_tile<T>(a, it, nitems, pend, ah);
             slots[0] = s0;
-            if (s0.item != ~0u && !(a.test_stall && blockIdx.x == 0)) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
+            if (s0.item != ~0u && !(a.test_stall && blockIdx.x == 0))
+                tma_load_1d(inbuf, s0.in, s0.cnt * (uint32_t)sizeof(E), bar0);
         }
     }
     __syncthreads();
@@ -802,19 +859,20 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
                 const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
                 slots[0] = sn;
                 if (sn.item != ~0u && !(a.test_stall && blockIdx.x == 0 && k == 0))
-                    tma_load_1d(inbuf, sn.in, sn.cnt * 16u, bar0);
+                    tma_load_1d(inbuf, sn.in, sn.cnt * (uint32_t)sizeof(E), bar0);
             }
             __syncthreads();
         }
         const TileSlot sl = slots[cur];
         if (sl.item == ~0u) break;
-        tuple_v *buf = inbuf + (size_t)cur * T;
+        E *buf = inbuf + (size_t)cur * T;
         // Prefetch the next tile into the other buffer; the barrier that ended the previous iteration
         // ordered every read of it before this copy.
         if (NBUF == 2 && tid == 0) {
             const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
             slots[cur ^ 1u] = sn;
-            if (sn.item != ~0u) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
+            if (sn.item != ~0u)
+                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * (uint32_t)sizeof(E), bar0 + 8u * (cur ^ 1u));
         }
         // First tile of a work item: load the item's per-digit output offsets.
         if (sl.first && tid < F) {
@@ -847,17 +905,17 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             break;
         }
 
-        // Tuples of this tile: warp w owns [w*32*ITEMS, (w+1)*32*ITEMS), one 512-byte row per item.
-        tuple_v v[ITEMS];
+        // Elements of this tile: warp w owns [w*32*ITEMS, (w+1)*32*ITEMS), one row of 32 per item.
+        E v[ITEMS];
         uint32_t d[ITEMS];
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
             if (idx < cnt) {
                 v[i] = buf[idx];
-                d[i] = (uint32_t)((v[i].x >> a.shift) & dmask);
+                d[i] = elem_digit(v[i], a.shift, dmask);
             } else {
-                v[i] = make_ulonglong2(0, 0);
+                v[i] = E{};
                 d[i] = (uint32_t)F;
             }
         }
@@ -948,7 +1006,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
             if (idx < cnt) {
-                const uint32_t di = (uint32_t)((v[i].x >> a.shift) & dmask);
+                const uint32_t di = elem_digit(v[i], a.shift, dmask);
                 const uint32_t pos = tdstart[di] + (STABLE ? whist[w * F + di] : 0u) + rk[i];
                 buf[pos] = v[i];
             }
@@ -961,39 +1019,29 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         if (cnt == (uint32_t)T) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
-                tuple_v t[ITEMS / 2];
+                E t[ITEMS / 2];
                 long long dst[ITEMS / 2];
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) t[i] = buf[tid + (hh * ITEMS / 2 + i) * THREADS];
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++)
-                    dst[i] = gbase[(uint32_t)((t[i].x >> a.shift) & dmask)] +
-                             (long long)(tid + (hh * ITEMS / 2 + i) * THREADS);
+                    dst[i] = gbase[elem_digit(t[i], a.shift, dmask)] + (long long)(tid + (hh * ITEMS / 2 + i) * THREADS);
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) {
-                    if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len) {
-                        if (ci)
-                            st_stream8(out8 + dst[i], ci_word(t[i].x, t[i].y, a.bits));
-                        else
-                            st_stream(sl.out + dst[i], t[i]);
-                    } else {
+                    if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len)
+                        store_elem(t[i], sl.out, out8, dst[i], ci, a.bits, b2);
+                    else
                         set_error(err, kErrBounds);
-                    }
                 }
             }
         } else
         for (uint32_t j = tid; j < cnt; j += THREADS) {
-            const tuple_v t = buf[j];
-            const uint32_t dd = (uint32_t)((t.x >> a.shift) & dmask);
-            const long long dst = gbase[dd] + (long long)j;
-            if (dst >= 0 && (uint64_t)dst < sl.out_len) {
-                if (ci)
-                    st_stream8(out8 + dst, ci_word(t.x, t.y, a.bits));
-                else
-                    st_stream(sl.out + dst, t);
-            } else {
+            const E t = buf[j];
+            const long long dst = gbase[elem_digit(t, a.shift, dmask)] + (long long)j;
+            if (dst >= 0 && (uint64_t)dst < sl.out_len)
+                store_elem(t, sl.out, out8, dst, ci, a.bits, b2);
+            else
                 set_error(err, kErrBounds);
-            }
         }
         __syncthreads();
     }
@@ -1025,6 +1073,8 @@ struct SegArgs {
     const tuple_v *R, *S;
     uint64_t nR, nS;
     int bits, F1;              // joint bins 2^bits; pass-1 digit = key & (F1 - 1)
+    int b1;                    // log2(F1)
+    int w8_first;              // a pass that wrote 8-byte words ran first: run only if w8_fits fails
     uint32_t it_tiles;         // tiles per work item
     uint32_t tilesR, tilesS;   // tiles of each relation
     uint32_t itemsR, items;    // items of R (first), all items
@@ -1093,10 +1143,15 @@ __device__ __forceinline__ void seg_flush(uint32_t *jh, uint32_t *row, int nbins
 }
 
 // K = ceil(F1 / 32): pass-1 digits per lane of warp 0, which keeps their segment state in registers.
-template <int THREADS, int ITEMS, int K>
+// W8: store 8-byte words (w8_word) in segments of 2 * kTile words (the same 32 KB); the launch that stores
+// tuples after it runs only when the widths did not allow words (w8_first).
+template <int THREADS, int ITEMS, int K, bool W8 = false>
 __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegArgs a) {
     constexpr int T = THREADS * ITEMS;
-    static_assert(T == kTile, "a segment holds one tile");
+    static_assert(T == kTile, "a tile fills one segment of tuples");
+    constexpr uint32_t SEGW = W8 ? 2 * T : T;  // elements per segment
+    if (!W8 && a.w8_first && w8_fits(a.counters, a.b1)) return;
+    unsigned long long *out8 = reinterpret_cast<unsigned long long *>(a.out);
     static_assert(K >= 1 && K <= 8, "at most 256 pass-1 digits");
     extern __shared__ __align__(128) unsigned char smem[];
     tuple_v *inbuf = reinterpret_cast<tuple_v *>(smem);              // [2][T]
@@ -1116,7 +1171,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
     const uint32_t G = gridDim.x, c = blockIdx.x;
     unsigned int *err = &a.counters[kCtrErr];
     const uint32_t bar0 = smem_addr(&bars[0]);
-    const uint64_t cap = (uint64_t)a.max_segs * T;
+    const uint64_t cap = (uint64_t)a.max_segs * SEGW;
 
     for (int j = tid; j < 256; j += THREADS) thist[j] = 0;
     for (int j = tid; j < (nbins >> 1); j += THREADS) jh[j] = 0;
@@ -1248,7 +1303,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
 #pragma unroll
             for (int j = 0; j < K; j++) {
                 hv[j] = d0 + j < F ? thist[d0 + j] : 0u;
-                const bool nw = hv[j] && (scur[j] == kSegNone || sfill[j] + hv[j] > (uint32_t)T);
+                const bool nw = hv[j] && (scur[j] == kSegNone || sfill[j] + hv[j] > SEGW);
                 packed += hv[j] + (nw ? 0x10000u : 0u);
             }
             uint32_t incl = packed;
@@ -1291,8 +1346,8 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                     if (h) {
                         const uint32_t sc = scur[j], fill = sfill[j];
                         SegRun r;
-                        if (sc != kSegNone && fill + h <= (uint32_t)T) {
-                            r.base = (long long)sc * T + fill - ex;
+                        if (sc != kSegNone && fill + h <= SEGW) {
+                            r.base = (long long)sc * SEGW + fill - ex;
                             r.jump = 0;
                             r.split = ex + h;
                             sfill[j] = fill + h;
@@ -1303,25 +1358,25 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                                 if (sc == kSegNone) {
                                     // The whole run starts the chain.
                                     a.seg_head[((size_t)phase_rel * G + c) * F + d] = id;
-                                    r.base = (long long)id * T - ex;
+                                    r.base = (long long)id * SEGW - ex;
                                     r.jump = 0;
                                     r.split = ex + h;
                                     sfill[j] = h;
                                 } else {
                                     // The run fills the current segment, then goes on in segment
-                                    // id: staged index ex + (T - fill) lands at id * T.
+                                    // id: staged index ex + (SEGW - fill) lands at id * SEGW.
                                     a.seg_next[sc] = id;
-                                    r.base = (long long)sc * T + fill - ex;
+                                    r.base = (long long)sc * SEGW + fill - ex;
                                     r.jump = (int)id - (int)sc - 1;
-                                    r.split = ex + ((uint32_t)T - fill);
-                                    sfill[j] = h - ((uint32_t)T - fill);
+                                    r.split = ex + (SEGW - fill);
+                                    sfill[j] = h - (SEGW - fill);
                                 }
                                 scur[j] = id;
                             } else {
                                 // Cannot happen with the storage phj_carve reserves; the run's
                                 // stores fail their bounds check and report it.
                                 set_error(err, kErrCapacity);
-                                r.base = -(long long)cap - (long long)T;
+                                r.base = -(long long)cap - (long long)SEGW;
                                 r.jump = 0;
                                 r.split = ex + h;
                                 scur[j] = kSegNone;
@@ -1354,25 +1409,33 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 for (int i = 0; i < ITEMS / 2; i++) {
                     const uint32_t j = (uint32_t)(tid + (hh * ITEMS / 2 + i) * THREADS);
                     const SegRun r = runs[(uint32_t)t[i].x & dmask];
-                    dst[i] = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * T);
+                    dst[i] = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * SEGW);
                 }
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) {
-                    if (dst[i] >= 0 && (uint64_t)dst[i] < cap)
-                        st_stream(a.out + dst[i], t[i]);
-                    else
+                    if (dst[i] >= 0 && (uint64_t)dst[i] < cap) {
+                        if (W8)
+                            st_stream8(out8 + dst[i], w8_word(t[i].x, t[i].y, a.b1));
+                        else
+                            st_stream(a.out + dst[i], t[i]);
+                    } else {
                         set_error(err, kErrBounds);
+                    }
                 }
             }
         } else {
             for (uint32_t j = tid; j < cnt; j += THREADS) {
                 const tuple_v t = buf[j];
                 const SegRun r = runs[(uint32_t)t.x & dmask];
-                const long long dst = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * T);
-                if (dst >= 0 && (uint64_t)dst < cap)
-                    st_stream(a.out + dst, t);
-                else
+                const long long dst = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * SEGW);
+                if (dst >= 0 && (uint64_t)dst < cap) {
+                    if (W8)
+                        st_stream8(out8 + dst, w8_word(t.x, t.y, a.b1));
+                    else
+                        st_stream(a.out + dst, t);
+                } else {
                     set_error(err, kErrBounds);
+                }
             }
         }
         __syncthreads();
@@ -1391,6 +1454,15 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         if (kor) atomicOr(mx, kor);
         if (ror) atomicOr(mx + 1, ror);
         if (rors) atomicOr(mx + 2, rors);
+    }
+}
+
+// After a pass 1 that wrote 8-byte words: if the widths did not allow them, pass 1 runs again with
+// tuples, from fresh item and segment counters (its own CTAs zero their histogram rows).
+__global__ void seg_reset_if_wide(uint32_t *counters, int b1) {
+    if (threadIdx.x == 0 && !w8_fits(counters, b1)) {
+        counters[kCtrItem1] = 0;
+        counters[kCtrSegAlloc] = 0;
     }
 }
 
@@ -2244,6 +2316,17 @@ int phj_prepare_device() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
     HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 8>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 1, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 2, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 4, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 8, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+    HJ_CU(cudaFuncSetAttribute(
+        scatter_kernel<kScatterThreads, 2 * kScatterItems, false, kScatterBufs, kScatterWordCtasPerSm, true>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2276,6 +2359,12 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     const uint32_t nchunks = cg.cR + cg.cS;
     // A segment-mode scratch holds the segment storage, not the exact-offset pipeline's buffers.
     const bool segm = s.seg;
+    // 8-byte words in the partitions (compact final partitions, and in segment mode an 8-byte pass 1):
+    // joins without per-match output whose key 0 may match (all but the materialising ones and
+    // phj_radix_lp), unless the caller asked for tuples (test_flags bit 2), when the widths allow them
+    // (decided on the device).
+    const int ci_ok = (!mat && !skip0 && !(test_flags & 2)) ? 1 : 0;
+    const bool seg_words = segm && ci_ok;
     if (segm && (lp || g.passes != 2 || g.bits > kSegMaxBits)) return HJ_E_INVAL;
     {
         const int rc = phj_prepare_device();
@@ -2305,15 +2394,36 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         ga.hist = s.chunk_hist;
         ga.counters = s.counters;
         ga.test_stall = (test_flags & 1) ? 1 : 0;
+        ga.b1 = g.b1;
+        ga.w8_first = 0;
         const size_t sm = seg_smem_bytes(g.bits);
-        if (F1 <= 32)
-            seg_pass1_kernel<kScatterThreads, kScatterItems, 1><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
-        else if (F1 <= 64)
-            seg_pass1_kernel<kScatterThreads, kScatterItems, 2><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
-        else if (F1 <= 128)
-            seg_pass1_kernel<kScatterThreads, kScatterItems, 4><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
-        else
-            seg_pass1_kernel<kScatterThreads, kScatterItems, 8><<<s.seg_grid, kScatterThreads, sm, st>>>(ga);
+        auto launch_pass1 = [&](bool words) {
+#define HJ_SEG_LAUNCH(KK)                                                                                  \
+    if (words)                                                                                             \
+        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, true><<<s.seg_grid, kScatterThreads, sm, st>>>(ga); \
+    else                                                                                                   \
+        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, false><<<s.seg_grid, kScatterThreads, sm, st>>>(ga)
+            if (F1 <= 32) {
+                HJ_SEG_LAUNCH(1);
+            } else if (F1 <= 64) {
+                HJ_SEG_LAUNCH(2);
+            } else if (F1 <= 128) {
+                HJ_SEG_LAUNCH(4);
+            } else {
+                HJ_SEG_LAUNCH(8);
+            }
+#undef HJ_SEG_LAUNCH
+        };
+        if (seg_words) {
+            // Pass 1 in 8-byte words; if the widths turn out not to allow them, the counters are reset and
+            // pass 1 runs again with tuples (that launch returns at once otherwise).
+            launch_pass1(true);
+            seg_reset_if_wide<<<1, 32, 0, st>>>(s.counters, g.b1);
+            ga.w8_first = 1;
+            ga.test_stall = 0;
+            nlaunch += 2;
+        }
+        launch_pass1(false);
         HJ_CU(cudaGetLastError());
         nlaunch++;
     } else {
@@ -2342,9 +2452,6 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     pa.max_large = s.max_large;
     pa.large_table_words = s.large_table_words;
     pa.agg_ok = mat ? 0 : 1;
-    // Compact final partitions: joins without per-match output whose key 0 may match (every join but
-    // the materialising ones and phj_radix_lp), when the widths allow (decided on the device).
-    const int ci_ok = (!mat && !skip0) ? 1 : 0;
     plan_kernel<<<1, 1024, g.bits <= kPlanStageBits ? (size_t)2 * np * 4 : 0, st>>>(pa);
     {
         const int ut = F1 < 32 ? 32 : F1;
@@ -2390,6 +2497,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.ci_out = (pass == g.passes - 1) ? ci_ok : 0;
         sa.outR8 = reinterpret_cast<unsigned long long *>(out);
         sa.outS8 = sa.outR8 + nR;
+        sa.w8 = 0;
         if (lp) {
             // First-match joins need each final build partition in input order (the join keeps the
             // lowest position among equal keys), so the build relation's items take the stable rank.
@@ -2410,6 +2518,16 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
             if (all_items > r_items)
                 scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
                     <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+        } else if (segm && seg_words) {
+            // Pass 2 over the chains of an 8-byte pass 1: tiles of 4096 words (one segment); the tuple
+            // launch after it runs only if pass 1 had to fall back to tuples.
+            sa.w8 = 1;
+            scatter_kernel<kScatterThreads, 2 * kScatterItems, false, kScatterBufs, kScatterWordCtasPerSm, true>
+                <<<num_sms * kScatterWordCtasPerSm, kScatterThreads, scatter_smem, st>>>(sa);
+            nlaunch++;
+            sa.w8 = 2;
+            scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
+                <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
         } else {
             scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
                 <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);

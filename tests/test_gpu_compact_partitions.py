@@ -105,3 +105,28 @@ def test_headline_shape_uses_compact_partitions(hj, cuda):
         r = hj.join("phj_radix_bc", R, S, on_device=True, flags=flags)
         assert (r.matched_cnt, r.checksum) == hj.pkfk_closed_form(nR, nS)
         assert r.flags & hj.HJ_RES_COMPACT_PARTITIONS
+
+
+def test_segment_mode_word_pass1_and_its_fallback(hj, oracle, cuda):
+    """Segment mode stores pass 1 as 8-byte words when every build key >> b1 (7 of 14 bits here) is below
+    2^31; otherwise pass 1 runs again with tuples on the device (counters reset), and the final partitions
+    can still be compact (build keys >> 14 below 2^31). HJ_F_WIDE keeps tuples everywhere. Same results."""
+    R, S = rels(5)
+    # build keys in [2^38, 2^45): key >> 7 does not fit 31 bits, key >> 14 does
+    R2 = R.copy()
+    R2[:, 0] |= np.uint64(1 << 40)
+    S2 = S.copy()
+    S2[:, 0] |= np.uint64(1 << 40)
+    for RR, SS in ((R, S), (R2, S2)):
+        assert run(hj, oracle, cuda, "phj_radix_bc", RR, SS, hj.HJ_F_SEGMENTS)
+        assert not run(hj, oracle, cuda, "phj_radix_bc", RR, SS, hj.HJ_F_SEGMENTS | hj.HJ_F_WIDE)
+        assert not run(hj, oracle, cuda, "phj_radix_bc", RR, SS, hj.HJ_F_EXACT | hj.HJ_F_WIDE)
+    # probe keys whose key >> 7 does not fit: kept as non-matching words, their digits intact
+    S3 = S.copy()
+    S3[::3, 0] = np.uint64(((1 << 45) + 12345) << 7) | (S3[::3, 0] & np.uint64(0x3FFF))
+    assert run(hj, oracle, cuda, "phj_radix_bc", R, S3, hj.HJ_F_SEGMENTS)
+    # the stall hook still reports the expired wait with word passes
+    with pytest.raises(hj.JoinError) as e:
+        hj.join("phj_radix_bc", dev(cuda, R), dev(cuda, S), on_device=True, flags=hj.HJ_F_SEGMENTS | hj.HJ_F_TEST_STALL)
+    assert e.value.status == hj.HJ_E_TIMEOUT
+    assert run(hj, oracle, cuda, "phj_radix_bc", R, S, hj.HJ_F_SEGMENTS)  # the context recovers

@@ -3,16 +3,17 @@ hashjoin-scm_b200/csrc/hj_partition.cu, restated tile by tile in numpy): with pa
 items in an interleaved order, every store lands inside the segment storage, no slot is written twice,
 segment ids stay below the bound that phj_carve reserves (floor(n / 2048) + 2 * CTAs * F1 + 32 * CTAs),
 and walking each (CTA, relation, digit) chain for its histogram count returns exactly that CTA's tuples
-of that digit. No GPU is used."""
+of that digit. Segments hold 2048 tuples, or 4096 8-byte words when pass 1 stores words (the same 32 KB;
+pass 2 then reads one segment per 4096-word tile). No GPU is used."""
 import numpy as np
 import pytest
 
-T = 2048          # tuples per tile and per segment
+T = 2048          # tuples per pass-1 tile (and per segment of tuples)
 SLAB = 32         # segment ids a CTA takes from the global counter at once
 NONE = 0xFFFFFFFF
 
 
-def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
+def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False, segw=T):
     rng = np.random.default_rng(seed)
     hi = 50 if skew else 1 << 40
     rels = [rng.integers(1, hi, nR, dtype=np.uint64), rng.integers(1, hi, nS, dtype=np.uint64)]
@@ -20,8 +21,8 @@ def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
     tiles = [-(-nR // T), -(-nS // T)]
     itemsR = -(-tiles[0] // it_tiles)
     items = itemsR + -(-tiles[1] // it_tiles)
-    max_segs = (nR + nS) // T + 2 * G * F1 + G * SLAB
-    cap = max_segs * T
+    max_segs = (nR + nS) // T + 2 * G * F1 + G * SLAB  # reserved for 2048-tuple segments
+    cap = max_segs * segw
     out = np.full(cap, -1, dtype=np.int64)
     seg_head = np.full((2 * G, F1), -1, dtype=np.int64)
     seg_next = np.full(max_segs, -1, dtype=np.int64)
@@ -60,7 +61,7 @@ def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
         h = np.bincount(d, minlength=F1)
         order = np.argsort(d, kind="stable")  # staged tile, sorted by digit
         ex = np.concatenate([[0], np.cumsum(h)[:-1]])
-        need = [int(h[x] > 0 and (s["cur"][x] == NONE or s["fill"][x] + h[x] > T)) for x in range(F1)]
+        need = [int(h[x] > 0 and (s["cur"][x] == NONE or s["fill"][x] + h[x] > segw)) for x in range(F1)]
         ntot = sum(need)
         old_lo, old_rem, nb = s["lo"], s["rem"], 0
         if ntot:
@@ -80,8 +81,8 @@ def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
             if not hh:
                 continue
             sc, fill = s["cur"][x], s["fill"][x]
-            if sc != NONE and fill + hh <= T:
-                base[x], split[x] = sc * T + fill - e0, e0 + hh
+            if sc != NONE and fill + hh <= segw:
+                base[x], split[x] = sc * segw + fill - e0, e0 + hh
                 s["fill"][x] = fill + hh
                 continue
             sid = old_lo + e if e < old_rem else nb + (e - old_rem)
@@ -89,17 +90,17 @@ def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
             assert sid < max_segs, "segment id beyond the reserved storage"
             if sc == NONE:
                 seg_head[row, x] = sid
-                base[x], split[x] = sid * T - e0, e0 + hh
+                base[x], split[x] = sid * segw - e0, e0 + hh
                 s["fill"][x] = hh
             else:
                 seg_next[sc] = sid
-                base[x], jump[x], split[x] = sc * T + fill - e0, sid - sc - 1, e0 + (T - fill)
-                s["fill"][x] = hh - (T - fill)
+                base[x], jump[x], split[x] = sc * segw + fill - e0, sid - sc - 1, e0 + (segw - fill)
+                s["fill"][x] = hh - (segw - fill)
             s["cur"][x] = sid
         for j in range(cnt):
             src = int(order[j])
             x = int(d[src])
-            dst = base[x] + j + (0 if j < split[x] else jump[x] * T)
+            dst = base[x] + j + (0 if j < split[x] else jump[x] * segw)
             assert 0 <= dst < cap
             assert out[dst] == -1, "slot written twice"
             out[dst] = (rel << 40) | (lo + src)
@@ -112,8 +113,8 @@ def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
             sid, done = int(seg_head[row, x]), 0
             while done < want:
                 assert 0 <= sid < max_segs
-                k = min(T, want - done)
-                vals = out[sid * T:sid * T + k]
+                k = min(segw, want - done)
+                vals = out[sid * segw:sid * segw + k]
                 assert (vals >= 0).all(), "chain reaches an unwritten slot"
                 r = vals >> 40
                 idx = vals & ((1 << 40) - 1)
@@ -127,6 +128,7 @@ def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
     return alloc, max_segs
 
 
+@pytest.mark.parametrize("segw", [2048, 4096])
 @pytest.mark.parametrize("nR,nS,bits,F1,G,it_tiles,seed,skew", [
     (5000, 20000, 4, 4, 3, 1, 1, False),
     (100_000, 300_001, 6, 8, 5, 2, 2, False),
@@ -135,6 +137,6 @@ def emulate(nR, nS, bits, F1, G, it_tiles, seed, skew=False):
     (2048 * 7, 2048 * 9 + 5, 8, 16, 2, 16, 5, True),
     (300_000, 10, 10, 32, 7, 4, 6, False),       # almost only R; CTAs without S tiles
 ])
-def test_segment_chains(nR, nS, bits, F1, G, it_tiles, seed, skew):
-    used, bound = emulate(nR, nS, bits, F1, G, it_tiles, seed, skew)
+def test_segment_chains(nR, nS, bits, F1, G, it_tiles, seed, skew, segw):
+    used, bound = emulate(nR, nS, bits, F1, G, it_tiles, seed, skew, segw)
     assert used <= bound
