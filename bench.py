@@ -73,6 +73,8 @@ def parse_args():
     ap.add_argument("--passes", type=int, default=2)
     ap.add_argument("--pipeline", choices=["auto", "segments", "exact"], default="auto",
                     help="radix joins: segment mode (no histogram pass) by size, always, or never")
+    ap.add_argument("--wide", action="store_true",
+                    help="radix joins: 16-byte tuples in every partition pass (HJ_F_WIDE), no 8-byte words")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -305,7 +307,8 @@ def run_ours(a, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     want = hj.pkfk_closed_form(nR, nS)
     ctx = hj.Context(local_rank)
-    pipe_flag = {"auto": 0, "segments": hj.HJ_F_SEGMENTS, "exact": hj.HJ_F_EXACT}[a.pipeline]
+    pipe_flag = {"auto": 0, "segments": hj.HJ_F_SEGMENTS, "exact": hj.HJ_F_EXACT}[a.pipeline] | (
+        hj.HJ_F_WIDE if a.wide else 0)
     flags = hj.HJ_F_PHASE_TIMES | pipe_flag
 
     def step():
