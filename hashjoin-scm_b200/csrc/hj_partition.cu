@@ -788,6 +788,14 @@ struct ScatterElem<true> {
     using type = unsigned long long;
 };
 
+// Bytes a tile's bulk copy moves: a bulk copy's size must be a multiple of 16, so a word tile with an odd
+// count also copies the next word of its segment (segments hold 4096 words, so an odd count is at most
+// 4095 and the extra word stays inside the segment; it lands in an unused buffer slot).
+template <typename E>
+__device__ __forceinline__ uint32_t tile_copy_bytes(uint32_t cnt) {
+    return sizeof(E) == 16 ? cnt * 16u : ((cnt + 1u) & ~1u) * (uint32_t)sizeof(E);
+}
+
 // Digit of an element in this pass: (key >> shift) & mask; a word holds key >> b1, which is pass 2's shift.
 __device__ __forceinline__ uint32_t elem_digit(const tuple_v &v, int shift, uint64_t dmask) {
     return (uint32_t)((v.x >> shift) & dmask);
@@ -845,7 +853,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             const TileSlot s0 = next_tile<T>(a, it, nitems, pend, ah);
             slots[0] = s0;
             if (s0.item != ~0u && !(a.test_stall && blockIdx.x == 0))
-                tma_load_1d(inbuf, s0.in, s0.cnt * (uint32_t)sizeof(E), bar0);
+                tma_load_1d(inbuf, s0.in, tile_copy_bytes<E>(s0.cnt), bar0);
         }
     }
     __syncthreads();
@@ -859,7 +867,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
                 const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
                 slots[0] = sn;
                 if (sn.item != ~0u && !(a.test_stall && blockIdx.x == 0 && k == 0))
-                    tma_load_1d(inbuf, sn.in, sn.cnt * (uint32_t)sizeof(E), bar0);
+                    tma_load_1d(inbuf, sn.in, tile_copy_bytes<E>(sn.cnt), bar0);
             }
             __syncthreads();
         }
@@ -872,7 +880,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
             slots[cur ^ 1u] = sn;
             if (sn.item != ~0u)
-                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * (uint32_t)sizeof(E), bar0 + 8u * (cur ^ 1u));
+                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, tile_copy_bytes<E>(sn.cnt), bar0 + 8u * (cur ^ 1u));
         }
         // First tile of a work item: load the item's per-digit output offsets.
         if (sl.first && tid < F) {
@@ -1534,7 +1542,7 @@ constexpr size_t kCompactSmem = (size_t)kCompactCap * (4 + 4 + 2 + 2);
 // within a partition the low `bits` key bits are equal, so comparing key >> bits is comparing keys.
 // MAT: write one (r.row_id, s.row_id) pair per match (the ptr_* joins) instead of summing; the probe
 // then runs in block-wide rounds (count, reserve output slots, walk again and write).
-template <bool MAT>
+template <bool MAT, bool CI = false>
 __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t *rkey = reinterpret_cast<uint32_t *>(smem);         // [kCompactCap]
@@ -1549,7 +1557,9 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
     const int tid = threadIdx.x;
     unsigned int *err = &a.counters[kCtrErr];
     const uint32_t nA = a.counters[kCtrNItemsA];
-    const bool ci = !MAT && a.ci && ci_applies(a.counters, a.bits);
+    // Compiled once per partition layout; only the launch matching the device's choice runs.
+    if (CI != (!MAT && a.ci && ci_applies(a.counters, a.bits))) return;
+    constexpr bool ci = CI;
     const int B = ci ? 0 : a.bits;  // shift from a stored x to the key's bits above the radix bits
     const bool lp = a.lp != 0;
     const bool skip0 = a.skip0 != 0;
@@ -1681,7 +1691,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
 }
 
-template <bool MAT>
+template <bool MAT, bool CI = false>
 __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     tuple_v *rt = reinterpret_cast<tuple_v *>(smem);                      // [kSmemCap]
@@ -1701,7 +1711,9 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
     }
     __syncthreads();
     const uint32_t nitems = a.counters[kCtrNItems];
-    const bool ci = !MAT && a.ci && ci_applies(a.counters, a.bits);
+    // Compiled once per partition layout; only the launch matching the device's choice runs.
+    if (CI != (!MAT && a.ci && ci_applies(a.counters, a.bits))) return;
+    constexpr bool ci = CI;
     const int B = ci ? 0 : a.bits;  // shift from a stored x to the key's bits above the radix bits
     const bool lp = a.lp != 0;
     const bool skip0 = a.skip0 != 0;
@@ -2328,6 +2340,10 @@ int phj_prepare_device() {
         scatter_kernel<kScatterThreads, 2 * kScatterItems, false, kScatterBufs, kScatterWordCtasPerSm, true>,
         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
+    HJ_CU(cudaFuncSetAttribute(join_small_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kJoinSmem));
+    HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kCompactSmem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kCompactSmem));
@@ -2559,8 +2575,15 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         join_compact_kernel<true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
         join_small_kernel<true><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
     } else {
-        join_compact_kernel<false><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
-        join_small_kernel<false><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
+        // One launch per partition layout (tuples, compact words); the one that does not match the
+        // device's choice returns at once.
+        join_compact_kernel<false, false><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+        join_small_kernel<false, false><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
+        if (ci_ok) {
+            join_compact_kernel<false, true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+            join_small_kernel<false, true><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
+            nlaunch += 2;
+        }
     }
     HJ_CU(cudaGetLastError());
     HJ_PH(segm ? 4 : 5);
