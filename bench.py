@@ -349,17 +349,28 @@ def run_ours(a, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     step_s = ms / 1e3 / a.steps
     compact = bool(results[-1].flags & hj.HJ_RES_COMPACT_PARTITIONS)
+    words1 = bool(results[-1].flags & hj.HJ_RES_WORD_PASS1)
     if a.algo.startswith("phj"):
         P = results[-1].physical_passes
-        last_b = 24 if compact else 32
-        pass_b = [32, last_b] if P == 2 else [last_b]
+        # bytes per tuple of each pass: read + write; 8-byte words halve what a pass writes (and what the
+        # next pass reads)
+        if P == 2:
+            pass_b = [16 + (8 if words1 else 16), (8 if words1 else 16) + (8 if compact else 16)]
+        else:
+            pass_b = [16 + (8 if compact else 16)]
         pass_t = [phases["pass1"], phases["pass2"]] if P == 2 else [phases["pass1"]]
         scatter_bytes = sum(pass_b) / len(pass_b) * (nR + nS)  # per launch, averaged like the times
         pass_s = statistics.mean(pass_t)
         achieved = scatter_bytes / pass_s / 1e9
         prof = traffic_profile("scatter_kernel")
         traffic = prof["dram_bytes_per_tuple"] * (nR + nS) if prof else None
-        if seg_mode:
+        if seg_mode and words1:
+            # ncu traffic of the two passes with 8-byte words (profiles/segment_passes_words.json), per
+            # launch, averaged over the two passes like `achieved`
+            pw = traffic_profile("segment_passes_words")
+            traffic = ((pw["dram_bytes_per_tuple_pass1"] + pw["dram_bytes_per_tuple_pass2"]) / 2 * (nR + nS)
+                       if pw else None)
+        elif seg_mode:
             # per launch, averaged over the two passes like `achieved`
             p1 = traffic_profile("seg_pass1_kernel")
             key2 = "dram_bytes_per_tuple_pass2_compact" if compact else "dram_bytes_per_tuple_pass2"
@@ -374,6 +385,8 @@ def run_ours(a, rank, world, local_rank):
                     "per_pass": [{"bytes_per_tuple": b, "ms": t * 1e3, "gbs": b * (nR + nS) / t / 1e9,
                                   "frac": b * (nR + nS) / t / 1e9 / peak} for b, t in zip(pass_b, pass_t)]}
         per_tuple = sum(pass_b) + (8 if compact else 16)
+        # the same time against the 16-byte-tuple model of the survey (32 B per pass, 16 B for the join)
+        roofline["frac_of_tuple_model"] = (16 * (2 * P + 1) * (nR + nS) / step_s / 1e9) / peak
     else:
         per_tuple = 32
         join_bytes = per_tuple * (nR + nS)
@@ -384,7 +397,7 @@ def run_ours(a, rank, world, local_rank):
                     "algorithmic_bytes_per_launch": join_bytes, "launch_ms": step_s * 1e3}
     pipe_bytes = per_tuple * (nR + nS)
     pipeline = {"algorithmic_bytes_per_tuple": per_tuple, "bytes_per_step": pipe_bytes,
-                "compact_final_partitions": compact,
+                "compact_final_partitions": compact, "word_pass1": words1 if a.algo.startswith("phj") else False,
                 "achieved_gbs": pipe_bytes / step_s / 1e9, "frac": pipe_bytes / step_s / 1e9 / peak,
                 "phase_ms": {k: v * 1e3 for k, v in phases.items()}}
 

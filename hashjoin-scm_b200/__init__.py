@@ -61,6 +61,7 @@ HJ_E_NOT_FOUND, HJ_E_IO, HJ_E_OVERFLOW, HJ_E_BUDGET, HJ_E_CAPACITY, HJ_E_ROWID =
 HJ_F_NO_TIMING = 0x1
 HJ_F_PINNED_HOST = 0x2
 HJ_RES_COMPACT_PARTITIONS = 0x1
+HJ_RES_WORD_PASS1 = 0x2
 HJ_F_PHASE_TIMES = 0x4
 HJ_F_SEGMENTS = 0x20  # radix joins counting every match: segment mode at any size
 HJ_F_EXACT = 0x40     # radix joins: always the histogram pass and exact pass-1 offsets

@@ -1505,6 +1505,7 @@ struct JoinArgs {
     MatOut mat; // materialising joins (MAT kernels): where the (r.row_id, s.row_id) pairs go
     int ci;     // the final partitions may be compact words (when ci_applies holds) at finR8 / finS8
     const unsigned long long *finR8, *finS8;
+    int w8_b1;  // segment mode with a word pass 1: its shift (reported when w8_fits held); -1 otherwise
 };
 
 // A tuple of a final partition: the stored tuple, or for compact partitions {key >> bits, row id}.
@@ -1945,8 +1946,8 @@ __global__ void join_large_build(JoinArgs a) {
     const bool ci = a.ci && ci_applies(a.counters, a.bits);
     const int bshift = ci ? 0 : a.bits;
     if (a.counters[kCtrLargeAgg]) {
-        // Warp-uniform rounds: lanes holding equal keys (equal keys always share a partition) combine
-        // their count, row-id sum and smallest position first, so a hot key costs one update per warp.
+        // Warp-uniform rounds: lanes holding equal keys of one partition combine their count, row-id sum
+        // and smallest position first, so a hot key costs one update per warp.
         const unsigned lane = threadIdx.x & 31;
         for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); g0 < total;
              g0 += (uint64_t)gridDim.x * blockDim.x) {
@@ -1963,7 +1964,10 @@ __global__ void join_large_build(JoinArgs a) {
             }
             const unsigned act_mask = __ballot_sync(0xffffffffu, act);
             if (!act) continue;
-            const unsigned peers = __match_any_sync(act_mask, r.x);
+            // Group lanes by key and partition: a compact word holds only key >> bits, which keys of two
+            // partitions can share (full keys of different partitions differ in their low bits anyway).
+            const unsigned long long gkey = ci ? (r.x | ((unsigned long long)(unsigned)l << 32)) : r.x;
+            const unsigned peers = __match_any_sync(act_mask, gkey);
             // Row-id sum of the group in three pieces of at most 24 bits (32 addends cannot overflow them).
             const unsigned s0 = __reduce_add_sync(peers, (unsigned)(r.y & 0xffffffu));
             const unsigned s1 = __reduce_add_sync(peers, (unsigned)((r.y >> 24) & 0xffffffu));
@@ -2117,6 +2121,8 @@ __global__ void join_large_probe(JoinArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (nl) atomicAdd(&a.acc->large_parts, (unsigned long long)nl);
         if (ci) atomicOr(&a.acc->flags, (unsigned long long)HJ_RES_COMPACT_PARTITIONS);
+        if (a.w8_b1 >= 0 && w8_fits(a.counters, a.w8_b1))
+            atomicOr(&a.acc->flags, (unsigned long long)HJ_RES_WORD_PASS1);
     }
 }
 
@@ -2571,6 +2577,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     ja.ci = ci_ok;
     ja.finR8 = reinterpret_cast<const unsigned long long *>(s.tmp2);
     ja.finS8 = ja.finR8 + nR;
+    ja.w8_b1 = seg_words ? g.b1 : -1;
     if (mat) {
         join_compact_kernel<true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
         join_small_kernel<true><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);

@@ -125,6 +125,7 @@ constexpr int kSkipAheadWindow = 16;
 
 // Continuous batching.
 constexpr int kWaveLanes = 2;               // waves on the GPU at once
+constexpr double kServerWaveTableBytes = 1e9;  // table bytes of one wave unless the config's tuner says
 constexpr int kWaveMaxRequestsCap = 1024;   // the multi-join kernels stage count + 1 prefix sums in shared memory
 constexpr unsigned kWaveMaxChunks = 1u << 15;  // build chunks (and probe chunks) of one wave
 
@@ -622,7 +623,13 @@ int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out) {
         delete s;
         return rc;
     }
-    if (cfg->tuner.partition_target > 0) s->ctx->tuner = cfg->tuner;
+    if (cfg->tuner.partition_target > 0) {
+        s->ctx->tuner = cfg->tuner;
+    } else {
+        // Waves of served requests are sized for throughput, not for L2: a request's table averages
+        // ~16 MB on the served workload, so an L2-sized budget would cap waves at a few requests.
+        s->ctx->tuner.wave_table_bytes = kServerWaveTableBytes;
+    }
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(cfg->device);

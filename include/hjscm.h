@@ -144,6 +144,10 @@ typedef struct {
  * (key >> radix bits) << 32 | row id, which the joins read (radix joins without per-match output and
  * without the key-0 rule, when every build key >> radix bits is below 2^31 and every row id below 2^32). */
 #define HJ_RES_COMPACT_PARTITIONS 0x1u
+/* hj_result_t.flags: segment mode stored the pass-1 chains as 8-byte words (key >> pass-1 bits) << 32 |
+ * row id as well (every build key >> pass-1 bits below 2^31, every row id below 2^32), so pass 1 wrote
+ * 8 bytes per tuple and pass 2 read 8. */
+#define HJ_RES_WORD_PASS1 0x2u
 
 typedef struct hj_ctx hj_ctx_t;
 
