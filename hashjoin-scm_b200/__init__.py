@@ -517,7 +517,8 @@ class Batch:
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double),
                 ("autotune", ctypes.c_int), ("tuner", Tuner), ("small_request_tuples", ctypes.c_double),
-                ("large_sm_share", ctypes.c_double), ("waves", ctypes.c_int), ("wave_max_requests", ctypes.c_int)]
+                ("large_sm_share", ctypes.c_double), ("waves", ctypes.c_int), ("wave_max_requests", ctypes.c_int),
+                ("max_large_inflight", ctypes.c_int)]
 
 
 class Completion(ctypes.Structure):
@@ -566,7 +567,7 @@ class Server:
 
     def __init__(self, device: int = 0, slots: int = 8, hbm_budget_bytes: float = 150e9, autotune: bool = True,
                  tuner: dict | None = None, large_sm_share: float | None = None, waves: bool = True,
-                 wave_max_requests: int | None = None):
+                 wave_max_requests: int | None = None, max_large_inflight: int | None = None):
         L = _bind_server()
         cfg = ServerConfig()
         L.hj_server_config_init(ctypes.byref(cfg))
@@ -574,6 +575,8 @@ class Server:
         cfg.waves = int(waves)
         if wave_max_requests is not None:
             cfg.wave_max_requests = wave_max_requests
+        if max_large_inflight is not None:
+            cfg.max_large_inflight = max_large_inflight
         for k, v in (tuner or {}).items():
             setattr(cfg.tuner, k, v)
         if large_sm_share is not None:

@@ -758,6 +758,10 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         if (rc) return rc;
     }
     const int grid = num_sms * 8;
+    // Joins that may use compact slots launch the 16-byte-table kernels (and the table clear) as
+    // fallbacks that usually return at once; their grid is kept small, since a launch of idle blocks
+    // still costs time in proportion to the blocks.
+    const int fb_grid = a.compact_ok ? num_sms * 4 : grid;
     uint32_t nl = 0;
     if (do_build) {
     if (!a.compact_ok) HJ_CU(cudaMemsetAsync(table, 0xff, cap * 16, st));
@@ -774,7 +778,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
             nphj_slice_plan<<<1, 1024, 0, st>>>(a, slice_total);
             nl += 2;
         }
-        nphj_clear_table<<<grid, 256, 0, st>>>(a);
+        nphj_clear_table<<<num_sms * 2, 256, 0, st>>>(a);
         nl++;
         if (a.nslices) {
             nphj_slice_scatter<<<a.hist_blocks, kSliceThreads, hist_smem, st>>>(a);
@@ -783,12 +787,12 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
             nl += 2;
         }
     }
-    nphj_build<<<grid, 256, 0, st>>>(a);
+    nphj_build<<<fb_grid, 256, 0, st>>>(a);
     nl++;
     if (lp) {
-        nphj_lp_refill<<<grid, 256, 0, st>>>(a);
-        nphj_lp_dedup_build<<<grid, 256, 0, st>>>(a);
-        nphj_lp_resolve<<<grid, 256, 0, st>>>(a);
+        nphj_lp_refill<<<fb_grid, 256, 0, st>>>(a);
+        nphj_lp_dedup_build<<<fb_grid, 256, 0, st>>>(a);
+        nphj_lp_resolve<<<fb_grid, 256, 0, st>>>(a);
         nl += 3;
     }
     HJ_CU(cudaGetLastError());
@@ -805,7 +809,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         if (mat) {
             nphj_probe_mat<<<grid, 256, 0, st>>>(a);
         } else {
-            nphj_probe<<<grid, 256, 0, st>>>(a);
+            nphj_probe<<<fb_grid, 256, 0, st>>>(a);
             if (a.compact_ok) nphj_probe_compact<<<grid, 256, 0, st>>>(a);
         }
     }

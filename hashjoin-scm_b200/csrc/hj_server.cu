@@ -218,6 +218,9 @@ namespace {
 
 bool wave_eligible(const hj_server *s, const Request &r) { return s->cfg.waves && r.impl == 0 && r.nR && r.nS; }
 
+// Requests above small_request_tuples run on low-priority streams with kernels sized for a share of the SMs.
+bool is_large(const hj_server *s, const Request &r) { return (double)(r.nR + r.nS) > s->cfg.small_request_tuples; }
+
 int request_need(hj_server *s, Request &r) {
     hj_params_t p;
     hj_params_init(&p);
@@ -474,6 +477,8 @@ void worker_main(hj_server *s) {
             double w_tables = 0;
             int scanned = 0;
             bool blocked_seen = false;
+            int large_busy = 0;
+            for (Slot &sl : s->slots) large_busy += sl.busy && is_large(s, sl.req);
             for (auto it = s->queue.begin(); it != s->queue.end() && scanned < kSkipAheadWindow;) {
                 if (wave_eligible(s, *it)) {
                     if (free_lane && (int)wave.size() < wave_max) {
@@ -493,6 +498,12 @@ void worker_main(hj_server *s) {
                     // behind it could take: it neither blocks those nor counts toward the window.
                     ++it;
                     continue;
+                } else if (s->cfg.max_large_inflight > 0 && is_large(s, *it) &&
+                           large_busy >= s->cfg.max_large_inflight) {
+                    // Waits for the large request on the GPU to finish; like a request waiting for a
+                    // wave, it holds nothing back from the requests behind it.
+                    ++it;
+                    continue;
                 } else {
                     Slot *free_slot = nullptr;
                     for (Slot &sl : s->slots)
@@ -502,6 +513,7 @@ void worker_main(hj_server *s) {
                         }
                     size_t off = 0;
                     if (free_slot && s->pool.alloc(it->need, &off)) {
+                        large_busy += is_large(s, *it);
                         it->off = off;
                         it->start_s = t;
                         free_slot->req = *it;
@@ -609,12 +621,14 @@ int hj_server_config_init(hj_server_config_t *c) {
     c->large_sm_share = 0.75;
     c->waves = 1;
     c->wave_max_requests = 512;
+    c->max_large_inflight = 1;
     return HJ_OK;
 }
 
 int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out) {
     if (!cfg || !out || cfg->slots < 1 || cfg->slots > 256 || !(cfg->hbm_budget_bytes > 0)) return HJ_E_INVAL;
     if (cfg->waves && (cfg->wave_max_requests < 1 || cfg->wave_max_requests > kWaveMaxRequestsCap)) return HJ_E_INVAL;
+    if (cfg->max_large_inflight < 0) return HJ_E_INVAL;
     *out = nullptr;
     hj_server *s = new hj_server();
     s->cfg = *cfg;
