@@ -684,6 +684,9 @@ def run_serve_mode(a, rank, world, local_rank):
     # 2. sequential per-join loops on the same sequences
     loop_out = []
     with hj.Context(local_rank) as ctx:
+        # the same per-request decisions as the server's defaults (non-partitioned up to 16 MB tables)
+        hj.tuner_set(ctx, nphj_max_table_bytes=16e6)
+
         def decided(R, S):
             impl, bits, passes = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
             hj._bind_batch().hj_tuner_decide(ctx.handle, R.shape[0], S.shape[0], ctypes.byref(impl),

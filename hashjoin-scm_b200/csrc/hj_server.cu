@@ -126,6 +126,7 @@ constexpr int kSkipAheadWindow = 16;
 // Continuous batching.
 constexpr int kWaveLanes = 2;               // waves on the GPU at once
 constexpr double kServerWaveTableBytes = 1e9;  // table bytes of one wave unless the config's tuner says
+constexpr double kServerNphjTableBytes = 16e6; // largest non-partitioned table unless the config's tuner says
 constexpr int kWaveMaxRequestsCap = 1024;   // the multi-join kernels stage count + 1 prefix sums in shared memory
 constexpr unsigned kWaveMaxChunks = 1u << 15;  // build chunks (and probe chunks) of one wave
 
@@ -621,7 +622,7 @@ int hj_server_config_init(hj_server_config_t *c) {
     c->large_sm_share = 0.75;
     c->waves = 1;
     c->wave_max_requests = 512;
-    c->max_large_inflight = 1;
+    c->max_large_inflight = 0;
     return HJ_OK;
 }
 
@@ -641,8 +642,10 @@ int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out) {
         s->ctx->tuner = cfg->tuner;
     } else {
         // Waves of served requests are sized for throughput, not for L2: a request's table averages
-        // ~16 MB on the served workload, so an L2-sized budget would cap waves at a few requests.
+        // ~16 MB on the served workload, so an L2-sized budget would cap waves at a few requests. Joins
+        // whose table would exceed 16 MB run partitioned (on slots): the budget batches tune to.
         s->ctx->tuner.wave_table_bytes = kServerWaveTableBytes;
+        s->ctx->tuner.nphj_max_table_bytes = kServerNphjTableBytes;
     }
     int prev = -1;
     cudaGetDevice(&prev);

@@ -399,9 +399,7 @@ typedef struct {
     int waves;                   /* 1: coalesce non-partitioned requests into waves (default); 0: one slot
                                     per request */
     int wave_max_requests;       /* requests per wave (1..1024; default 512) */
-    int max_large_inflight;      /* larger requests on the GPU at once (default 1: a large join's persistent
-                                    kernels take their share of every SM, so two of them only queue
-                                    behind each other while waves wait for SMs); 0 = no limit */
+    int max_large_inflight;      /* larger requests on the GPU at once; 0 = no limit (default) */
 } hj_server_config_t;
 
 typedef struct {
@@ -427,8 +425,9 @@ typedef struct hj_server hj_server_t;
 
 /* Monotonic clock in seconds, the one completions are stamped with. */
 double hj_now(void);
-/* Defaults: device 0, 8 slots, 150e9 bytes, autotune, small requests up to 2^25 tuples, large requests
- * on 0.75 of the SMs and one at a time, waves of up to 512 requests. */
+/* Defaults: device 0, 8 slots, 150e9 bytes, autotune (non-partitioned joins up to 16 MB tables), small
+ * requests up to 2^25 tuples, large requests on 0.75 of the SMs, waves of up to 512 requests and 1e9
+ * bytes of tables. */
 int hj_server_config_init(hj_server_config_t *cfg);
 int hj_server_create(const hj_server_config_t *cfg, hj_server_t **out);
 int hj_server_submit(hj_server_t *srv, hj_algo_t algo, const hj_tuple_t *R, size_t nR, const hj_tuple_t *S,
