@@ -96,7 +96,9 @@ enum : int {
 // every row id (build and probe) below 2^32, the last partition pass stores each tuple as one 8-byte
 // word, (key >> bits) << 32 | row id, and the joins read 8 bytes per tuple instead of 16. Inside a
 // final partition the low `bits` key bits are equal, so comparing key >> bits compares keys. A probe
-// key whose high part does not fit is stored as 0xffffffff: no build key has that high part. The
+// key whose high part is 2^31 or more is stored as 0xffffffff: no build key has that high part. Joins
+// where a build key 0 never matches (lp_join's empty-slot rule) store that key's words with high part
+// 0x80000000, which no build key and no probe word has (ci_word_z0). The
 // widths are ORed together by the pass that reads the relations first (hist_chunk_kernel or
 // seg_pass1_kernel), so the choice is made on the device, before the last pass.
 __device__ __forceinline__ bool ci_applies(const uint32_t *counters, int bits) {
@@ -120,9 +122,22 @@ __device__ __forceinline__ unsigned long long w8_word(unsigned long long key, un
     return (h32 << 32) | (rid & 0xffffffffull);
 }
 
+// Build relations whose key 0 never matches (z0): key 0's word takes the high part 0x80000000, which no
+// other build word has; the last pass keeps it (store_elem) and stores every probe word whose high part
+// has bit 31 set as 0xffffffff, so nothing matches it.
+__device__ __forceinline__ unsigned long long w8_word_z0(unsigned long long key, unsigned long long rid, int b1,
+                                                         bool z0) {
+    return z0 && key == 0 ? (0x80000000ull << 32) | (rid & 0xffffffffull) : w8_word(key, rid, b1);
+}
+
 __device__ __forceinline__ unsigned long long ci_word(unsigned long long key, unsigned long long rid, int bits) {
     const unsigned long long hi = key >> bits;
-    return ((hi < 0xffffffffull ? hi : 0xffffffffull) << 32) | (rid & 0xffffffffull);
+    return ((hi < 0x80000000ull ? hi : 0xffffffffull) << 32) | (rid & 0xffffffffull);
+}
+
+__device__ __forceinline__ unsigned long long ci_word_z0(unsigned long long key, unsigned long long rid, int bits,
+                                                         bool z0) {
+    return z0 && key == 0 ? (0x80000000ull << 32) | (rid & 0xffffffffull) : ci_word(key, rid, bits);
 }
 
 // Build partitions up to this size whose keys (above the radix bits) and row ids fit 32 bits are
@@ -619,6 +634,7 @@ struct ScatterArgs {
     // Last pass of a join that may read compact final partitions: when ci_applies holds, the output is
     // 8-byte words (ci_word) at outR8 / outS8 instead of tuples at outR / outS.
     int ci_out;
+    int ci_z0;                  // build key 0 never matches: its compact words take ci_word_z0's high part
     unsigned long long *outR8, *outS8;
     // Segment mode after a pass 1 that may have written 8-byte words: 1 = this launch reads words (runs
     // when w8_fits holds), 2 = this launch reads tuples (runs when it does not); 0 = no such pass 1.
@@ -767,15 +783,18 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
 // Store one element of the last pass: a tuple, its compact final word (ci), or - from an 8-byte word of
 // a segment-mode pass 1, which holds key >> b1 - the final word with key >> bits.
 __device__ __forceinline__ void store_elem(const tuple_v &t, tuple_v *out, unsigned long long *out8, long long dst,
-                                           bool ci, int bits, int) {
+                                           bool ci, int bits, int, bool z0) {
     if (ci)
-        st_stream8(out8 + dst, ci_word(t.x, t.y, bits));
+        st_stream8(out8 + dst, ci_word_z0(t.x, t.y, bits, z0));
     else
         st_stream(out + dst, t);
 }
 __device__ __forceinline__ void store_elem(unsigned long long w, tuple_v *, unsigned long long *out8, long long dst,
-                                           bool, int, int b2) {
-    st_stream8(out8 + dst, (((w >> 32) >> b2) << 32) | (w & 0xffffffffull));
+                                           bool, int, int b2, bool z0) {
+    // A pass-1 high part with bit 31 set is a probe key beyond every build key, or (z0) a build key 0.
+    const unsigned long long h1 = w >> 32;
+    const unsigned long long h = h1 < 0x80000000ull ? h1 >> b2 : (z0 ? 0x80000000ull : 0xffffffffull);
+    st_stream8(out8 + dst, (h << 32) | (w & 0xffffffffull));
 }
 
 // Elements of a tile: 16-byte tuples, or (WIN) the 8-byte words of a segment-mode pass 1 (w8_word).
@@ -806,7 +825,6 @@ __device__ __forceinline__ uint32_t elem_digit(unsigned long long v, int, uint64
 
 template <int THREADS, int ITEMS, bool STABLE, int NBUF, int MINB, bool WIN = false>
 __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
-    static_assert(!(WIN && STABLE), "8-byte-word tiles only for joins that count every match");
     using E = typename ScatterElem<WIN>::type;
     constexpr int T = THREADS * ITEMS;
     constexpr int NW = THREADS / 32;
@@ -1024,6 +1042,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         // compact final partitions). Full tiles load their staged tuples in two halves so that the stores
         // issue back to back.
         unsigned long long *out8 = sl.out == a.outS ? a.outS8 : a.outR8;
+        const bool z0 = a.ci_z0 && sl.out == a.outR;
         if (cnt == (uint32_t)T) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
@@ -1037,7 +1056,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) {
                     if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len)
-                        store_elem(t[i], sl.out, out8, dst[i], ci, a.bits, b2);
+                        store_elem(t[i], sl.out, out8, dst[i], ci, a.bits, b2, z0);
                     else
                         set_error(err, kErrBounds);
                 }
@@ -1047,7 +1066,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             const E t = buf[j];
             const long long dst = gbase[elem_digit(t, a.shift, dmask)] + (long long)j;
             if (dst >= 0 && (uint64_t)dst < sl.out_len)
-                store_elem(t, sl.out, out8, dst, ci, a.bits, b2);
+                store_elem(t, sl.out, out8, dst, ci, a.bits, b2, z0);
             else
                 set_error(err, kErrBounds);
         }
@@ -1093,6 +1112,7 @@ struct SegArgs {
     uint32_t *hist;            // [2*grid][2^bits]: row c = R tuples of CTA c, row grid + c = its S tuples
     uint32_t *counters;        // kCtrItem1 (items), kCtrSegAlloc, kCtrErr, kCtrMaxKey/kCtrMaxRid
     int test_stall;            // test hook: CTA 0 withholds its first tile load (its wait must expire)
+    int z0;                    // build key 0 never matches: its words take the high part 0x80000000
 };
 
 struct SegSlot {
@@ -1109,12 +1129,18 @@ struct SegRun {
     uint32_t split;
 };
 
-// Thread 0: the next tile of this CTA's current work item, claiming items as needed.
+// Thread 0: the next tile of this CTA's current work item, claiming items as needed. STATIC_R: the build
+// relation's items [r_next, r_end) belong to this CTA and come first, in order; the probe relation's
+// items are claimed from the counter.
+template <bool STATIC_R>
 __device__ __forceinline__ SegSlot seg_next_tile(const SegArgs &a, uint32_t &item, uint32_t &t_next,
-                                                 uint32_t &t_end) {
+                                                 uint32_t &t_end, uint32_t &r_next, uint32_t r_end) {
     SegSlot s;
     while (item == ~0u || t_next >= t_end) {
-        item = atomicAdd(&a.counters[kCtrItem1], 1u);
+        if (STATIC_R && r_next < r_end)
+            item = r_next++;
+        else
+            item = atomicAdd(&a.counters[kCtrItem1], 1u) + (STATIC_R ? a.itemsR : 0u);
         if (item >= a.items) {
             item = ~0u;
             s.in = nullptr;
@@ -1153,7 +1179,12 @@ __device__ __forceinline__ void seg_flush(uint32_t *jh, uint32_t *row, int nbins
 // K = ceil(F1 / 32): pass-1 digits per lane of warp 0, which keeps their segment state in registers.
 // W8: store 8-byte words (w8_word) in segments of 2 * kTile words (the same 32 KB); the launch that stores
 // tuples after it runs only when the widths did not allow words (w8_first).
-template <int THREADS, int ITEMS, int K, bool W8 = false>
+// STABLE_R (first-match joins): every build-relation chain keeps input order. CTA c takes the build
+// relation's items [c * itemsR / G, (c + 1) * itemsR / G) in order before any probe item, and ranks
+// their tiles stably (warp-ordered ballots, as the stable scatter does), so pass 2, which writes each
+// digit's chains in CTA order and each chain in order, leaves every final build partition in input
+// order. Probe tiles keep the atomic rank: their order inside a partition changes no result.
+template <int THREADS, int ITEMS, int K, bool W8 = false, bool STABLE_R = false>
 __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegArgs a) {
     constexpr int T = THREADS * ITEMS;
     static_assert(T == kTile, "a tile fills one segment of tuples");
@@ -1167,9 +1198,10 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
     uint32_t *thist = reinterpret_cast<uint32_t *>(runs + 256);        // [256] tile histogram
     uint32_t *tdstart = thist + 256;                                   // [256] digit start in the staged tile
     uint32_t *jh = tdstart + 256;                                      // [2^bits / 2] counter pairs
+    uint16_t *whist = reinterpret_cast<uint16_t *>(jh + (1 << a.bits) / 2);  // STABLE_R: [warps][F1]
     __shared__ __align__(8) unsigned long long bars[2];
     __shared__ SegSlot slots[2];
-    __shared__ uint32_t s_item, s_tnext, s_tend;  // thread 0's item iterator
+    __shared__ uint32_t s_item, s_tnext, s_tend, s_rnext, s_rend;  // thread 0's item iterator
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int F = a.F1;
@@ -1197,14 +1229,17 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
     if (tid == 0) {
         s_item = ~0u;
         s_tnext = s_tend = 0;
+        s_rnext = (uint32_t)((uint64_t)c * a.itemsR / G);
+        s_rend = (uint32_t)((uint64_t)(c + 1) * a.itemsR / G);
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        uint32_t item = s_item, tn = s_tnext, te = s_tend;
-        const SegSlot s0 = seg_next_tile(a, item, tn, te);
+        uint32_t item = s_item, tn = s_tnext, te = s_tend, rn = s_rnext;
+        const SegSlot s0 = seg_next_tile<STABLE_R>(a, item, tn, te, rn, s_rend);
         s_item = item;
         s_tnext = tn;
         s_tend = te;
+        s_rnext = rn;
         slots[0] = s0;
         if (s0.cnt && !(a.test_stall && blockIdx.x == 0)) tma_load_1d(inbuf, s0.in, s0.cnt * 16u, bar0);
     }
@@ -1221,11 +1256,12 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         if (sl.cnt == 0) break;
         tuple_v *buf = inbuf + (size_t)cur * T;
         if (tid == 0) {
-            uint32_t item = s_item, tn = s_tnext, te = s_tend;
-            const SegSlot sn = seg_next_tile(a, item, tn, te);
+            uint32_t item = s_item, tn = s_tnext, te = s_tend, rn = s_rnext;
+            const SegSlot sn = seg_next_tile<STABLE_R>(a, item, tn, te, rn, s_rend);
             s_item = item;
             s_tnext = tn;
             s_tend = te;
+            s_rnext = rn;
             slots[cur ^ 1u] = sn;
             if (sn.cnt) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
         }
@@ -1284,13 +1320,14 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
 
         tuple_v v[ITEMS];
         uint32_t rk[ITEMS];
+        const bool st = STABLE_R && sl.rel == 0;  // uniform: this tile takes the stable rank
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
             if (idx < cnt) {
                 v[i] = buf[idx];
                 const uint32_t d = (uint32_t)v[i].x & dmask;
-                rk[i] = atomicAdd(&thist[d], 1u);
+                if (!st) rk[i] = atomicAdd(&thist[d], 1u);
                 const uint32_t bin = (uint32_t)(v[i].x & bmask);
                 atomicAdd(&jh[bin >> 1], 1u << ((bin & 1u) << 4));
                 if (sl.rel == 0) {
@@ -1299,6 +1336,47 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 } else {
                     rors |= v[i].y;
                 }
+            }
+        }
+        if (STABLE_R && st) {
+            // Stable rank within the warp: items in order, lanes in order; the lanes holding one digit
+            // are found with one ballot per digit bit (plus the bit that marks padding lanes).
+            uint16_t *wh = whist + w * F;
+            for (int j = lane; j < F; j += 32) wh[j] = 0;
+            __syncwarp();
+            const unsigned ltmask = lanemask_lt();
+            const int nbits = a.b1 + (cnt < (uint32_t)T ? 1 : 0);
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
+                const uint32_t d = idx < cnt ? (uint32_t)v[i].x & dmask : (uint32_t)F;
+                unsigned peers = 0xffffffffu;
+#pragma unroll
+                for (int b = 0; b < 9; b++) {
+                    if (b < nbits) {
+                        const unsigned bit = (d >> b) & 1u;
+                        const unsigned bal = __ballot_sync(0xffffffffu, bit);
+                        peers &= bit ? bal : ~bal;
+                    }
+                }
+                const bool valid = d < (uint32_t)F;
+                uint32_t pre = 0;
+                if (valid) pre = wh[d];
+                rk[i] = pre + __popc(peers & ltmask);
+                __syncwarp();
+                if (valid && (peers & ltmask) == 0) wh[d] = (uint16_t)(pre + __popc(peers));
+                __syncwarp();
+            }
+            __syncthreads();
+            // Tile count per digit, and each warp's start within the digit's run.
+            if (tid < F) {
+                uint32_t h = 0;
+                for (int q = 0; q < THREADS / 32; q++) {
+                    const uint32_t n = whist[q * F + tid];
+                    whist[q * F + tid] = (uint16_t)h;
+                    h += n;
+                }
+                thist[tid] = h;
             }
         }
         __syncthreads();
@@ -1402,10 +1480,14 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
-            if (idx < cnt) buf[tdstart[(uint32_t)v[i].x & dmask] + rk[i]] = v[i];
+            if (idx < cnt) {
+                const uint32_t d = (uint32_t)v[i].x & dmask;
+                buf[tdstart[d] + (STABLE_R && st ? (uint32_t)whist[w * F + d] : 0u) + rk[i]] = v[i];
+            }
         }
         __syncthreads();
-        // Write each digit run: consecutive threads write consecutive 16-byte tuples.
+        // Write each digit run: consecutive threads write consecutive 16-byte tuples (8-byte words).
+        const bool z0 = a.z0 && sl.rel == 0;
         if (cnt == (uint32_t)T) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
@@ -1423,7 +1505,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 for (int i = 0; i < ITEMS / 2; i++) {
                     if (dst[i] >= 0 && (uint64_t)dst[i] < cap) {
                         if (W8)
-                            st_stream8(out8 + dst[i], w8_word(t[i].x, t[i].y, a.b1));
+                            st_stream8(out8 + dst[i], w8_word_z0(t[i].x, t[i].y, a.b1, z0));
                         else
                             st_stream(a.out + dst[i], t[i]);
                     } else {
@@ -1438,7 +1520,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 const long long dst = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * SEGW);
                 if (dst >= 0 && (uint64_t)dst < cap) {
                     if (W8)
-                        st_stream8(out8 + dst, w8_word(t.x, t.y, a.b1));
+                        st_stream8(out8 + dst, w8_word_z0(t.x, t.y, a.b1, z0));
                     else
                         st_stream(a.out + dst, t);
                 } else {
@@ -1577,8 +1659,8 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
         uint32_t *head32 = reinterpret_cast<uint32_t *>(head);
         for (uint32_t q = tid; q < (nb + 1) / 2; q += kCompactThreads) head32[q] = 0;
         __syncthreads();
-        // Load and chain the build side; lp_join skips key 0, which reads as an empty slot there (compact
-        // final partitions are never used by joins with that rule).
+        // Load and chain the build side; lp_join skips key 0, which reads as an empty slot there (in
+        // compact final partitions such a key's words have a high part that no probe word has).
         const tuple_v *R = a.finR + item.r_begin;
         const unsigned long long *R8 = a.finR8 + item.r_begin;
         for (uint32_t i0 = tid; i0 < nr; i0 += 4 * kCompactThreads) {
@@ -1594,7 +1676,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 if (i >= nr) continue;
                 rkey[i] = (uint32_t)(t[u].x >> B);
                 rrid[i] = (uint32_t)t[u].y;
-                if (skip0 && t[u].x == 0) continue;
+                if (!ci && skip0 && t[u].x == 0) continue;
                 nxt[i] = (uint16_t)atomic_exch_u16(&head[(t[u].x >> B) & hmask], i + 1);
             }
         }
@@ -1768,7 +1850,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
         // Build: chain every R tuple (lp_join skips key 0, which reads as an empty slot there).
         for (uint32_t i = tid; i < nr; i += kJoinThreads) {
             const uint64_t k = rt[i].x;
-            if (skip0 && k == 0) continue;
+            if (!ci && skip0 && k == 0) continue;
             const uint32_t h = (uint32_t)((k >> B) & hmask);
             nxt[i] = (uint16_t)atomic_exch_u16(&head[h], i + 1);
         }
@@ -1960,7 +2042,7 @@ __global__ void join_large_build(JoinArgs a) {
                 l = find_large(a.large, nl, g, true);
                 i = g - a.large[l].r_flat;
                 r = fin_r(a, ci, a.large[l].r_begin + i);
-                act = !(a.skip0 && r.x == 0);
+                act = !(a.skip0 && !ci && r.x == 0);
             }
             const unsigned act_mask = __ballot_sync(0xffffffffu, act);
             if (!act) continue;
@@ -1993,7 +2075,7 @@ __global__ void join_large_build(JoinArgs a) {
         const LargePart &L = a.large[l];
         const uint64_t i = g - L.r_flat;
         const uint64_t k = fin_r(a, ci, L.r_begin + i).x;
-        if (a.skip0 && k == 0) continue;
+        if (a.skip0 && !ci && k == 0) continue;
         uint32_t *head = a.large_table + L.table_off;
         uint32_t *nxt = head + (1ull << L.nb_log);
         const uint64_t h = (k >> bshift) & ((1ull << L.nb_log) - 1);
@@ -2198,8 +2280,8 @@ struct PhjSizes {
 // (2 * CTAs * F1 * kTile tuples).
 constexpr uint64_t kSegMinTuples = 1ull << 27;
 
-bool phj_seg_applies(const RadixGeom &g, bool lp, size_t nR, size_t nS) {
-    return !lp && g.passes == 2 && g.bits <= kSegMaxBits && (uint64_t)nR + nS >= kSegMinTuples;
+bool phj_seg_applies(const RadixGeom &g, bool, size_t nR, size_t nS) {
+    return g.passes == 2 && g.bits <= kSegMaxBits && (uint64_t)nR + nS >= kSegMinTuples;
 }
 
 static PhjSizes phj_sizes(const RadixGeom &g, size_t nR, size_t nS, int num_sms, bool seg) {
@@ -2307,10 +2389,12 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
 
 static bool g_attr_done[64] = {};
 
-// Dynamic shared memory of seg_pass1_kernel: two tile buffers, per-digit state, 2^bits 16-bit counters.
-static size_t seg_smem_bytes(int bits) {
-    // tile buffers, runs[256], thist[256], tdstart[256], counter pairs
-    return (size_t)2 * kTile * 16 + 256 * sizeof(SegRun) + 256 * 4 * 2 + ((size_t)1 << bits) * 2;
+// Dynamic shared memory of seg_pass1_kernel: two tile buffers, per-digit state, 2^bits 16-bit counters,
+// and for the stable build-relation rank one 16-bit counter per (warp, digit).
+static size_t seg_smem_bytes(int bits, bool stable) {
+    // tile buffers, runs[256], thist[256], tdstart[256], counter pairs, whist
+    return (size_t)2 * kTile * 16 + 256 * sizeof(SegRun) + 256 * 4 * 2 + ((size_t)1 << bits) * 2 +
+           (stable ? (size_t)(kScatterThreads / 32) * 256 * 2 : 0);
 }
 
 int phj_prepare_device() {
@@ -2326,24 +2410,25 @@ int phj_prepare_device() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 1>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 2>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 4>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 8>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 1, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 2, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 4, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, 8, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits)));
+#define HJ_SEG_ATTR(KK, W, ST)                                                                             \
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, ST>,                  \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits, ST)))
+#define HJ_SEG_ATTR4(W, ST) \
+    HJ_SEG_ATTR(1, W, ST);  \
+    HJ_SEG_ATTR(2, W, ST);  \
+    HJ_SEG_ATTR(4, W, ST);  \
+    HJ_SEG_ATTR(8, W, ST)
+    HJ_SEG_ATTR4(false, false);
+    HJ_SEG_ATTR4(true, false);
+    HJ_SEG_ATTR4(false, true);
+    HJ_SEG_ATTR4(true, true);
+#undef HJ_SEG_ATTR4
+#undef HJ_SEG_ATTR
     HJ_CU(cudaFuncSetAttribute(
         scatter_kernel<kScatterThreads, 2 * kScatterItems, false, kScatterBufs, kScatterWordCtasPerSm, true>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
+    HJ_CU(cudaFuncSetAttribute(
+        scatter_kernel<kScatterThreads, 2 * kScatterItems, true, kScatterBufs, kScatterWordCtasPerSm, true>,
         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2382,12 +2467,11 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     // A segment-mode scratch holds the segment storage, not the exact-offset pipeline's buffers.
     const bool segm = s.seg;
     // 8-byte words in the partitions (compact final partitions, and in segment mode an 8-byte pass 1):
-    // joins without per-match output whose key 0 may match (all but the materialising ones and
-    // phj_radix_lp), unless the caller asked for tuples (test_flags bit 2), when the widths allow them
-    // (decided on the device).
-    const int ci_ok = (!mat && !skip0 && !(test_flags & 2)) ? 1 : 0;
+    // joins without per-match output (all but the materialising ones), unless the caller asked for
+    // tuples (test_flags bit 2), when the widths allow them (decided on the device).
+    const int ci_ok = (!mat && !(test_flags & 2)) ? 1 : 0;
     const bool seg_words = segm && ci_ok;
-    if (segm && (lp || g.passes != 2 || g.bits > kSegMaxBits)) return HJ_E_INVAL;
+    if (segm && (g.passes != 2 || g.bits > kSegMaxBits)) return HJ_E_INVAL;
     {
         const int rc = phj_prepare_device();
         if (rc) return rc;
@@ -2418,13 +2502,21 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         ga.test_stall = (test_flags & 1) ? 1 : 0;
         ga.b1 = g.b1;
         ga.w8_first = 0;
-        const size_t sm = seg_smem_bytes(g.bits);
+        ga.z0 = skip0 ? 1 : 0;
+        // First-match joins keep every build partition in input order (the stable build-relation form).
+        const size_t sm = seg_smem_bytes(g.bits, lp);
         auto launch_pass1 = [&](bool words) {
-#define HJ_SEG_LAUNCH(KK)                                                                                  \
-    if (words)                                                                                             \
-        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, true><<<s.seg_grid, kScatterThreads, sm, st>>>(ga); \
-    else                                                                                                   \
-        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, false><<<s.seg_grid, kScatterThreads, sm, st>>>(ga)
+#define HJ_SEG_LAUNCH_W(KK, W)                                                                                   \
+    if (lp)                                                                                                      \
+        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, true><<<s.seg_grid, kScatterThreads, sm, st>>>(ga); \
+    else                                                                                                         \
+        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, false><<<s.seg_grid, kScatterThreads, sm, st>>>(ga)
+#define HJ_SEG_LAUNCH(KK)         \
+    if (words) {                  \
+        HJ_SEG_LAUNCH_W(KK, true);  \
+    } else {                      \
+        HJ_SEG_LAUNCH_W(KK, false); \
+    }
             if (F1 <= 32) {
                 HJ_SEG_LAUNCH(1);
             } else if (F1 <= 64) {
@@ -2435,6 +2527,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
                 HJ_SEG_LAUNCH(8);
             }
 #undef HJ_SEG_LAUNCH
+#undef HJ_SEG_LAUNCH_W
         };
         if (seg_words) {
             // Pass 1 in 8-byte words; if the widths turn out not to allow them, the counters are reset and
@@ -2517,9 +2610,30 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.ctr_item = pass == 0 ? kCtrItem1 : kCtrItem2;
         sa.item_base = sa.item_end = 0;
         sa.ci_out = (pass == g.passes - 1) ? ci_ok : 0;
+        sa.ci_z0 = skip0 ? 1 : 0;
         sa.outR8 = reinterpret_cast<unsigned long long *>(out);
         sa.outS8 = sa.outR8 + nR;
         sa.w8 = 0;
+        // One pass over [item_base, item_end): in segment mode after an 8-byte pass 1, the launch over
+        // 4096-word tiles and the tuple launch after it (which runs only if pass 1 fell back to tuples).
+        auto launch_scatter = [&](bool stable) {
+#define HJ_SCATTER(ST)                                                                                         \
+    if (segm && seg_words) {                                                                                   \
+        sa.w8 = 1;                                                                                             \
+        scatter_kernel<kScatterThreads, 2 * kScatterItems, ST, kScatterBufs, kScatterWordCtasPerSm, true>        \
+            <<<num_sms * kScatterWordCtasPerSm, kScatterThreads, scatter_smem, st>>>(sa);                      \
+        nlaunch++;                                                                                             \
+        sa.w8 = 2;                                                                                             \
+    }                                                                                                          \
+    scatter_kernel<kScatterThreads, kScatterItems, ST, kScatterBufs, kScatterCtasPerSm>                          \
+        <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa)
+            if (stable) {
+                HJ_SCATTER(true);
+            } else {
+                HJ_SCATTER(false);
+            }
+#undef HJ_SCATTER
+        };
         if (lp) {
             // First-match joins need each final build partition in input order (the join keeps the
             // lowest position among equal keys), so the build relation's items take the stable rank.
@@ -2529,30 +2643,17 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
             const uint32_t r_items = cg.cR * per_chunk, all_items = (cg.cR + cg.cS) * per_chunk;
             sa.item_end = r_items;
             if (r_items) {
-                scatter_kernel<kScatterThreads, kScatterItems, true, kScatterBufs, kScatterCtasPerSm>
-                    <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+                launch_scatter(true);
                 nlaunch++;
             }
             sa.item_base = r_items;
             sa.item_end = all_items;
             sa.ctr_item = pass == 0 ? kCtrItem1S : kCtrItem2S;
             sa.test_stall = 0;
-            if (all_items > r_items)
-                scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
-                    <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
-        } else if (segm && seg_words) {
-            // Pass 2 over the chains of an 8-byte pass 1: tiles of 4096 words (one segment); the tuple
-            // launch after it runs only if pass 1 had to fall back to tuples.
-            sa.w8 = 1;
-            scatter_kernel<kScatterThreads, 2 * kScatterItems, false, kScatterBufs, kScatterWordCtasPerSm, true>
-                <<<num_sms * kScatterWordCtasPerSm, kScatterThreads, scatter_smem, st>>>(sa);
-            nlaunch++;
-            sa.w8 = 2;
-            scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
-                <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+            sa.w8 = 0;
+            if (all_items > r_items) launch_scatter(false);
         } else {
-            scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>
-                <<<scatter_grid, kScatterThreads, scatter_smem, st>>>(sa);
+            launch_scatter(false);
         }
         HJ_CU(cudaGetLastError());
         nlaunch++;

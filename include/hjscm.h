@@ -99,10 +99,11 @@ typedef struct {
 #define HJ_F_NO_TIMING   0x1u /* skip the per-phase CUDA events (buildpart/probejoin stay 0) */
 #define HJ_F_PINNED_HOST 0x2u /* host inputs are already page-locked */
 #define HJ_F_PHASE_TIMES 0x4u /* also time each kernel group (fills hj_result_t.phase) */
-/* Radix joins that count every match (bc, sc, hr, hro; two passes, <= 14 bits) from 2^27 tuples run
- * in segment mode: pass 1 writes chains of fixed-size segments and counts the histograms itself, so no
- * histogram pass reads the relations first (if the larger scratch does not fit, the exact-offset
- * pipeline runs). These flags pick the pipeline regardless of size; results are the same. */
+/* Radix joins (two passes, <= 14 bits) from 2^27 tuples run in segment mode: pass 1 writes chains of
+ * fixed-size segments and counts the histograms itself, so no histogram pass reads the relations first
+ * (if the larger scratch does not fit, the exact-offset pipeline runs). First-match joins (lp) keep each
+ * build partition in input order there too: every pass-1 CTA takes a contiguous range of the build
+ * relation and ranks it stably. These flags pick the pipeline regardless of size; results are the same. */
 #define HJ_F_SEGMENTS    0x20u /* segment mode whenever the algorithm allows it */
 #define HJ_F_EXACT       0x40u /* always the histogram pass and exact pass-1 offsets */
 /* Radix joins store a tuple as one 8-byte word in the partitions when the widths allow (see

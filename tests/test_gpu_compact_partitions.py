@@ -2,7 +2,7 @@
 2^31 and every row id (build and probe) below 2^32, the last partition pass stores 8-byte words
 (key >> bits) << 32 | row id and the joins read those (hj_result_t.flags has HJ_RES_COMPACT_PARTITIONS).
 Results equal the oracle's on both sides of every limit, through both pipelines and the large-partition
-path; joins with per-match output or the key-0 rule never use them."""
+path; joins with per-match output never use them."""
 import numpy as np
 import pytest
 
@@ -64,15 +64,42 @@ def test_flag_and_results_at_the_limits(hj, oracle, cuda, pipeline):
     assert run(hj, oracle, cuda, "phj_radix_bc", R, S5, flags)
 
 
-def test_semantics_that_keep_tuples(hj, oracle, cuda):
+def test_other_names_and_geometries(hj, oracle, cuda):
     R, S = rels(2)
-    R[::50, 0] = 0  # key 0: ignored by phj_radix_lp
-    for algo in ("phj_radix_sc", "phj_radix_hr", "phj_asymm_radix_bc", "phj_radix_bw_reg_bc"):
+    R[::50, 0] = 0  # key 0: ignored by phj_radix_lp, a key like any other for the rest
+    for algo in ("phj_radix_sc", "phj_radix_hr", "phj_asymm_radix_bc", "phj_radix_bw_reg_bc", "phj_radix_lp"):
         assert run(hj, oracle, cuda, algo, R, S)
-    assert not run(hj, oracle, cuda, "phj_radix_lp", R, S)
     # one pass (8 bits) and two passes with an uneven split
     assert run(hj, oracle, cuda, "phj_radix_bc", R, S, bits=8, passes=1)
     assert run(hj, oracle, cuda, "phj_radix_bc", R, S, bits=11, passes=2)
+
+
+def test_first_match_join_reads_compact_words(hj, oracle, cuda):
+    """phj_radix_lp reads compact words: a build key 0 never matches (its words carry the high part
+    0x80000000, which no build key has and no probe word gets: probe keys whose key >> bits is 2^31 or
+    more are stored as 0xffffffff), and among duplicates the first build tuple in input order wins, in
+    the compact, the 16-byte and the global-memory partition joins."""
+    R, S = rels(4)
+    R[::50, 0] = 0
+    R[1::3, 0] = R[::3, 0][: R[1::3].shape[0]]          # duplicates: every key of R[::3] twice
+    S[::11, 0] = 0                                       # probe key 0 finds nothing
+    S[1::13, 0] = np.uint64((1 << 31) << BITS)           # partition 0, key >> bits = 2^31
+    S[2::13, 0] = np.uint64(((1 << 31) + 5) << BITS | 3)
+    for flags in (0, hj.HJ_F_EXACT):
+        assert run(hj, oracle, cuda, "phj_radix_lp", R, S, flags)
+    # partition 0 (the one key 0 lives in) with ~9000 and then ~16000 build tuples, key 0 and duplicates
+    rng = np.random.default_rng(6)
+    for n0 in (9000, 16000):
+        base, _ = rels(7, nR=1 << 16, nS=1 << 17)
+        p0 = np.empty((n0, 2), dtype=np.uint64)
+        p0[:, 0] = rng.integers(0, 3000, n0, dtype=np.uint64) << np.uint64(BITS)
+        p0[::40, 0] = 0
+        p0[:, 1] = rng.integers(0, 1 << 32, n0, dtype=np.uint64)
+        R2 = np.concatenate([p0[: n0 // 2], base, p0[n0 // 2:]])
+        S2 = R2[rng.integers(0, R2.shape[0], 4 * R2.shape[0])].copy()
+        S2[:, 1] = rng.integers(0, 1 << 32, S2.shape[0], dtype=np.uint64)
+        S2[::17, 0] = np.uint64((1 << 31) << BITS)
+        assert run(hj, oracle, cuda, "phj_radix_lp", R2, S2)
 
 
 def test_mid_and_large_partitions_read_compact_words(hj, oracle, cuda):

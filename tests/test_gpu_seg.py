@@ -1,5 +1,5 @@
-"""GPU parity of segment mode: the radix joins that count every match partition in pass 1 into
-chains of fixed-size segments and count the histograms on the way (no histogram pass). Forced at
+"""GPU parity of segment mode: the radix joins partition in pass 1 into chains of fixed-size segments
+and count the histograms on the way (no histogram pass). Forced at
 small sizes with HJ_F_SEGMENTS, its results must equal the oracle's and the exact-offset pipeline's
 (HJ_F_EXACT) bit for bit, on uniform, skewed, duplicate-heavy and ragged inputs."""
 import numpy as np
@@ -96,15 +96,77 @@ def test_segment_mode_hot_bin(hj, cuda):
     assert seg.large_partitions == 1
 
 
-def test_segment_mode_not_for_first_match(hj, oracle, cuda):
-    # phj_radix_lp depends on input order within partitions: the flag leaves it on the exact pipeline.
+def narrow(a):
+    """Row ids below 2^32: with small keys the 8-byte word layout applies."""
+    a = a.copy()
+    a[:, 1] &= np.uint64(0xFFFFFFFF)
+    return a
+
+
+def test_segment_mode_first_match(hj, oracle, cuda):
+    """phj_radix_lp in segment mode: each pass-1 CTA takes a contiguous range of the build relation, in
+    order, and ranks its tiles stably, and pass 2 writes each digit's chains in CTA order, so every
+    final build partition keeps input order and the first match is the reference's. Duplicates spread
+    over the whole build relation (over many pass-1 CTAs), key 0, ragged tiles; 16-byte tuples, 8-byte
+    words in pass 1 and the final partitions, and build keys too wide for pass-1 words (pass 1 runs
+    again with tuples)."""
     rng = np.random.default_rng(8)
-    R = random_rel(rng, 40_000, 1, 10_000)
-    S = random_rel(rng, 90_000, 1, 12_000)
-    seg, exact = both(hj, cuda, "phj_radix_lp", R, S)
+    cases = [
+        (random_rel(rng, 40_000, 1, 10_000), random_rel(rng, 90_000, 1, 12_000), False),
+        (narrow(random_rel(rng, 300_000, 0, 3_000)), narrow(random_rel(rng, 200_000, 0, 3_500)), True),
+        (narrow(random_rel(rng, 2047, 0, 50)), narrow(random_rel(rng, 4099, 0, 60)), True),
+        (narrow(random_rel(rng, 1, 0, 0)), narrow(random_rel(rng, 3, 0, 0)), True),
+        (random_rel(rng, 250_000, 0, 2_000), random_rel(rng, 100_000, 0, 2_200), False),
+    ]
+    wide = narrow(random_rel(rng, 100_000, 0, 4_000))
+    wide[:, 0] = (wide[:, 0] << np.uint64(40)) | (wide[:, 0] & np.uint64(0x3FFF))  # key >> 7 beyond 2^31
+    wide[::97, 0] = 0
+    wide_s = wide[rng.integers(0, wide.shape[0], 150_000)].copy()
+    wide_s[:, 1] = rng.integers(0, 1 << 32, wide_s.shape[0], dtype=np.uint64)
+    cases.append((wide, wide_s, False))
+    for R, S, words in cases:
+        want = oracle.join("phj_radix_lp", R, S)
+        seg, exact = both(hj, cuda, "phj_radix_lp", R, S)
+        assert (seg.matched_cnt, seg.checksum) == want, (len(R), len(S))
+        assert (exact.matched_cnt, exact.checksum) == want
+        assert seg.phase[0] == 0.0 and exact.phase[0] > 0.0  # no histogram pass in segment mode
+        assert bool(seg.flags & hj.HJ_RES_WORD_PASS1) == words
+
+
+def test_segment_mode_first_match_pairs(hj, oracle, cuda):
+    """The materialising first-match join in segment mode writes the reference's pairs."""
+    rng = np.random.default_rng(21)
+    R = np.empty((60_000, 2), dtype=np.uint64)
+    R[:, 0] = rng.integers(0, 5_000, R.shape[0], dtype=np.uint64)
+    R[:, 1] = np.arange(1, R.shape[0] + 1, dtype=np.uint64)  # row ids: 1-based positions (retrieve)
+    S = np.empty((90_000, 2), dtype=np.uint64)
+    S[:, 0] = rng.integers(0, 5_500, S.shape[0], dtype=np.uint64)
+    S[:, 1] = np.arange(1, S.shape[0] + 1, dtype=np.uint64)
+    want = oracle.join_pairs("ptr_phj_radix_lp", R, S)
+    out = cuda.zeros((want.shape[0] + 10, 2), dtype=cuda.int64, device="cuda")
+    r = hj.join_mat("ptr_phj_radix_lp", dev(cuda, R), dev(cuda, S), pairs=out, on_device=True,
+                    flags=hj.HJ_F_SEGMENTS)
+    assert r.matched_cnt == want.shape[0]
+    got = out[: r.matched_cnt].cpu().numpy().view(np.uint64)
+    got = got[np.lexsort((got[:, 1], got[:, 0]))]
+    assert np.array_equal(got, want)
+
+
+def test_segment_mode_first_match_large_partitions(hj, oracle, cuda):
+    """First-match joins in segment mode with build partitions above the shared-memory tables (the
+    global-memory join keeps the lowest position among equal keys), with key 0 among them."""
+    rng = np.random.default_rng(22)
+    n = 64 * 12_000
+    R = np.empty((n, 2), dtype=np.uint64)
+    R[:, 0] = (rng.integers(0, 6_000, n, dtype=np.uint64) << np.uint64(14)) | rng.integers(0, 64, n, dtype=np.uint64)
+    R[::50, 0] = 0
+    R[:, 1] = rng.integers(0, 1 << 32, n, dtype=np.uint64)
+    S = R[rng.integers(0, n, 2 * n)].copy()
+    S[:, 1] = rng.integers(0, 1 << 32, S.shape[0], dtype=np.uint64)
     want = oracle.join("phj_radix_lp", R, S)
+    seg, exact = both(hj, cuda, "phj_radix_lp", R, S)
     assert (seg.matched_cnt, seg.checksum) == want == (exact.matched_cnt, exact.checksum)
-    assert seg.phase[0] > 0.0  # the histogram pass ran
+    assert seg.large_partitions > 0
 
 
 def test_segment_mode_materialising(hj, oracle, cuda):
