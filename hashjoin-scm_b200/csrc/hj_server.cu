@@ -139,6 +139,7 @@ struct WaveLayout {
     size_t jobs_rel, rf_rel, sf_rel, tf_rel, rc_rel, sc_rel;  // offsets inside the descriptor region
     size_t sides_off, tables_off, copies_off, total;
     unsigned n_r_chunks, n_s_chunks;
+    unsigned r_piece, s_piece;  // chunk lengths of the build and probe relations (mj_piece)
 };
 
 struct WaveLane {
@@ -174,12 +175,19 @@ size_t wave_desc_bytes(size_t n, size_t nrc, size_t nsc, WaveLayout *L) {
     return o;
 }
 
-void wave_layout(const std::vector<Request> &reqs, WaveLayout *L) {
+void wave_layout(const std::vector<Request> &reqs, int num_sms, WaveLayout *L) {
     const size_t n = reqs.size();
     size_t nrc = 0, nsc = 0, table_bytes = 0, copy_bytes = 0;
+    unsigned long long tr = 0, ts = 0;
     for (const Request &r : reqs) {
-        nrc += ceil_div(r.nR, hj::kBuildChunk);
-        nsc += ceil_div(r.nS, hj::kProbeChunkMJ);
+        tr += r.nR;
+        ts += r.nS;
+    }
+    L->r_piece = hj::mj_piece(tr, hj::kBuildChunk, num_sms);
+    L->s_piece = hj::mj_piece(ts, hj::kProbeChunkMJ, num_sms);
+    for (const Request &r : reqs) {
+        nrc += ceil_div(r.nR, L->r_piece);
+        nsc += ceil_div(r.nS, L->s_piece);
         table_bytes += hj::mj_slots(r.nR) * 16;
         if (!r.on_device) copy_bytes += a256(r.nR * 16) + a256(r.nS * 16);
     }
@@ -239,7 +247,7 @@ int request_need(hj_server *s, Request &r) {
         need += a256(hj::nphj_scratch_bytes(r.nR, 0.5));
         if (wave_eligible(s, r)) {  // it will run in a wave: a wave of this request alone must fit
             WaveLayout lay;
-            wave_layout(std::vector<Request>(1, r), &lay);
+            wave_layout(std::vector<Request>(1, r), s->ctx->num_sms, &lay);
             if (lay.total > need) need = lay.total;
         }
     } else {
@@ -399,15 +407,15 @@ int launch_wave(hj_server *s, WaveLane &L) {
         m.lp = hj::algo_lp(r.algo) ? 1u : 0u;
         m.skip0 = hj::algo_skip0(r.algo) ? 1u : 0u;
         any_lp = any_lp || m.lp;
-        for (size_t b = 0; b < r.nR; b += hj::kBuildChunk, nrc++) {
+        for (size_t b = 0; b < r.nR; b += lay.r_piece, nrc++) {
             rc[nrc].job = (unsigned)q;
             rc[nrc].begin = b;
-            rc[nrc].len = (unsigned)(r.nR - b < hj::kBuildChunk ? r.nR - b : hj::kBuildChunk);
+            rc[nrc].len = (unsigned)(r.nR - b < lay.r_piece ? r.nR - b : lay.r_piece);
         }
-        for (size_t b = 0; b < r.nS; b += hj::kProbeChunkMJ, nsc++) {
+        for (size_t b = 0; b < r.nS; b += lay.s_piece, nsc++) {
             sc[nsc].job = (unsigned)q;
             sc[nsc].begin = b;
-            sc[nsc].len = (unsigned)(r.nS - b < hj::kProbeChunkMJ ? r.nS - b : hj::kProbeChunkMJ);
+            sc[nsc].len = (unsigned)(r.nS - b < lay.s_piece ? r.nS - b : lay.s_piece);
         }
         rf[q + 1] = rf[q] + r.nR;
         sf[q + 1] = sf[q] + r.nS;
@@ -537,14 +545,14 @@ void worker_main(hj_server *s) {
                 // The wave's block must fit the pool now; under memory pressure the wave shrinks (the
                 // requests left out stay queued, in order).
                 WaveLayout lay;
-                wave_layout(wave, &lay);
+                wave_layout(wave, s->ctx->num_sms, &lay);
                 size_t off = 0;
                 bool got = false;
                 for (;;) {
                     got = lay.desc_bytes <= s->stage_bytes && s->pool.alloc(lay.total, &off);
                     if (got || wave.size() == 1) break;
                     wave.resize(wave.size() / 2);
-                    wave_layout(wave, &lay);
+                    wave_layout(wave, s->ctx->num_sms, &lay);
                 }
                 if (got) {
                     // Take the wave's requests out of the queue (they are in queue order).

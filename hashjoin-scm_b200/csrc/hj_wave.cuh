@@ -42,6 +42,16 @@ struct MChunk {
 
 constexpr unsigned kBuildChunk = 8192, kProbeChunkMJ = 16384;
 
+// Chunk length for `total` tuples of a wave: the fixed piece, or a smaller one (a multiple of 256, at
+// least 256) when the wave is too small to give every SM four chunks; a lone small request would
+// otherwise run on a handful of CTAs, each working through thousands of dependent table accesses.
+inline unsigned mj_piece(unsigned long long total, unsigned max_piece, int num_sms) {
+    const unsigned long long want = (unsigned long long)(num_sms > 0 ? num_sms : 148) * 4;
+    unsigned long long p = (total + want - 1) / want;
+    p = (p + 255) / 256 * 256;
+    return p < 256 ? 256u : p > max_piece ? max_piece : (unsigned)p;
+}
+
 // Table slots of one job (load factor 0.5, two spare slots).
 inline unsigned long long mj_slots(size_t nR) { return (unsigned long long)((double)nR / 0.5) + 2; }
 
