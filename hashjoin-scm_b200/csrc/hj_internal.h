@@ -22,6 +22,16 @@ struct RadixGeom {
     int nparts() const { return 1 << bits; }
 };
 
+// Record `ev` on `st`. While the stream is being captured into a CUDA graph the record becomes an
+// event-record node (recorded at every launch of the graph, so its timings stay readable); a plain
+// cudaEventRecord there would only order the capture.
+inline cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+        return cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
+    return cudaEventRecord(ev, st);
+}
+
 // b1_req > 0 asks for that many pass-1 bits (clamped so that both passes have 1..8 bits).
 int radix_geom(int bits, int passes, RadixGeom *g, int b1_req = 0);
 

@@ -768,7 +768,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     HJ_CU(cudaMemsetAsync(a.side, 0, sizeof(NphjSide), st));
     HJ_CU(cudaMemsetAsync(&a.side->minpos, 0xff, sizeof(unsigned long long), st));
     // Phase slots: build spans [0, 1], probe spans [4, 5]; the others stay empty.
-    if (ph) HJ_CU(cudaEventRecord(ph[0], st));
+    if (ph) HJ_CU(record_event(ph[0], st));
     if (a.compact_ok) {
         const size_t hist_smem = (size_t)a.nslices * 4;
         nphj_widths<<<a.hist_blocks, kSliceThreads, hist_smem, st>>>(a);
@@ -801,9 +801,9 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         if (launches) *launches = nl;
         return HJ_OK;
     }
-    if (ev_mid) HJ_CU(cudaEventRecord(ev_mid, st));
+    if (ev_mid) HJ_CU(record_event(ev_mid, st));
     if (ph) {
-        for (int i = 1; i <= 4; i++) HJ_CU(cudaEventRecord(ph[i], st));
+        for (int i = 1; i <= 4; i++) HJ_CU(record_event(ph[i], st));
     }
     if (nS) {
         if (mat) {
@@ -815,8 +815,8 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     }
     HJ_CU(cudaGetLastError());
     if (ph) {
-        HJ_CU(cudaEventRecord(ph[5], st));
-        HJ_CU(cudaEventRecord(ph[6], st));
+        HJ_CU(record_event(ph[5], st));
+        HJ_CU(record_event(ph[6], st));
     }
     if (launches) *launches = nl + (nS ? (mat || !a.compact_ok ? 1u : 2u) : 0u);
     return HJ_OK;

@@ -827,6 +827,10 @@ template <int THREADS, int ITEMS, bool STABLE, int NBUF, int MINB, bool WIN = fa
 __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     using E = typename ScatterElem<WIN>::type;
     constexpr int T = THREADS * ITEMS;
+    // Where the prefetch of the next tile is issued: after this tile's wait barrier (atomic ranks, two
+    // buffers; measured faster: one barrier less per tile), or at the top of the iteration (stable
+    // ranks: measured faster there, as the rank's ballots keep warp 0 busy after the barrier).
+    constexpr bool LATE = NBUF == 2 && !STABLE;
     constexpr int NW = THREADS / 32;
     extern __shared__ __align__(128) unsigned char smem[];
     E *inbuf = reinterpret_cast<E *>(smem);                              // [NBUF][T]
@@ -892,9 +896,9 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         const TileSlot sl = slots[cur];
         if (sl.item == ~0u) break;
         E *buf = inbuf + (size_t)cur * T;
-        // Prefetch the next tile into the other buffer; the barrier that ended the previous iteration
-        // ordered every read of it before this copy.
-        if (NBUF == 2 && tid == 0) {
+        // Stable ranks: prefetch the next tile into the other buffer now; the barrier that ended the
+        // previous iteration ordered every access to it before this copy.
+        if (NBUF == 2 && !LATE && tid == 0) {
             const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
             slots[cur ^ 1u] = sn;
             if (sn.item != ~0u)
@@ -923,12 +927,22 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
                 set_error(err, kErrSpinLimit);
                 // Before leaving, let every copy this CTA issued land (bounded waits as well): no copy
                 // may write into shared memory the CTA no longer owns. The load into this buffer was
-                // issued unless the stall hook withheld it (CTA 0's first tile); the prefetch into the
-                // other buffer was issued if it has a tile.
+                // issued unless the stall hook withheld it (CTA 0's first tile); a prefetch into the
+                // other buffer is in flight only with stable ranks (issued above) if it has a tile.
                 if (!(a.test_stall && blockIdx.x == 0 && k == 0)) mbar_wait(bar0 + 8u * cur, par);
-                if (NBUF == 2 && slots[cur ^ 1u].item != ~0u) mbar_wait(bar0 + 8u * (cur ^ 1u), ((k + 1) >> 1) & 1u);
+                if (NBUF == 2 && !LATE && slots[cur ^ 1u].item != ~0u)
+                    mbar_wait(bar0 + 8u * (cur ^ 1u), ((k + 1) >> 1) & 1u);
             }
             break;
+        }
+        // Atomic ranks: prefetch the next tile into the other buffer now. Every thread has passed the
+        // barrier above, so the previous tile's staging and write-out, the last accesses to that
+        // buffer, are done, and no barrier has to end the iteration.
+        if (NBUF == 2 && LATE && tid == 0) {
+            const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
+            slots[cur ^ 1u] = sn;
+            if (sn.item != ~0u)
+                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, tile_copy_bytes<E>(sn.cnt), bar0 + 8u * (cur ^ 1u));
         }
 
         // Elements of this tile: warp w owns [w*32*ITEMS, (w+1)*32*ITEMS), one row of 32 per item.
@@ -1070,7 +1084,9 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             else
                 set_error(err, kErrBounds);
         }
-        __syncthreads();
+        // The next copy into this buffer (at the top of the next iteration with one buffer or stable
+        // ranks) must wait for this write-out; otherwise the next tile's wait barrier orders them.
+        if (!LATE) __syncthreads();
     }
 }
 
@@ -1255,16 +1271,6 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         const SegSlot sl = slots[cur];
         if (sl.cnt == 0) break;
         tuple_v *buf = inbuf + (size_t)cur * T;
-        if (tid == 0) {
-            uint32_t item = s_item, tn = s_tnext, te = s_tend, rn = s_rnext;
-            const SegSlot sn = seg_next_tile<STABLE_R>(a, item, tn, te, rn, s_rend);
-            s_item = item;
-            s_tnext = tn;
-            s_tend = te;
-            s_rnext = rn;
-            slots[cur ^ 1u] = sn;
-            if (sn.cnt) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
-        }
         // R tiles come before S tiles in every CTA's sequence: on the first S tile, R's counters go
         // to their row and the segment state starts over.
         if (sl.rel != phase_rel) {
@@ -1310,12 +1316,23 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 set_error(err, kErrSpinLimit);
-                // Let the copies this CTA issued land first (bounded): this buffer's, unless the stall
-                // hook withheld it (CTA 0's first tile), and the prefetch into the other one.
+                // Let this buffer's copy land first (bounded), unless the stall hook withheld it (CTA 0's
+                // first tile); nothing else is in flight (the next tile's copy is issued below).
                 if (!(a.test_stall && blockIdx.x == 0 && k == 0)) mbar_wait(bar0 + 8u * cur, (k >> 1) & 1u);
-                if (slots[cur ^ 1u].cnt) mbar_wait(bar0 + 8u * (cur ^ 1u), ((k + 1) >> 1) & 1u);
             }
             break;
+        }
+        // Prefetch the next tile into the other buffer: every thread has passed the barrier above, so
+        // the previous tile's staging and write-out, the last accesses to that buffer, are done.
+        if (tid == 0) {
+            uint32_t item = s_item, tn = s_tnext, te = s_tend, rn = s_rnext;
+            const SegSlot sn = seg_next_tile<STABLE_R>(a, item, tn, te, rn, s_rend);
+            s_item = item;
+            s_tnext = tn;
+            s_tend = te;
+            s_rnext = rn;
+            slots[cur ^ 1u] = sn;
+            if (sn.cnt) tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, sn.cnt * 16u, bar0 + 8u * (cur ^ 1u));
         }
 
         tuple_v v[ITEMS];
@@ -1380,12 +1397,14 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
             }
         }
         __syncthreads();
-        // Warp 0: digit starts in the staged tile and where each digit's run goes: the rest of its
-        // current segment, then (when that fills) a new segment. Lane l owns digits [l*K, l*K + K).
+        // Warp 0, step 1: digit starts in the staged tile, and which digits' runs need a new segment
+        // (a run that does not fit the rest of its current segment). Lane l owns digits [l*K, l*K + K).
+        uint32_t hv[K];      // warp 0: tile count of each owned digit
+        uint32_t exl = 0;    // warp 0: tuples (low 16 bits) and new segments (high 16 bits) before lane l
+        uint32_t ntot = 0;   // warp 0: new segments of the tile
         if (w == 0) {
             const int d0 = lane * K;
-            uint32_t hv[K];
-            uint32_t packed = 0;  // tuples (low 16 bits) and new segments (high 16 bits) of this lane
+            uint32_t packed = 0;
 #pragma unroll
             for (int j = 0; j < K; j++) {
                 hv[j] = d0 + j < F ? thist[d0 + j] : 0u;
@@ -1398,7 +1417,33 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
-            const uint32_t ntot = __shfl_sync(0xffffffffu, incl, 31) >> 16;
+            ntot = __shfl_sync(0xffffffffu, incl, 31) >> 16;
+            exl = incl - packed;
+            uint32_t ex = exl & 0xffffu;
+#pragma unroll
+            for (int j = 0; j < K; j++) {
+                const int d = d0 + j;
+                if (d < F) {
+                    thist[d] = 0;
+                    tdstart[d] = ex;
+                    ex += hv[j];
+                }
+            }
+        }
+        __syncthreads();
+        // Stage the tile sorted by digit, in place.
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
+            if (idx < cnt) {
+                const uint32_t d = (uint32_t)v[i].x & dmask;
+                buf[tdstart[d] + (STABLE_R && st ? (uint32_t)whist[w * F + d] : 0u) + rk[i]] = v[i];
+            }
+        }
+        // Warp 0, step 2 (while the other warps stage): where each digit's run goes, the rest of its
+        // current segment, then (when that fills) a new segment.
+        if (w == 0) {
+            const int d0 = lane * K;
             // New segment ids: first what is left of the slab, then a fresh slab.
             uint32_t old_lo = 0, old_rem = 0, nb = 0;
             if (ntot) {
@@ -1420,15 +1465,12 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 old_rem = __shfl_sync(0xffffffffu, old_rem, 0);
                 nb = __shfl_sync(0xffffffffu, nb, 0);
             }
-            const uint32_t exl = incl - packed;
             uint32_t ex = exl & 0xffffu, e = exl >> 16;
 #pragma unroll
             for (int j = 0; j < K; j++) {
                 const int d = d0 + j;
                 if (d < F) {
                     const uint32_t h = hv[j];
-                    thist[d] = 0;
-                    tdstart[d] = ex;
                     if (h) {
                         const uint32_t sc = scur[j], fill = sfill[j];
                         SegRun r;
@@ -1476,16 +1518,6 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
             }
         }
         __syncthreads();
-        // Stage the tile sorted by digit, in place.
-#pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
-            if (idx < cnt) {
-                const uint32_t d = (uint32_t)v[i].x & dmask;
-                buf[tdstart[d] + (STABLE_R && st ? (uint32_t)whist[w * F + d] : 0u) + rk[i]] = v[i];
-            }
-        }
-        __syncthreads();
         // Write each digit run: consecutive threads write consecutive 16-byte tuples (8-byte words).
         const bool z0 = a.z0 && sl.rel == 0;
         if (cnt == (uint32_t)T) {
@@ -1528,7 +1560,8 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 }
             }
         }
-        __syncthreads();
+        // No barrier here: the next tile's wait barrier orders this write-out before the next prefetch
+        // into this buffer and before the next tile's planning rewrites runs and tdstart.
     }
     // The counters of the relation in progress go to their row (the other row is complete).
     __syncthreads();
@@ -2449,7 +2482,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat, int test_flags) {
     uint32_t nlaunch = 0;
 #define HJ_PH(i) \
-    if (ph) HJ_CU(cudaEventRecord(ph[i], st))
+    if (ph) HJ_CU(record_event(ph[i], st))
     if (nR >= (1ull << 32) || nS >= (1ull << 32)) return HJ_E_INVAL;
     const int np = g.nparts();
     const int F1 = g.F1, F2 = g.F2;
@@ -2659,8 +2692,8 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         nlaunch++;
         HJ_PH(segm ? 3 : 3 + pass);
     }
-    if (ph && g.passes == 1) HJ_CU(cudaEventRecord(ph[4], st));
-    if (ev_mid) HJ_CU(cudaEventRecord(ev_mid, st));
+    if (ph && g.passes == 1) HJ_CU(record_event(ph[4], st));
+    if (ev_mid) HJ_CU(record_event(ev_mid, st));
 
     // 6. joins
     JoinArgs ja;
