@@ -81,9 +81,29 @@ int scratch_need(hj_algo_t algo, const hj_params_t &p, size_t nR, size_t nS, boo
     return HJ_OK;
 }
 
+// Drop the context's join graphs (they address the arena).
+void drop_graphs(hj_ctx *c) {
+    for (hj_graph_entry &e : c->graphs)
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+    c->graphs.clear();
+    c->last_key = hj_graph_key();
+}
+
+constexpr size_t kMaxJoinGraphs = 4;
+
+hj_graph_entry *find_graph(hj_ctx *c, const hj_graph_key &k) {
+    for (hj_graph_entry &e : c->graphs)
+        if (e.key == k) {
+            e.used = ++c->graph_tick;
+            return &e;
+        }
+    return nullptr;
+}
+
 int ensure_arena(hj_ctx *c, size_t bytes) {
     if (c->arena_bytes >= bytes) return HJ_OK;
     CU_OR(cudaStreamSynchronize(c->stream), HJ_E_DEVICE);
+    drop_graphs(c);
     if (c->arena) cudaFree(c->arena);
     c->arena = nullptr;
     c->arena_bytes = 0;
@@ -205,6 +225,7 @@ int hj_ctx_destroy(hj_ctx_t *c) {
         DeviceGuard g(c->device);
         std::lock_guard<std::mutex> lk(c->mu);
         if (c->stream) cudaStreamSynchronize(c->stream);
+        drop_graphs(c);
         if (c->arena) cudaFree(c->arena);
         if (c->acc_host) cudaFreeHost(c->acc_host);
         cudaEventDestroy(c->ev_h2d);
@@ -300,26 +321,88 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
         dR = r;
         dS = s;
     }
-    CU_OR(cudaMemsetAsync(acc, 0, sizeof(JoinAccum), st), out->status = HJ_E_DEVICE);
-    if (timing) CU_OR(cudaEventRecord(c->ev_start, st), out->status = HJ_E_DEVICE);
-    if (is_phj(algo)) {
-        hj::PhjScratch s;
-        hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s, seg);
-        rc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
-                             timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches, nullptr,
-                             ((p.flags & HJ_F_TEST_STALL) ? 1 : 0) | ((p.flags & HJ_F_WIDE) ? 2 : 0));
+    // Everything from the result reset to the result copy; a repeated device-resident join replays it
+    // from a CUDA graph (the key holds every input of the enqueued work).
+    auto enqueue = [&]() -> int {
+        if (cudaMemsetAsync(acc, 0, sizeof(JoinAccum), st) != cudaSuccess) return HJ_E_DEVICE;
+        if (timing && hj::record_event(c->ev_start, st) != cudaSuccess) return HJ_E_DEVICE;
+        int erc;
+        if (is_phj(algo)) {
+            hj::PhjScratch s;
+            hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s, seg);
+            erc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
+                                  timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches, nullptr,
+                                  ((p.flags & HJ_F_TEST_STALL) ? 1 : 0) | ((p.flags & HJ_F_WIDE) ? 2 : 0));
+        } else {
+            const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
+            erc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
+                                   timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
+        }
+        if (erc) return erc;
+        if (timing && hj::record_event(c->ev_end, st) != cudaSuccess) return HJ_E_DEVICE;
+        if (cudaMemcpyAsync(c->acc_host, acc, sizeof(JoinAccum), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return HJ_E_DEVICE;
+        return HJ_OK;
+    };
+    hj_graph_key key;
+    const bool graphable = !host_in && st == c->stream && !(p.flags & HJ_F_TEST_STALL);
+    if (graphable) {
+        key.algo = (int)algo;
+        key.R = R;
+        key.S = S;
+        key.nR = nR;
+        key.nS = nS;
+        key.flags = p.flags;
+        key.bits = p.num_radix_bits;
+        key.passes = p.num_passes;
+        key.bits_pass1 = p.radix_bits_pass1;
+        key.table_load = p.table_load;
+        key.seg = seg;
+        key.arena = c->arena;
+        key.arena_bytes = c->arena_bytes;
+    }
+    if (hj_graph_entry *ge = graphable ? find_graph(c, key) : nullptr) {
+        CU_OR(cudaGraphLaunch(ge->exec, st), out->status = HJ_E_DEVICE);
+        launches = ge->launches;
+    } else if (graphable && key == c->last_key) {
+        // Second identical call in a row: capture, instantiate, launch; keep the graph.
+        CU_OR(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), out->status = HJ_E_DEVICE);
+        rc = enqueue();
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        cudaGraphExec_t exec = nullptr;
+        if (!rc && ce == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+            if (c->graphs.size() >= kMaxJoinGraphs) {
+                size_t lru = 0;
+                for (size_t i = 1; i < c->graphs.size(); i++)
+                    if (c->graphs[i].used < c->graphs[lru].used) lru = i;
+                cudaGraphExecDestroy(c->graphs[lru].exec);
+                c->graphs.erase(c->graphs.begin() + (long)lru);
+            }
+            hj_graph_entry e;
+            e.key = key;
+            e.exec = exec;
+            e.launches = launches;
+            e.used = ++c->graph_tick;
+            c->graphs.push_back(e);
+        } else if (!rc) {
+            rc = HJ_E_DEVICE;
+        }
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (rc) {
+            if (exec) cudaGraphExecDestroy(exec);
+            return out->status = rc;
+        }
+        CU_OR(cudaGraphLaunch(exec, st), out->status = HJ_E_DEVICE);
     } else {
-        const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
-        rc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
-                              timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches);
+        rc = enqueue();
+        if (rc) {
+            cudaStreamSynchronize(st);
+            return out->status = rc;
+        }
     }
-    if (rc) {
-        cudaStreamSynchronize(st);
-        return out->status = rc;
-    }
-    if (timing) CU_OR(cudaEventRecord(c->ev_end, st), out->status = HJ_E_DEVICE);
-    CU_OR(cudaMemcpyAsync(c->acc_host, acc, sizeof(JoinAccum), cudaMemcpyDeviceToHost, st),
-          out->status = HJ_E_DEVICE);
+    if (graphable) c->last_key = key;
     if (p.watchdog_ms > 0) {
         // Host watchdog: poll the join's completion against a deadline instead of blocking.
         CU_OR(cudaEventRecord(c->ev_done, st), out->status = HJ_E_DEVICE);
