@@ -309,11 +309,13 @@ def run_ours(a, rank, world, local_rank):
     ctx = hj.Context(local_rank)
     pipe_flag = {"auto": 0, "segments": hj.HJ_F_SEGMENTS, "exact": hj.HJ_F_EXACT}[a.pipeline] | (
         hj.HJ_F_WIDE if a.wide else 0)
-    flags = hj.HJ_F_PHASE_TIMES | pipe_flag
+    # Timed steps carry no timing events (the library's own event records and elapsed-time queries
+    # would add host work to every step); the phase breakdown comes from extra untimed steps.
+    flags = hj.HJ_F_NO_TIMING | pipe_flag
 
-    def step():
+    def step(fl=flags):
         r = hj.join(a.algo, R, S, on_device=True, bits=a.bits, passes=a.passes, device=local_rank,
-                    stream=stream.cuda_stream, flags=flags, ctx=ctx)
+                    stream=stream.cuda_stream, flags=fl, ctx=ctx)
         if (r.matched_cnt, r.checksum) != want:
             raise RuntimeError(f"wrong result {(r.matched_cnt, r.checksum)} != {want}")
         return r
@@ -337,7 +339,8 @@ def run_ours(a, rank, world, local_rank):
         dist.barrier()
     ms = reduce_over_ranks(e0.elapsed_time(e1), dist, dev)
     value = whole_job_rate((nR + nS) * a.steps, world, ms / 1e3)
-    phases = {name: statistics.mean(r.phase[i] for r in results) for i, name in enumerate(hj.PHASES)}
+    phase_runs = [step(hj.HJ_F_PHASE_TIMES | pipe_flag) for _ in range(3)]
+    phases = {name: statistics.mean(r.phase[i] for r in phase_runs) for i, name in enumerate(hj.PHASES)}
     launches = sum(r.kernel_launches for r in results)
     seg_mode = a.algo.startswith("phj") and phases["hist"] == 0.0
 

@@ -51,7 +51,7 @@ struct NphjSide {
     unsigned long long kmax;     // largest build key (compact-slot test)
     unsigned long long ror;      // OR of all build row ids
     unsigned int sliced;         // the compact table is built (and probed) slice by slice
-    unsigned int pad;
+    unsigned int colscan_done;   // blocks of nphj_slice_colscan that have written their totals
 };
 
 constexpr unsigned long long kCompactEmpty = ~0ull;
@@ -89,6 +89,10 @@ struct NphjArgs {
     uint32_t *slice_hist;      // [hist_blocks][nslices] build tuples per (block, slice)
     uint32_t *slice_off;       // [hist_blocks][nslices] the block's offset inside the slice
     uint32_t *slice_start;     // [nslices + 1] first staging index of each slice
+    // Sliced builds: the kernels of the other table forms (clear, build, 16-byte probe) run inside the
+    // sliced build's own launches (scatter, slice build, compact probe) when the device finds that the
+    // table is not built by slices, instead of as launches of their own that return at once.
+    int fused_fallback;
 };
 
 __device__ __forceinline__ bool compact_sliced(const NphjSide *side) {
@@ -162,41 +166,9 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_widths(NphjArgs a) {
     }
 }
 
-// Per slice, the offset of every block's tuples inside the slice (an exclusive scan down the column
-// of the histogram) and the slice's total. 32 slices per CTA; warp w sums a contiguous run of rows.
-__global__ void __launch_bounds__(1024) nphj_slice_colscan(NphjArgs a, uint32_t *total) {
-    __shared__ uint32_t part[32][33];
-    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned sidx = blockIdx.x * 32 + lane;
-    const bool valid = sidx < a.nslices;
-    const unsigned rpw = (a.hist_blocks + 31) / 32;
-    const unsigned r0 = w * rpw, r1 = min(a.hist_blocks, r0 + rpw);
-    uint32_t sum = 0;
-    for (unsigned r = r0; r < r1 && valid; r++) sum += a.slice_hist[(size_t)r * a.nslices + sidx];
-    part[w][lane] = sum;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t run = 0;
-        for (int q = 0; q < 32; q++) {
-            const uint32_t v = part[q][lane];
-            part[q][lane] = run;
-            run += v;
-        }
-        if (valid) total[sidx] = run;
-    }
-    __syncthreads();
-    uint32_t run = part[w][lane];
-    for (unsigned r = r0; r < r1 && valid; r++) {
-        const size_t q = (size_t)r * a.nslices + sidx;
-        const uint32_t v = a.slice_hist[q];
-        a.slice_off[q] = run;
-        run += v;
-    }
-}
-
-// One CTA: the first staging index of every slice, and the mode of the build: sliced when the table
-// is compact and no slice is filled above kSliceMaxFill.
-__global__ void __launch_bounds__(1024) nphj_slice_plan(NphjArgs a, const uint32_t *total) {
+// One CTA (the last block of the column scan): the first staging index of every slice, and the mode of
+// the build: sliced when the table is compact and no slice is filled above kSliceMaxFill.
+__device__ __forceinline__ void slice_plan_body(const NphjArgs &a, const uint32_t *total) {
     __shared__ uint32_t scan_tmp[32];
     __shared__ uint32_t s_max;
     const unsigned n = a.nslices;
@@ -204,8 +176,9 @@ __global__ void __launch_bounds__(1024) nphj_slice_plan(NphjArgs a, const uint32
     const unsigned j0 = min(n, threadIdx.x * per), j1 = min(n, j0 + per);
     uint32_t sum = 0, mx = 0;
     for (unsigned j = j0; j < j1; j++) {
-        sum += total[j];
-        mx = max(mx, total[j]);
+        const uint32_t t = __ldcg(total + j);  // written by other blocks of the column scan
+        sum += t;
+        mx = max(mx, t);
     }
     if (threadIdx.x == 0) s_max = 0;
     __syncthreads();
@@ -234,7 +207,7 @@ __global__ void __launch_bounds__(1024) nphj_slice_plan(NphjArgs a, const uint32
     uint32_t run = scan_tmp[w] + incl - sum;
     for (unsigned j = j0; j < j1; j++) {
         a.slice_start[j] = run;
-        run += total[j];
+        run += __ldcg(total + j);
     }
     if (threadIdx.x == blockDim.x - 1) a.slice_start[n] = run;
     if (threadIdx.x == 0) {
@@ -243,10 +216,51 @@ __global__ void __launch_bounds__(1024) nphj_slice_plan(NphjArgs a, const uint32
     }
 }
 
+// Per slice, the offset of every block's tuples inside the slice (an exclusive scan down the column
+// of the histogram) and the slice's total. 32 slices per CTA; warp w sums a contiguous run of rows. The
+// last CTA to finish then plans the slices (slice_plan_body).
+__global__ void __launch_bounds__(1024) nphj_slice_colscan(NphjArgs a, uint32_t *total) {
+    __shared__ uint32_t part[32][33];
+    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned sidx = blockIdx.x * 32 + lane;
+    const bool valid = sidx < a.nslices;
+    const unsigned rpw = (a.hist_blocks + 31) / 32;
+    const unsigned r0 = w * rpw, r1 = min(a.hist_blocks, r0 + rpw);
+    uint32_t sum = 0;
+    for (unsigned r = r0; r < r1 && valid; r++) sum += a.slice_hist[(size_t)r * a.nslices + sidx];
+    part[w][lane] = sum;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t run = 0;
+        for (int q = 0; q < 32; q++) {
+            const uint32_t v = part[q][lane];
+            part[q][lane] = run;
+            run += v;
+        }
+        if (valid) total[sidx] = run;
+    }
+    __syncthreads();
+    uint32_t run = part[w][lane];
+    for (unsigned r = r0; r < r1 && valid; r++) {
+        const size_t q = (size_t)r * a.nslices + sidx;
+        const uint32_t v = a.slice_hist[q];
+        a.slice_off[q] = run;
+        run += v;
+    }
+    __shared__ bool s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&a.side->colscan_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    slice_plan_body(a, total);
+}
+
 // Empties the table the build will claim slots in: the 16-byte table when the keys or row ids are too
 // wide for compact slots, the compact table when it is built by global CAS. A table built by slices
 // is written whole by nphj_slice_build.
-__global__ void nphj_clear_table(NphjArgs a) {
+__device__ __forceinline__ void clear_table_body(const NphjArgs &a) {
     const bool compact = use_compact(a);
     if (compact && compact_sliced(a.side)) return;
     const unsigned long long words16 = compact ? a.ccap / 2 : a.cap;  // 16-byte units
@@ -255,11 +269,16 @@ __global__ void nphj_clear_table(NphjArgs a) {
         a.table[i] = make_ulonglong2(kEmpty, kEmpty);
 }
 
+__global__ void nphj_clear_table(NphjArgs a) { clear_table_body(a); }
+
 // Build tuples in slice order as compact words (key << 32 | row id); block b writes its tuples of
 // slice s from start[s] + off[b][s] on, ranked by shared-memory counters.
 __global__ void __launch_bounds__(kSliceThreads) nphj_slice_scatter(NphjArgs a) {
     extern __shared__ uint32_t sh_pos[];  // [nslices]
-    if (!compact_sliced(a.side)) return;
+    if (!compact_sliced(a.side)) {
+        if (a.fused_fallback) clear_table_body(a);
+        return;
+    }
     const uint32_t *off = a.slice_off + (size_t)blockIdx.x * a.nslices;
     for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) sh_pos[j] = a.slice_start[j] + off[j];
     __syncthreads();
@@ -292,9 +311,14 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_slice_scatter(NphjArgs a) 
 // First-match joins: a tuple whose key already has a slot lowers the slot's position (64-bit min on
 // key << 32 | position), and before the write-out each slot's position is replaced by the row id of
 // that build tuple.
+__device__ void build_body(const NphjArgs &a);
+
 __global__ void __launch_bounds__(kSliceThreads) nphj_slice_build(NphjArgs a) {
     extern __shared__ unsigned long long tab[];  // [kSliceSlots]
-    if (!compact_sliced(a.side)) return;
+    if (!compact_sliced(a.side)) {
+        if (a.fused_fallback) build_body(a);
+        return;
+    }
     bool seen_dup = false;
     unsigned long long *ctab = reinterpret_cast<unsigned long long *>(a.table);
     for (unsigned sl = blockIdx.x; sl < a.nslices; sl += gridDim.x) {
@@ -402,7 +426,9 @@ __device__ __forceinline__ void nphj_insert(const NphjArgs &a, const tuple_v t, 
     }
 }
 
-__global__ void nphj_build(NphjArgs a) {
+// Build of the table forms other than the sliced one: the compact table by global CAS, or the 16-byte
+// table. All threads of a block call it (block-wide vote at the end).
+__device__ void build_body(const NphjArgs &a) {
     constexpr int U = 4;
     bool seen_dup = false;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
@@ -440,6 +466,8 @@ __global__ void nphj_build(NphjArgs a) {
     }
     if (__syncthreads_or(seen_dup) && threadIdx.x == 0) atomicOr(&a.side->dup, 1u);
 }
+
+__global__ void nphj_build(NphjArgs a) { build_body(a); }
 
 // Duplicate-key rebuild for nphj_lp: one slot per distinct key holding the minimum input position.
 __global__ void nphj_lp_refill(NphjArgs a) {
@@ -490,9 +518,14 @@ __global__ void nphj_lp_resolve(NphjArgs a) {
 
 // Probe of a compact-slot table (see nphj_build); a no-op otherwise. Four probes per thread: the
 // 8-byte slots leave the registers for it.
+__device__ __forceinline__ void probe16_body(const NphjArgs &a, unsigned long long *red);
+
 __global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
     __shared__ unsigned long long red[64];
-    if (!use_compact(a)) return;
+    if (!use_compact(a)) {
+        if (a.fused_fallback) probe16_body(a, red);
+        return;
+    }
     // Compact slots: no build key is the empty pattern, so there is no side record; a probe key
     // at or above 2^32 - 1 cannot match.
     constexpr int V = 4;
@@ -545,10 +578,8 @@ __global__ void __launch_bounds__(256) nphj_probe_compact(NphjArgs a) {
 
 // Two probes per thread at eight 256-thread blocks per SM measured best for tables that sit in L2
 // (more probes per thread cost occupancy through registers).
-__global__ void __launch_bounds__(256, 8) nphj_probe(NphjArgs a) {
-    __shared__ unsigned long long red[64];
+__device__ __forceinline__ void probe16_body(const NphjArgs &a, unsigned long long *red) {
     constexpr int U = 2;
-    if (use_compact(a)) return;  // nphj_probe_compact probes instead
     ProbeArgs P;
     P.table = a.table;
     P.cap = a.cap;
@@ -574,6 +605,12 @@ __global__ void __launch_bounds__(256, 8) nphj_probe(NphjArgs a) {
         probe_group<U>(P, sv, valid, cnt, sum);
     }
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
+}
+
+__global__ void __launch_bounds__(256, 8) nphj_probe(NphjArgs a) {
+    __shared__ unsigned long long red[64];
+    if (use_compact(a)) return;  // nphj_probe_compact probes instead
+    probe16_body(a, red);
 }
 
 // Materialising probe: block-wide rounds of one probe tuple per thread; each thread counts its matches,
@@ -733,6 +770,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     // the sliced build's staging array, histograms and slice starts.
     a.ccap = (cap + kSliceSlots - 1) / kSliceSlots * kSliceSlots;
     a.nslices = 0;
+    a.fused_fallback = 0;
     a.hist_blocks = (unsigned)num_sms * 2;
     a.stage = nullptr;
     a.slice_hist = a.slice_off = a.slice_start = nullptr;
@@ -751,6 +789,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
             a.slice_off = reinterpret_cast<uint32_t *>(q + hist_bytes);
             a.slice_start = reinterpret_cast<uint32_t *>(q + 2 * hist_bytes);
             slice_total = reinterpret_cast<uint32_t *>(q + 2 * hist_bytes + (((ns + 1) * 4 + 255) & ~(size_t)255));
+            a.fused_fallback = 1;
         }
     }
     if (a.compact_ok) {
@@ -775,20 +814,19 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         nl++;
         if (a.nslices) {
             nphj_slice_colscan<<<(a.nslices + 31) / 32, 1024, 0, st>>>(a, slice_total);
-            nphj_slice_plan<<<1, 1024, 0, st>>>(a, slice_total);
-            nl += 2;
-        }
-        nphj_clear_table<<<num_sms * 2, 256, 0, st>>>(a);
-        nl++;
-        if (a.nslices) {
             nphj_slice_scatter<<<a.hist_blocks, kSliceThreads, hist_smem, st>>>(a);
             const unsigned bgrid = a.nslices < (unsigned)num_sms * 3 ? a.nslices : (unsigned)num_sms * 3;
             nphj_slice_build<<<bgrid, kSliceThreads, kSliceSlots * 8, st>>>(a);
-            nl += 2;
+            nl += 3;
+        } else {
+            nphj_clear_table<<<num_sms * 2, 256, 0, st>>>(a);
+            nl++;
         }
     }
-    nphj_build<<<fb_grid, 256, 0, st>>>(a);
-    nl++;
+    if (!a.fused_fallback) {
+        nphj_build<<<fb_grid, 256, 0, st>>>(a);
+        nl++;
+    }
     if (lp) {
         nphj_lp_refill<<<fb_grid, 256, 0, st>>>(a);
         nphj_lp_dedup_build<<<fb_grid, 256, 0, st>>>(a);
@@ -809,7 +847,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         if (mat) {
             nphj_probe_mat<<<grid, 256, 0, st>>>(a);
         } else {
-            nphj_probe<<<fb_grid, 256, 0, st>>>(a);
+            if (!a.fused_fallback) nphj_probe<<<fb_grid, 256, 0, st>>>(a);
             if (a.compact_ok) nphj_probe_compact<<<grid, 256, 0, st>>>(a);
         }
     }
@@ -818,7 +856,7 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
         HJ_CU(record_event(ph[5], st));
         HJ_CU(record_event(ph[6], st));
     }
-    if (launches) *launches = nl + (nS ? (mat || !a.compact_ok ? 1u : 2u) : 0u);
+    if (launches) *launches = nl + (nS ? (mat || !a.compact_ok || a.fused_fallback ? 1u : 2u) : 0u);
     return HJ_OK;
 }
 
