@@ -1138,11 +1138,10 @@ struct SegSlot {
 };
 
 // Where a digit's run of the staged tile goes: staged index j < split to base + j (the rest of the
-// current segment), j >= split to base + j + jump * kTile (the new segment).
+// current segment), j >= split to base2 + j (the new segment).
 struct SegRun {
-    long long base;
-    int jump;
-    uint32_t split;
+    long long base, base2;
+    uint32_t split, pad;
 };
 
 // Thread 0: the next tile of this CTA's current work item, claiming items as needed. STATIC_R: the build
@@ -1263,7 +1262,9 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
 
     int phase_rel = 0;           // relation whose tuples the counters and segment state hold
     uint32_t since = 0;          // upper bound of every counter (uniform)
-    unsigned long long kor = 0, ror = 0, rors = 0;
+    // ORs of the high 32 bits of build keys, build row ids and probe row ids: every width test
+    // (w8_fits, ci_applies, compact_applies) compares with a power of two of 2^32 or more.
+    uint32_t kor = 0, ror = 0, rors = 0;
     __shared__ uint32_t s_max[THREADS / 32];
 
     for (uint32_t k = 0;; k++) {
@@ -1338,22 +1339,38 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         tuple_v v[ITEMS];
         uint32_t rk[ITEMS];
         const bool st = STABLE_R && sl.rel == 0;  // uniform: this tile takes the stable rank
+        uint32_t xo = 0, yo = 0;
+        if (cnt == (uint32_t)T) {
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
-            if (idx < cnt) {
-                v[i] = buf[idx];
+            for (int i = 0; i < ITEMS; i++) {
+                v[i] = buf[w * 32 * ITEMS + i * 32 + lane];
                 const uint32_t d = (uint32_t)v[i].x & dmask;
                 if (!st) rk[i] = atomicAdd(&thist[d], 1u);
                 const uint32_t bin = (uint32_t)(v[i].x & bmask);
                 atomicAdd(&jh[bin >> 1], 1u << ((bin & 1u) << 4));
-                if (sl.rel == 0) {
-                    kor |= v[i].x;
-                    ror |= v[i].y;
-                } else {
-                    rors |= v[i].y;
+                xo |= (uint32_t)(v[i].x >> 32);
+                yo |= (uint32_t)(v[i].y >> 32);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
+                if (idx < cnt) {
+                    v[i] = buf[idx];
+                    const uint32_t d = (uint32_t)v[i].x & dmask;
+                    if (!st) rk[i] = atomicAdd(&thist[d], 1u);
+                    const uint32_t bin = (uint32_t)(v[i].x & bmask);
+                    atomicAdd(&jh[bin >> 1], 1u << ((bin & 1u) << 4));
+                    xo |= (uint32_t)(v[i].x >> 32);
+                    yo |= (uint32_t)(v[i].y >> 32);
                 }
             }
+        }
+        if (sl.rel == 0) {
+            kor |= xo;
+            ror |= yo;
+        } else {
+            rors |= yo;
         }
         if (STABLE_R && st) {
             // Stable rank within the warp: items in order, lanes in order; the lanes holding one digit
@@ -1475,8 +1492,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                         const uint32_t sc = scur[j], fill = sfill[j];
                         SegRun r;
                         if (sc != kSegNone && fill + h <= SEGW) {
-                            r.base = (long long)sc * SEGW + fill - ex;
-                            r.jump = 0;
+                            r.base = r.base2 = (long long)sc * SEGW + fill - ex;
                             r.split = ex + h;
                             sfill[j] = fill + h;
                         } else {
@@ -1486,8 +1502,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                                 if (sc == kSegNone) {
                                     // The whole run starts the chain.
                                     a.seg_head[((size_t)phase_rel * G + c) * F + d] = id;
-                                    r.base = (long long)id * SEGW - ex;
-                                    r.jump = 0;
+                                    r.base = r.base2 = (long long)id * SEGW - ex;
                                     r.split = ex + h;
                                     sfill[j] = h;
                                 } else {
@@ -1495,7 +1510,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                                     // id: staged index ex + (SEGW - fill) lands at id * SEGW.
                                     a.seg_next[sc] = id;
                                     r.base = (long long)sc * SEGW + fill - ex;
-                                    r.jump = (int)id - (int)sc - 1;
+                                    r.base2 = r.base + ((long long)id - (long long)sc - 1) * SEGW;
                                     r.split = ex + (SEGW - fill);
                                     sfill[j] = h - (SEGW - fill);
                                 }
@@ -1504,8 +1519,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                                 // Cannot happen with the storage phj_carve reserves; the run's
                                 // stores fail their bounds check and report it.
                                 set_error(err, kErrCapacity);
-                                r.base = -(long long)cap - (long long)SEGW;
-                                r.jump = 0;
+                                r.base = r.base2 = -(long long)cap - (long long)SEGW;
                                 r.split = ex + h;
                                 scur[j] = kSegNone;
                                 sfill[j] = 0;
@@ -1519,7 +1533,8 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         }
         __syncthreads();
         // Write each digit run: consecutive threads write consecutive 16-byte tuples (8-byte words).
-        const bool z0 = a.z0 && sl.rel == 0;
+        // A destination outside the segment storage (negative included) fails the unsigned bound check.
+        const bool z0 = STABLE_R && a.z0 && sl.rel == 0;
         if (cnt == (uint32_t)T) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
@@ -1531,11 +1546,11 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 for (int i = 0; i < ITEMS / 2; i++) {
                     const uint32_t j = (uint32_t)(tid + (hh * ITEMS / 2 + i) * THREADS);
                     const SegRun r = runs[(uint32_t)t[i].x & dmask];
-                    dst[i] = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * SEGW);
+                    dst[i] = (j < r.split ? r.base : r.base2) + (long long)j;
                 }
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) {
-                    if (dst[i] >= 0 && (uint64_t)dst[i] < cap) {
+                    if ((uint64_t)dst[i] < cap) {
                         if (W8)
                             st_stream8(out8 + dst[i], w8_word_z0(t[i].x, t[i].y, a.b1, z0));
                         else
@@ -1549,8 +1564,8 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
             for (uint32_t j = tid; j < cnt; j += THREADS) {
                 const tuple_v t = buf[j];
                 const SegRun r = runs[(uint32_t)t.x & dmask];
-                const long long dst = r.base + (long long)j + (j < r.split ? 0ll : (long long)r.jump * SEGW);
-                if (dst >= 0 && (uint64_t)dst < cap) {
+                const long long dst = (j < r.split ? r.base : r.base2) + (long long)j;
+                if ((uint64_t)dst < cap) {
                     if (W8)
                         st_stream8(out8 + dst, w8_word_z0(t.x, t.y, a.b1, z0));
                     else
@@ -1574,9 +1589,9 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
     }
     if (lane == 0 && (kor | ror | rors)) {
         unsigned long long *mx = reinterpret_cast<unsigned long long *>(a.counters + kCtrMaxKey);
-        if (kor) atomicOr(mx, kor);
-        if (ror) atomicOr(mx + 1, ror);
-        if (rors) atomicOr(mx + 2, rors);
+        if (kor) atomicOr(mx, (unsigned long long)kor << 32);
+        if (ror) atomicOr(mx + 1, (unsigned long long)ror << 32);
+        if (rors) atomicOr(mx + 2, (unsigned long long)rors << 32);
     }
 }
 
