@@ -948,15 +948,24 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         // Elements of this tile: warp w owns [w*32*ITEMS, (w+1)*32*ITEMS), one row of 32 per item.
         E v[ITEMS];
         uint32_t d[ITEMS];
+        const bool full = cnt == (uint32_t)T;
+        if (full) {
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
-            if (idx < cnt) {
-                v[i] = buf[idx];
+            for (int i = 0; i < ITEMS; i++) {
+                v[i] = buf[w * 32 * ITEMS + i * 32 + lane];
                 d[i] = elem_digit(v[i], a.shift, dmask);
-            } else {
-                v[i] = E{};
-                d[i] = (uint32_t)F;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
+                if (idx < cnt) {
+                    v[i] = buf[idx];
+                    d[i] = elem_digit(v[i], a.shift, dmask);
+                } else {
+                    v[i] = E{};
+                    d[i] = (uint32_t)F;
+                }
             }
         }
         uint32_t rk[ITEMS];
@@ -1045,7 +1054,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
             const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
-            if (idx < cnt) {
+            if (full || idx < cnt) {
                 const uint32_t di = elem_digit(v[i], a.shift, dmask);
                 const uint32_t pos = tdstart[di] + (STABLE ? whist[w * F + di] : 0u) + rk[i];
                 buf[pos] = v[i];
@@ -1055,9 +1064,11 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         // Write each digit run: consecutive threads write consecutive 16-byte tuples (8-byte words for
         // compact final partitions). Full tiles load their staged tuples in two halves so that the stores
         // issue back to back.
+        // A destination outside the output (negative included) fails the unsigned bound check. Build
+        // key-0 words (first-match joins) exist only in the stable launches of the build relation.
         unsigned long long *out8 = sl.out == a.outS ? a.outS8 : a.outR8;
-        const bool z0 = a.ci_z0 && sl.out == a.outR;
-        if (cnt == (uint32_t)T) {
+        const bool z0 = STABLE && a.ci_z0 && sl.out == a.outR;
+        if (full) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
                 E t[ITEMS / 2];
@@ -1069,7 +1080,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
                     dst[i] = gbase[elem_digit(t[i], a.shift, dmask)] + (long long)(tid + (hh * ITEMS / 2 + i) * THREADS);
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) {
-                    if (dst[i] >= 0 && (uint64_t)dst[i] < sl.out_len)
+                    if ((uint64_t)dst[i] < sl.out_len)
                         store_elem(t[i], sl.out, out8, dst[i], ci, a.bits, b2, z0);
                     else
                         set_error(err, kErrBounds);
@@ -1079,7 +1090,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         for (uint32_t j = tid; j < cnt; j += THREADS) {
             const E t = buf[j];
             const long long dst = gbase[elem_digit(t, a.shift, dmask)] + (long long)j;
-            if (dst >= 0 && (uint64_t)dst < sl.out_len)
+            if ((uint64_t)dst < sl.out_len)
                 store_elem(t, sl.out, out8, dst, ci, a.bits, b2, z0);
             else
                 set_error(err, kErrBounds);
