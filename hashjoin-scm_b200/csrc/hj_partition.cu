@@ -1679,18 +1679,19 @@ __device__ __forceinline__ bool compact_applies(const JoinArgs &a) {
 
 constexpr size_t kCompactSmem = (size_t)kCompactCap * (4 + 4 + 2 + 2);
 
-// Partition join with 4-byte keys (key >> bits) and 4-byte row ids in shared memory: 96 KiB per CTA,
+// Partition join with 4-byte keys (key >> bits) and 4-byte row ids in shared memory, packed into one
+// 8-byte word per build tuple (key-high << 32 | row id: one load per visited node): 96 KiB per CTA,
 // two CTAs per SM, so one CTA's build overlaps the other's probe. Same results as join_small_kernel;
 // within a partition the low `bits` key bits are equal, so comparing key >> bits is comparing keys.
 // MAT: write one (r.row_id, s.row_id) pair per match (the ptr_* joins) instead of summing; the probe
-// then runs in block-wide rounds (count, reserve output slots, walk again and write).
-template <bool MAT, bool CI = false>
+// then runs in block-wide rounds (count, reserve output slots, walk again and write). LP: first match
+// (the lowest build position) per probe tuple.
+template <bool MAT, bool CI = false, bool LP = false>
 __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
-    uint32_t *rkey = reinterpret_cast<uint32_t *>(smem);         // [kCompactCap]
-    uint32_t *rrid = rkey + kCompactCap;                           // [kCompactCap]
-    uint16_t *head = reinterpret_cast<uint16_t *>(rrid + kCompactCap);  // [kCompactCap]
-    uint16_t *nxt = head + kCompactCap;                            // [kCompactCap]
+    unsigned long long *rw = reinterpret_cast<unsigned long long *>(smem);  // [kCompactCap]
+    uint16_t *head = reinterpret_cast<uint16_t *>(rw + kCompactCap);         // [kCompactCap]
+    uint16_t *nxt = head + kCompactCap;                                      // [kCompactCap]
     __shared__ unsigned long long red[64];
     __shared__ uint32_t s_item;
     __shared__ uint32_t scan_tmp[32];
@@ -1703,7 +1704,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
     if (CI != (!MAT && a.ci && ci_applies(a.counters, a.bits))) return;
     constexpr bool ci = CI;
     const int B = ci ? 0 : a.bits;  // shift from a stored x to the key's bits above the radix bits
-    const bool lp = a.lp != 0;
+    constexpr bool lp = LP;
     const bool skip0 = a.skip0 != 0;
     unsigned long long cnt = 0, sum = 0;
     for (;;) {
@@ -1733,8 +1734,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
             for (int u = 0; u < 4; u++) {
                 const uint32_t i = i0 + u * kCompactThreads;
                 if (i >= nr) continue;
-                rkey[i] = (uint32_t)(t[u].x >> B);
-                rrid[i] = (uint32_t)t[u].y;
+                rw[i] = ((t[u].x >> B) << 32) | (t[u].y & 0xffffffffull);
                 if (!ci && skip0 && t[u].x == 0) continue;
                 nxt[i] = (uint16_t)atomic_exch_u16(&head[(t[u].x >> B) & hmask], i + 1);
             }
@@ -1760,7 +1760,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                     const uint64_t khi = sv[u].x >> B;
                     uint32_t e = head[khi & hmask], steps = 0;
                     while (e) {
-                        if ((uint64_t)rkey[e - 1] == khi) {
+                        if ((rw[e - 1] >> 32) == khi) {
                             if (!lp) mm[u]++;
                             else if (best[u] == 0 || e < best[u]) best[u] = e;
                         }
@@ -1779,13 +1779,14 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 for (int u = 0; u < U; u++) {
                     if (!mm[u]) continue;
                     if (lp) {
-                        mat_put(a.mat, o++, rrid[best[u] - 1], sv[u].y, err);
+                        mat_put(a.mat, o++, rw[best[u] - 1] & 0xffffffffull, sv[u].y, err);
                         continue;
                     }
                     const uint64_t khi = sv[u].x >> B;
                     uint32_t e = head[khi & hmask], steps = 0;
                     while (e && steps++ <= nr) {
-                        if ((uint64_t)rkey[e - 1] == khi) mat_put(a.mat, o++, rrid[e - 1], sv[u].y, err);
+                        const unsigned long long w = rw[e - 1];
+                        if ((w >> 32) == khi) mat_put(a.mat, o++, w & 0xffffffffull, sv[u].y, err);
                         e = nxt[e - 1];
                     }
                 }
@@ -1808,12 +1809,13 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 uint32_t e = head[khi & hmask];
                 uint32_t best = 0, steps = 0;
                 while (e) {
-                    if ((uint64_t)rkey[e - 1] == khi) {
+                    const unsigned long long w = rw[e - 1];
+                    if ((w >> 32) == khi) {
                         if (lp) {
                             if (best == 0 || e < best) best = e;
                         } else {
                             cnt++;
-                            sum += (unsigned long long)rrid[e - 1] + sv[u].y;
+                            sum += (w & 0xffffffffull) + sv[u].y;
                         }
                     }
                     e = nxt[e - 1];
@@ -1824,7 +1826,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 }
                 if (lp && best) {
                     cnt++;
-                    sum += (unsigned long long)rrid[best - 1] + sv[u].y;
+                    sum += (rw[best - 1] & 0xffffffffull) + sv[u].y;
                 }
             }
         }
@@ -2494,6 +2496,12 @@ int phj_prepare_device() {
                                (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kCompactSmem));
+    HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kCompactSmem));
+    HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kCompactSmem));
+    HJ_CU(cudaFuncSetAttribute(join_compact_kernel<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kCompactSmem));
     HJ_CU(cudaFuncSetAttribute(join_small_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJoinSmem));
     HJ_CU(cudaFuncSetAttribute(join_compact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kCompactSmem));
@@ -2739,15 +2747,24 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     ja.finS8 = ja.finR8 + nR;
     ja.w8_b1 = seg_words ? g.b1 : -1;
     if (mat) {
-        join_compact_kernel<true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+        if (lp)
+            join_compact_kernel<true, false, true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+        else
+            join_compact_kernel<true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
         join_small_kernel<true><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
     } else {
         // One launch per partition layout (tuples, compact words); the one that does not match the
         // device's choice returns at once.
-        join_compact_kernel<false, false><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+        if (lp)
+            join_compact_kernel<false, false, true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+        else
+            join_compact_kernel<false, false><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
         join_small_kernel<false, false><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
         if (ci_ok) {
-            join_compact_kernel<false, true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+            if (lp)
+                join_compact_kernel<false, true, true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
+            else
+                join_compact_kernel<false, true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);
             join_small_kernel<false, true><<<num_sms, kJoinThreads, kJoinSmem, st>>>(ja);
             nlaunch += 2;
         }
