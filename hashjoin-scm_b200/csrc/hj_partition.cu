@@ -815,6 +815,39 @@ __device__ __forceinline__ uint32_t tile_copy_bytes(uint32_t cnt) {
     return sizeof(E) == 16 ? cnt * 16u : ((cnt + 1u) & ~1u) * (uint32_t)sizeof(E);
 }
 
+// Lanes of the warp whose digit equals this lane's: one ballot per digit bit (NB bits).
+template <int NB>
+__device__ __forceinline__ unsigned digit_peers(uint32_t d) {
+    unsigned peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const unsigned bit = (d >> b) & 1u;
+        const unsigned bal = __ballot_sync(0xffffffffu, bit);
+        peers &= bal ^ (bit - 1u);  // bit ? bal : ~bal
+    }
+    return peers;
+}
+
+// The same for a digit width known only at run time (at most 9 bits; uniform across the warp).
+__device__ __forceinline__ unsigned digit_peers_n(uint32_t d, int nbits) {
+    switch (nbits) {
+        case 6: return digit_peers<6>(d);
+        case 7: return digit_peers<7>(d);
+        case 8: return digit_peers<8>(d);
+        default: break;
+    }
+    unsigned peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 9; b++) {
+        if (b < nbits) {
+            const unsigned bit = (d >> b) & 1u;
+            const unsigned bal = __ballot_sync(0xffffffffu, bit);
+            peers &= bal ^ (bit - 1u);
+        }
+    }
+    return peers;
+}
+
 // Digit of an element in this pass: (key >> shift) & mask; a word holds key >> b1, which is pass 2's shift.
 __device__ __forceinline__ uint32_t elem_digit(const tuple_v &v, int shift, uint64_t dmask) {
     return (uint32_t)((v.x >> shift) & dmask);
@@ -979,15 +1012,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             const int nbits = a.logF + (cnt < (uint32_t)T ? 1 : 0);
 #pragma unroll
             for (int i = 0; i < ITEMS; i++) {
-                unsigned peers = 0xffffffffu;
-#pragma unroll
-                for (int b = 0; b < 9; b++) {
-                    if (b < nbits) {
-                        const unsigned bit = (d[i] >> b) & 1u;
-                        const unsigned bal = __ballot_sync(0xffffffffu, bit);
-                        peers &= bit ? bal : ~bal;
-                    }
-                }
+                const unsigned peers = digit_peers_n(d[i], nbits);
                 const bool valid = d[i] < (uint32_t)F;
                 uint32_t pre = 0;
                 if (valid) pre = wh[d[i]];
@@ -1390,20 +1415,16 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
             for (int j = lane; j < F; j += 32) wh[j] = 0;
             __syncwarp();
             const unsigned ltmask = lanemask_lt();
-            const int nbits = a.b1 + (cnt < (uint32_t)T ? 1 : 0);
+            // Digit bits: K = F1 / 32 for K >= 2 gives log2(F1) exactly; K = 1 covers F1 <= 32 with 5
+            // bits (the unused high bits are zero in every lane). A partial tile's padding lanes carry
+            // digit F1, one bit more.
+            constexpr int NB = K == 1 ? 5 : K == 2 ? 6 : K == 4 ? 7 : 8;
+            const bool fullt = cnt == (uint32_t)T;
 #pragma unroll
             for (int i = 0; i < ITEMS; i++) {
                 const uint32_t idx = (uint32_t)(w * 32 * ITEMS + i * 32 + lane);
                 const uint32_t d = idx < cnt ? (uint32_t)v[i].x & dmask : (uint32_t)F;
-                unsigned peers = 0xffffffffu;
-#pragma unroll
-                for (int b = 0; b < 9; b++) {
-                    if (b < nbits) {
-                        const unsigned bit = (d >> b) & 1u;
-                        const unsigned bal = __ballot_sync(0xffffffffu, bit);
-                        peers &= bit ? bal : ~bal;
-                    }
-                }
+                const unsigned peers = fullt ? digit_peers<NB>(d) : digit_peers<NB + 1>(d);
                 const bool valid = d < (uint32_t)F;
                 uint32_t pre = 0;
                 if (valid) pre = wh[d];
