@@ -104,16 +104,45 @@ def workload_config(a, n_gpus):
 # GPU clock sampling during the timed region
 # ---------------------------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock, its maximum, power and the clock-event (throttle) reasons of this GPU, sampled every 5 ms
+    through NVML in a background thread (nvidia-smi every 200 ms when NVML is not importable). stop()
+    reports the samples inside the timed region when one is given (the host's bracket around the timed
+    steps, which end with a synchronize), else those under load."""
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    BITS = (0x8, 0x40, 0x20, 0x4)  # NVML clock-event reason bits, in the order of NAMES
     FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, bus_id: str | None):
         self.bus_id = (bus_id or "").lower()
+        self.samples = []  # (t, sm_mhz, max_mhz, reason_names, util)
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.stop_flag = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        for i in range(pynvml.nvmlDeviceGetCount()):
+            h = pynvml.nvmlDeviceGetHandleByIndex(i)
+            bus = pynvml.nvmlDeviceGetPciInfo(h).busId
+            bus = (bus.decode() if isinstance(bus, bytes) else bus).lower()
+            if not self.bus_id or bus.endswith(self.bus_id):
+                return pynvml, h
+        return None
 
     def start(self):
+        try:
+            got = self._nvml_handle()
+        except Exception:
+            got = None
+        if got:
+            self.nvml, self.handle = got
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
                                           "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
@@ -123,45 +152,59 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml, self.handle
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = get_reasons(h)
+                util = nv.nvmlDeviceGetUtilizationRates(h).gpu
+                names = [n for n, b in zip(self.NAMES, self.BITS) if bits & b]
+                self.samples.append((time.monotonic(), float(sm), float(mx), names, float(util)))
+            except Exception:
+                pass
+            time.sleep(0.005)
+
     def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.thread.join(timeout=2)
-        rows = []
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 10:
-                continue
-            if self.bus_id and not parts[1].lower().endswith(self.bus_id):
-                continue
-            rows.append(parts)
-        if not rows:
-            return None
-
         def num(x):
             try:
                 return float(x.split()[0])
             except (ValueError, IndexError):
                 return None
 
-        # Samples taken while the GPU was busy (utilization >= 50%); all samples when none were.
-        loaded = [r for r in rows if len(r) > 10 and (num(r[10]) or 0) >= 50] or rows
-        sm = [num(r[2]) for r in loaded if num(r[2]) is not None]
-        mx = [num(r[3]) for r in rows if num(r[3]) is not None]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows), "samples_under_load": len(loaded) if loaded is not rows
-                else 0}
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.strip().split(",")]
+            if len(parts) < 11 or (self.bus_id and not parts[1].lower().endswith(self.bus_id)):
+                continue
+            names = [n for i, n in enumerate(self.NAMES) if parts[6 + i].lower().startswith("active")]
+            self.samples.append((time.monotonic(), num(parts[2]), num(parts[3]), names, num(parts[10]) or 0.0))
+
+    def stop(self, window=None):
+        if self.nvml:
+            self.stop_flag.set()
+            self.thread.join(timeout=2)
+        elif self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+        else:
+            return None
+        rows = [r for r in self.samples if r[1] is not None]
+        if not rows:
+            return None
+        inside = [r for r in rows if window and window[0] <= r[0] <= window[1]]
+        loaded = [r for r in rows if r[4] >= 50]
+        use = inside or loaded or rows
+        reasons = sorted({n for r in use for n in r[3]})
+        return {"sm_mhz": statistics.median(r[1] for r in use), "sm_max_mhz": max(r[2] for r in rows),
+                "reasons": reasons, "samples": len(rows), "samples_in_timed_region": len(inside),
+                "samples_under_load": len(loaded), "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def reduce_over_ranks(value: float, dist, device, op: str = "max") -> float:
@@ -330,11 +373,13 @@ def run_ours(a, rank, world, local_rank):
     time.sleep(0.3)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    t_win0 = time.monotonic()
     e0.record(stream)
     results = [step() for _ in range(a.steps)]
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    clocks = sampler.stop()
+    t_win1 = time.monotonic()
+    clocks = sampler.stop((t_win0, t_win1))
     if dist:
         dist.barrier()
     ms = reduce_over_ranks(e0.elapsed_time(e1), dist, dev)

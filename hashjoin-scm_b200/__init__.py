@@ -66,6 +66,7 @@ HJ_F_PHASE_TIMES = 0x4
 HJ_F_SEGMENTS = 0x20  # radix joins counting every match: segment mode at any size
 HJ_F_EXACT = 0x40     # radix joins: always the histogram pass and exact pass-1 offsets
 HJ_F_WIDE = 0x80      # radix joins: 16-byte tuples in every partition pass (no 8-byte words)
+HJ_F_WORDS = 0x200    # radix joins: 8-byte words in every pass whenever the widths allow
 PHASES = ("hist", "plan", "pass1", "pass2", "join", "large")
 
 

@@ -332,7 +332,8 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
             hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s, seg);
             erc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
                                   timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches, nullptr,
-                                  ((p.flags & HJ_F_TEST_STALL) ? 1 : 0) | ((p.flags & HJ_F_WIDE) ? 2 : 0));
+                                  ((p.flags & HJ_F_TEST_STALL) ? 1 : 0) | ((p.flags & HJ_F_WIDE) ? 2 : 0) |
+                                      ((p.flags & HJ_F_WORDS) ? 4 : 0));
         } else {
             const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
             erc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,

@@ -636,9 +636,14 @@ struct ScatterArgs {
     int ci_out;
     int ci_z0;                  // build key 0 never matches: its compact words take ci_word_z0's high part
     unsigned long long *outR8, *outS8;
-    // Segment mode after a pass 1 that may have written 8-byte words: 1 = this launch reads words (runs
-    // when w8_fits holds), 2 = this launch reads tuples (runs when it does not); 0 = no such pass 1.
+    // After a pass 1 that may have written 8-byte words: 1 = this launch reads words (runs when w8_fits
+    // holds), 2 = this launch reads tuples (runs when it does not); 0 = no such pass 1.
     int w8;
+    // Exact-offset pipeline: pass 1 stores 8-byte words (w8_word) at outR8 / outS8 when w8_fits holds,
+    // and the word launch of pass 2 reads its units from inR8 / inS8 (word offsets, which may be odd:
+    // such a tile's copy starts one word early and the tile skips it).
+    int w8_out;
+    const unsigned long long *inR8, *inS8;
 };
 
 // A tile claimed for processing: its source, length, output region and owning work item.
@@ -649,7 +654,7 @@ struct TileSlot {
     uint32_t item;   // work item (valid flag: item != ~0u)
     uint32_t cnt;    // tuples in this tile
     uint32_t first;  // first tile of its item: the item's digit offsets must be loaded
-    uint32_t pad;
+    uint32_t pad;    // elements before the tile's first in its copy (a word tile at an odd offset)
 };
 
 // Thread-0 state of the work-item iterator.
@@ -706,6 +711,8 @@ __device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item,
         if (a.seg_head) {
             it.in = a.inR;
             it.seg = ah.seg;
+        } else if (a.w8 == 1) {
+            it.in = reinterpret_cast<const tuple_v *>((rel ? a.inS8 : a.inR8) + ah.off);
         } else {
             it.in = (rel ? a.inS : a.inR) + ah.off;
         }
@@ -718,7 +725,7 @@ __device__ __forceinline__ void item_decode(const ScatterArgs &a, uint32_t item,
 // tuples. Returns a slot with item == ~0u when the work is exhausted. Segment mode: `pend` carries
 // seg_next of the tile returned last, loaded then so that its latency passes while that tile is
 // processed.
-template <int T>
+template <int T, bool WIN = false>
 __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it, uint32_t nitems,
                                               uint32_t &pend, ItemAhead &ah) {
     TileSlot s;
@@ -763,12 +770,19 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
     }
     s.item = it.item;
     // A segment is kTile tuples (32 KB) in either layout; T counts the launch's elements per tile.
-    s.in = a.seg_head ? it.in + (uint64_t)it.seg * kTile : it.in + it.done;
+    s.pad = 0;
+    if (WIN && !a.seg_head) {
+        // Words at an odd offset: copy from one word earlier (bulk copies start on 16 bytes).
+        const unsigned long long *p = reinterpret_cast<const unsigned long long *>(it.in) + it.done;
+        s.pad = (reinterpret_cast<uintptr_t>(p) & 8u) ? 1u : 0u;
+        s.in = reinterpret_cast<const tuple_v *>(p - s.pad);
+    } else {
+        s.in = a.seg_head ? it.in + (uint64_t)it.seg * kTile : it.in + it.done;
+    }
     s.out = it.out;
     s.out_len = it.out_len;
     s.cnt = (uint32_t)(it.len - it.done < (uint64_t)T ? it.len - it.done : (uint64_t)T);
     s.first = it.done == 0;
-    s.pad = 0;
     it.done += s.cnt;
     if (a.seg_head && it.done < it.len) pend = a.seg_next[it.seg];
     return s;
@@ -783,14 +797,16 @@ __device__ __forceinline__ TileSlot next_tile(const ScatterArgs &a, ItemIter &it
 // Store one element of the last pass: a tuple, its compact final word (ci), or - from an 8-byte word of
 // a segment-mode pass 1, which holds key >> b1 - the final word with key >> bits.
 __device__ __forceinline__ void store_elem(const tuple_v &t, tuple_v *out, unsigned long long *out8, long long dst,
-                                           bool ci, int bits, int, bool z0) {
-    if (ci)
+                                           bool ci, int bits, int, bool z0, bool w8o, int b1) {
+    if (w8o)
+        st_stream8(out8 + dst, w8_word_z0(t.x, t.y, b1, z0));
+    else if (ci)
         st_stream8(out8 + dst, ci_word_z0(t.x, t.y, bits, z0));
     else
         st_stream(out + dst, t);
 }
 __device__ __forceinline__ void store_elem(unsigned long long w, tuple_v *, unsigned long long *out8, long long dst,
-                                           bool, int, int b2, bool z0) {
+                                           bool, int, int b2, bool z0, bool, int) {
     // A pass-1 high part with bit 31 set is a probe key beyond every build key, or (z0) a build key 0.
     const unsigned long long h1 = w >> 32;
     const unsigned long long h = h1 < 0x80000000ull ? h1 >> b2 : (z0 ? 0x80000000ull : 0xffffffffull);
@@ -865,9 +881,12 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     // ranks: measured faster there, as the rank's ballots keep warp 0 busy after the barrier).
     constexpr bool LATE = NBUF == 2 && !STABLE;
     constexpr int NW = THREADS / 32;
+    // Buffer stride: word tiles keep two spare words for a copy that starts one word early (and is
+    // rounded up to whole 16-byte units).
+    constexpr int ST = T + (WIN ? 2 : 0);
     extern __shared__ __align__(128) unsigned char smem[];
-    E *inbuf = reinterpret_cast<E *>(smem);                              // [NBUF][T]
-    long long *gbase = reinterpret_cast<long long *>(inbuf + NBUF * T);  // [256]
+    E *inbuf = reinterpret_cast<E *>(smem);                               // [NBUF][ST]
+    long long *gbase = reinterpret_cast<long long *>(inbuf + NBUF * ST);  // [256]
     long long *running = gbase + 256;                                   // [256]
     uint32_t *tdstart = reinterpret_cast<uint32_t *>(running + 256);    // [256]
     uint16_t *whist = reinterpret_cast<uint16_t *>(tdstart + 256);      // STABLE: [NW][F]
@@ -887,6 +906,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
     const uint32_t bar0 = smem_addr(&bars[0]);
     const int nbins = 1 << a.bits;
     const bool ci = a.ci_out && ci_applies(a.counters, a.bits);
+    const bool w8o = a.w8_out && w8_fits(a.counters, a.b1);  // pass 1 of the exact pipeline stores words
     const int b2 = a.bits - a.b1;
     if (a.w8 && (a.w8 == 1) != w8_fits(a.counters, a.b1)) return;  // the other layout's launch runs
     __shared__ ItemIter it;  // used by thread 0 only
@@ -905,10 +925,10 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         if (NBUF == 2) {
-            const TileSlot s0 = next_tile<T>(a, it, nitems, pend, ah);
+            const TileSlot s0 = next_tile<T, WIN>(a, it, nitems, pend, ah);
             slots[0] = s0;
             if (s0.item != ~0u && !(a.test_stall && blockIdx.x == 0))
-                tma_load_1d(inbuf, s0.in, tile_copy_bytes<E>(s0.cnt), bar0);
+                tma_load_1d(inbuf, s0.in, tile_copy_bytes<E>(s0.cnt + s0.pad), bar0);
         }
     }
     __syncthreads();
@@ -919,23 +939,24 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             // One buffer: load this tile now (the barrier that ended the previous iteration ordered
             // every read of the buffer before this copy).
             if (tid == 0) {
-                const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
+                const TileSlot sn = next_tile<T, WIN>(a, it, nitems, pend, ah);
                 slots[0] = sn;
                 if (sn.item != ~0u && !(a.test_stall && blockIdx.x == 0 && k == 0))
-                    tma_load_1d(inbuf, sn.in, tile_copy_bytes<E>(sn.cnt), bar0);
+                    tma_load_1d(inbuf, sn.in, tile_copy_bytes<E>(sn.cnt + sn.pad), bar0);
             }
             __syncthreads();
         }
         const TileSlot sl = slots[cur];
         if (sl.item == ~0u) break;
-        E *buf = inbuf + (size_t)cur * T;
+        E *buf = inbuf + (size_t)cur * ST + sl.pad;
         // Stable ranks: prefetch the next tile into the other buffer now; the barrier that ended the
         // previous iteration ordered every access to it before this copy.
         if (NBUF == 2 && !LATE && tid == 0) {
-            const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
+            const TileSlot sn = next_tile<T, WIN>(a, it, nitems, pend, ah);
             slots[cur ^ 1u] = sn;
             if (sn.item != ~0u)
-                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, tile_copy_bytes<E>(sn.cnt), bar0 + 8u * (cur ^ 1u));
+                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * ST, sn.in, tile_copy_bytes<E>(sn.cnt + sn.pad),
+                            bar0 + 8u * (cur ^ 1u));
         }
         // First tile of a work item: load the item's per-digit output offsets.
         if (sl.first && tid < F) {
@@ -972,10 +993,11 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         // barrier above, so the previous tile's staging and write-out, the last accesses to that
         // buffer, are done, and no barrier has to end the iteration.
         if (NBUF == 2 && LATE && tid == 0) {
-            const TileSlot sn = next_tile<T>(a, it, nitems, pend, ah);
+            const TileSlot sn = next_tile<T, WIN>(a, it, nitems, pend, ah);
             slots[cur ^ 1u] = sn;
             if (sn.item != ~0u)
-                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * T, sn.in, tile_copy_bytes<E>(sn.cnt), bar0 + 8u * (cur ^ 1u));
+                tma_load_1d(inbuf + (size_t)(cur ^ 1u) * ST, sn.in, tile_copy_bytes<E>(sn.cnt + sn.pad),
+                            bar0 + 8u * (cur ^ 1u));
         }
 
         // Elements of this tile: warp w owns [w*32*ITEMS, (w+1)*32*ITEMS), one row of 32 per item.
@@ -1012,6 +1034,11 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             const int nbits = a.logF + (cnt < (uint32_t)T ? 1 : 0);
 #pragma unroll
             for (int i = 0; i < ITEMS; i++) {
+                // A row of padding only (a partial tile): nothing to rank (uniform across the warp).
+                if ((uint32_t)(w * 32 * ITEMS + i * 32) >= cnt) {
+                    rk[i] = 0;
+                    continue;
+                }
                 const unsigned peers = digit_peers_n(d[i], nbits);
                 const bool valid = d[i] < (uint32_t)F;
                 uint32_t pre = 0;
@@ -1106,7 +1133,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
 #pragma unroll
                 for (int i = 0; i < ITEMS / 2; i++) {
                     if ((uint64_t)dst[i] < sl.out_len)
-                        store_elem(t[i], sl.out, out8, dst[i], ci, a.bits, b2, z0);
+                        store_elem(t[i], sl.out, out8, dst[i], ci, a.bits, b2, z0, w8o, a.b1);
                     else
                         set_error(err, kErrBounds);
                 }
@@ -1116,7 +1143,7 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
             const E t = buf[j];
             const long long dst = gbase[elem_digit(t, a.shift, dmask)] + (long long)j;
             if ((uint64_t)dst < sl.out_len)
-                store_elem(t, sl.out, out8, dst, ci, a.bits, b2, z0);
+                store_elem(t, sl.out, out8, dst, ci, a.bits, b2, z0, w8o, a.b1);
             else
                 set_error(err, kErrBounds);
         }
@@ -1667,7 +1694,7 @@ struct JoinArgs {
     MatOut mat; // materialising joins (MAT kernels): where the (r.row_id, s.row_id) pairs go
     int ci;     // the final partitions may be compact words (when ci_applies holds) at finR8 / finS8
     const unsigned long long *finR8, *finS8;
-    int w8_b1;  // segment mode with a word pass 1: its shift (reported when w8_fits held); -1 otherwise
+    int w8_b1;  // a pass 1 that may store words (either pipeline): its shift (reported when w8_fits held); -1 otherwise
 };
 
 // A tuple of a final partition: the stored tuple, or for compact partitions {key >> bits, row id}.
@@ -2484,7 +2511,7 @@ int phj_prepare_device() {
     HJ_CU(cudaGetDevice(&cur_dev));
     if (cur_dev < 0 || cur_dev >= 64) return HJ_E_INVAL;
     if (g_attr_done[cur_dev]) return HJ_OK;
-    const size_t scatter_smem = (size_t)kScatterBufs * kTile * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
+    const size_t scatter_smem = (size_t)kScatterBufs * (kTile * 16 + 16) + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
     HJ_CU(cudaFuncSetAttribute(hist_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 136 * 1024));
     HJ_CU(cudaFuncSetAttribute(plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)((size_t)2 * (1u << kPlanStageBits) * 4)));
@@ -2542,7 +2569,8 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     const int np = g.nparts();
     const int F1 = g.F1, F2 = g.F2;
     constexpr int T = kTile;
-    const size_t scatter_smem = (size_t)kScatterBufs * T * 16 + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
+    // tile buffers (word tiles: 16 spare bytes each), gbase, running, tdstart, per-warp digit counts
+    const size_t scatter_smem = (size_t)kScatterBufs * (T * 16 + 16) + 256 * 8 * 2 + 256 * 4 + (kScatterThreads / 32) * 256 * 2;
     const size_t hist_smem = (size_t)np * 4 + (size_t)16 * F1 * 4;  // 16 warps
     ChunkGeom cg;
     cg.chunk = s.chunk;
@@ -2559,6 +2587,13 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     // tuples (test_flags bit 2), when the widths allow them (decided on the device).
     const int ci_ok = (!mat && !(test_flags & 2)) ? 1 : 0;
     const bool seg_words = segm && ci_ok;
+    // The exact-offset pipeline with two passes stores pass 1 as words too (when w8_fits holds, which
+    // the histogram pass's ORs decide before pass 1) when its pass-2 units (chunk, pass-1 digit) average
+    // a full 4096-word tile, or when asked (test_flags bit 4). Pass 2 over 4096-word tiles is slower than
+    // over 2048-tuple tiles when most tiles are partial (2^24 x 2^26: 1.91 against 1.82 ms; 2^27 x 2^29:
+    // 9.01 against 10.68 ms).
+    const bool exact_words =
+        !segm && ci_ok && g.passes == 2 && ((test_flags & 4) || cg.chunk / (uint64_t)F1 >= 2ull * kTile);
     if (segm && (g.passes != 2 || g.bits > kSegMaxBits)) return HJ_E_INVAL;
     {
         const int rc = phj_prepare_device();
@@ -2702,11 +2737,15 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         sa.outR8 = reinterpret_cast<unsigned long long *>(out);
         sa.outS8 = sa.outR8 + nR;
         sa.w8 = 0;
-        // One pass over [item_base, item_end): in segment mode after an 8-byte pass 1, the launch over
-        // 4096-word tiles and the tuple launch after it (which runs only if pass 1 fell back to tuples).
+        sa.w8_out = (exact_words && pass == 0) ? 1 : 0;
+        sa.inR8 = reinterpret_cast<const unsigned long long *>(s.tmp1);
+        sa.inS8 = sa.inR8 + nR;
+        const bool words_in = (segm && seg_words) || (exact_words && pass == 1);
+        // One pass over [item_base, item_end): after a pass 1 that may have stored words, the launch over
+        // 4096-word tiles and the tuple launch after it (which runs only if pass 1 stored tuples).
         auto launch_scatter = [&](bool stable) {
 #define HJ_SCATTER(ST)                                                                                         \
-    if (segm && seg_words) {                                                                                   \
+    if (words_in) {                                                                                            \
         sa.w8 = 1;                                                                                             \
         scatter_kernel<kScatterThreads, 2 * kScatterItems, ST, kScatterBufs, kScatterWordCtasPerSm, true>        \
             <<<num_sms * kScatterWordCtasPerSm, kScatterThreads, scatter_smem, st>>>(sa);                      \
@@ -2766,7 +2805,7 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
     ja.ci = ci_ok;
     ja.finR8 = reinterpret_cast<const unsigned long long *>(s.tmp2);
     ja.finS8 = ja.finR8 + nR;
-    ja.w8_b1 = seg_words ? g.b1 : -1;
+    ja.w8_b1 = (seg_words || exact_words) ? g.b1 : -1;
     if (mat) {
         if (lp)
             join_compact_kernel<true, false, true><<<num_sms * 2, kCompactThreads, kCompactSmem, st>>>(ja);

@@ -107,9 +107,12 @@ typedef struct {
 #define HJ_F_SEGMENTS    0x20u /* segment mode whenever the algorithm allows it */
 #define HJ_F_EXACT       0x40u /* always the histogram pass and exact pass-1 offsets */
 /* Radix joins store a tuple as one 8-byte word in the partitions when the widths allow (see
- * HJ_RES_COMPACT_PARTITIONS): the final partitions, and in segment mode the pass-1 chains too. This flag
- * keeps 16-byte tuples in every pass instead; results are the same. */
+ * HJ_RES_COMPACT_PARTITIONS): the final partitions, and the pass-1 output of segment mode, and of the
+ * exact-offset pipeline when its pass-2 units average a full 4096-word tile (smaller units run faster on
+ * tuples). HJ_F_WIDE keeps 16-byte tuples in every pass instead; HJ_F_WORDS stores words in every pass
+ * whenever the widths allow, whatever the unit sizes. Results are the same. */
 #define HJ_F_WIDE        0x80u
+#define HJ_F_WORDS       0x200u
 /* Test hook for failure detection: the first partition pass of a radix join withholds one tile load,
  * so a bounded device wait (2 s) expires and the join returns HJ_E_TIMEOUT; the context stays usable. */
 #define HJ_F_TEST_STALL  0x100u

@@ -157,3 +157,32 @@ def test_segment_mode_word_pass1_and_its_fallback(hj, oracle, cuda):
         hj.join("phj_radix_bc", dev(cuda, R), dev(cuda, S), on_device=True, flags=hj.HJ_F_SEGMENTS | hj.HJ_F_TEST_STALL)
     assert e.value.status == hj.HJ_E_TIMEOUT
     assert run(hj, oracle, cuda, "phj_radix_bc", R, S, hj.HJ_F_SEGMENTS)  # the context recovers
+
+
+@pytest.mark.parametrize("algo", ["phj_radix_bc", "phj_radix_lp"])
+def test_exact_pipeline_word_pass1(hj, oracle, cuda, algo):
+    """The exact-offset pipeline stores pass 1 as 8-byte words too when the histogram pass's ORs allow
+    them (by default only for large units; HJ_F_WORDS asks for it here); pass 2 then reads its units at
+    word offsets, odd ones included (a tile's copy starts one word early). Build keys too wide for pass-1 words keep tuples in pass 1 (the final partitions can still be
+    compact); HJ_F_WIDE keeps tuples everywhere. Results equal the oracle's, with duplicates and key 0."""
+    R, S = rels(9)
+    R[::37, 0] = 0
+    R[1::5, 0] = R[::5, 0][: R[1::5].shape[0]]
+    R2 = R.copy()
+    S2 = S.copy()
+    R2[:, 0] |= np.uint64(1 << 40)  # key >> 7 does not fit 31 bits, key >> 14 does
+    S2[:, 0] |= np.uint64(1 << 40)
+    for RR, SS, words in ((R, S, True), (R2, S2, False)):
+        want = oracle.join(algo, RR, SS)
+        for bits, b1 in ((14, 7), (12, 5), (9, 4)):
+            r = hj.join(algo, dev(cuda, RR), dev(cuda, SS), on_device=True, bits=bits, passes=2,
+                        bits_pass1=b1, flags=hj.HJ_F_EXACT | hj.HJ_F_WORDS)
+            assert (r.matched_cnt, r.checksum) == want, (algo, bits, b1, words)
+            assert bool(r.flags & hj.HJ_RES_WORD_PASS1) == words, (bits, b1)
+        r = hj.join(algo, dev(cuda, RR), dev(cuda, SS), on_device=True, flags=hj.HJ_F_EXACT | hj.HJ_F_WIDE)
+        assert (r.matched_cnt, r.checksum) == want
+        assert not r.flags & hj.HJ_RES_WORD_PASS1
+        # by default these small units keep tuples in pass 1
+        r = hj.join(algo, dev(cuda, RR), dev(cuda, SS), on_device=True, flags=hj.HJ_F_EXACT)
+        assert (r.matched_cnt, r.checksum) == want
+        assert not r.flags & hj.HJ_RES_WORD_PASS1
