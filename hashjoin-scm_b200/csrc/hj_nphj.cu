@@ -51,7 +51,7 @@ struct NphjSide {
     unsigned long long kmax;     // largest build key (compact-slot test)
     unsigned long long ror;      // OR of all build row ids
     unsigned int sliced;         // the compact table is built (and probed) slice by slice
-    unsigned int colscan_done;   // blocks of nphj_slice_colscan that have written their totals
+    unsigned int overflow;       // a slice's staged tuples exceeded kSliceMaxFill (no sliced build)
 };
 
 constexpr unsigned long long kCompactEmpty = ~0ull;
@@ -84,14 +84,12 @@ struct NphjArgs {
     // Compact tables: capacity (a multiple of kSliceSlots) and the sliced build's buffers.
     unsigned long long ccap;
     unsigned int nslices;      // ccap / kSliceSlots; 0: no sliced build
-    unsigned int hist_blocks;  // blocks of the counting and scatter passes (each a contiguous range of R)
-    unsigned long long *stage; // [nR] build tuples as compact words, ordered by slice
-    uint32_t *slice_hist;      // [hist_blocks][nslices] build tuples per (block, slice)
-    uint32_t *slice_off;       // [hist_blocks][nslices] the block's offset inside the slice
-    uint32_t *slice_start;     // [nslices + 1] first staging index of each slice
-    // Sliced builds: the kernels of the other table forms (clear, build, 16-byte probe) run inside the
-    // sliced build's own launches (scatter, slice build, compact probe) when the device finds that the
-    // table is not built by slices, instead of as launches of their own that return at once.
+    unsigned int hist_blocks;  // blocks of the width and scatter passes (each a contiguous range of R)
+    unsigned long long *stage; // [nslices][kSliceMaxFill] build tuples as compact words, by slice
+    uint32_t *slice_fill;      // [nslices] tuples staged per slice (claimed by the scatter blocks)
+    // Sliced builds: the clear and the 16-byte probe of the other table forms run inside the slice build
+    // and the compact probe when the device finds that the table is not built by slices, instead of as
+    // launches of their own that return at once.
     int fused_fallback;
 };
 
@@ -122,15 +120,9 @@ __device__ __forceinline__ void block_range(unsigned long long n, unsigned long 
     *hi = *lo + per < n ? *lo + per : n;
 }
 
-// Largest build key and OR of build row ids (the compact-slot test) and, when the table may be built
-// by slices, the build tuples of every slice in this block's contiguous range of R.
+// Largest build key and OR of build row ids: the compact-slot test of a join whose compact table is
+// not built by slices (the sliced build takes them in nphj_slice_scatter).
 __global__ void __launch_bounds__(kSliceThreads) nphj_widths(NphjArgs a) {
-    extern __shared__ uint32_t sh_cnt[];  // [nslices]
-    const bool count = a.nslices != 0;
-    if (count) {
-        for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) sh_cnt[j] = 0;
-        __syncthreads();
-    }
     unsigned long long lo, hi;
     block_range(a.nR, &lo, &hi);
     unsigned long long kmax = 0, ror = 0;
@@ -146,8 +138,6 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_widths(NphjArgs a) {
         for (int u = 0; u < U; u++) {
             kmax = max(kmax, t[u].x);
             ror |= t[u].y;
-            if (count && i0 + u * blockDim.x < hi && t[u].x < 0xffffffffull)
-                atomicAdd(&sh_cnt[slice_of(t[u].x, a.ccap)], 1u);
         }
     }
 #pragma unroll
@@ -159,132 +149,37 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_widths(NphjArgs a) {
         atomicMax(&a.side->kmax, kmax);
         atomicOr(&a.side->ror, ror);
     }
-    if (count) {
-        __syncthreads();
-        uint32_t *row = a.slice_hist + (size_t)blockIdx.x * a.nslices;
-        for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) row[j] = sh_cnt[j];
-    }
-}
-
-// One CTA (the last block of the column scan): the first staging index of every slice, and the mode of
-// the build: sliced when the table is compact and no slice is filled above kSliceMaxFill.
-__device__ __forceinline__ void slice_plan_body(const NphjArgs &a, const uint32_t *total) {
-    __shared__ uint32_t scan_tmp[32];
-    __shared__ uint32_t s_max;
-    const unsigned n = a.nslices;
-    const unsigned per = (n + blockDim.x - 1) / blockDim.x;
-    const unsigned j0 = min(n, threadIdx.x * per), j1 = min(n, j0 + per);
-    uint32_t sum = 0, mx = 0;
-    for (unsigned j = j0; j < j1; j++) {
-        const uint32_t t = __ldcg(total + j);  // written by other blocks of the column scan
-        sum += t;
-        mx = max(mx, t);
-    }
-    if (threadIdx.x == 0) s_max = 0;
-    __syncthreads();
-    atomicMax(&s_max, mx);
-    // Block-wide exclusive scan of the per-thread sums.
-    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (unsigned)o) incl += v;
-    }
-    if (lane == 31) scan_tmp[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t v = lane < blockDim.x / 32 ? scan_tmp[lane] : 0;
-        uint32_t x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= (unsigned)o) x += y;
-        }
-        scan_tmp[lane] = x - v;
-    }
-    __syncthreads();
-    uint32_t run = scan_tmp[w] + incl - sum;
-    for (unsigned j = j0; j < j1; j++) {
-        a.slice_start[j] = run;
-        run += __ldcg(total + j);
-    }
-    if (threadIdx.x == blockDim.x - 1) a.slice_start[n] = run;
-    if (threadIdx.x == 0) {
-        const bool compact = nphj_compact(a.side);
-        a.side->sliced = (compact && s_max <= kSliceMaxFill) ? 1u : 0u;
-    }
-}
-
-// Per slice, the offset of every block's tuples inside the slice (an exclusive scan down the column
-// of the histogram) and the slice's total. 32 slices per CTA; warp w sums a contiguous run of rows. The
-// last CTA to finish then plans the slices (slice_plan_body).
-__global__ void __launch_bounds__(1024) nphj_slice_colscan(NphjArgs a, uint32_t *total) {
-    __shared__ uint32_t part[32][33];
-    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned sidx = blockIdx.x * 32 + lane;
-    const bool valid = sidx < a.nslices;
-    const unsigned rpw = (a.hist_blocks + 31) / 32;
-    const unsigned r0 = w * rpw, r1 = min(a.hist_blocks, r0 + rpw);
-    uint32_t sum = 0;
-    for (unsigned r = r0; r < r1 && valid; r++) sum += a.slice_hist[(size_t)r * a.nslices + sidx];
-    part[w][lane] = sum;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t run = 0;
-        for (int q = 0; q < 32; q++) {
-            const uint32_t v = part[q][lane];
-            part[q][lane] = run;
-            run += v;
-        }
-        if (valid) total[sidx] = run;
-    }
-    __syncthreads();
-    uint32_t run = part[w][lane];
-    for (unsigned r = r0; r < r1 && valid; r++) {
-        const size_t q = (size_t)r * a.nslices + sidx;
-        const uint32_t v = a.slice_hist[q];
-        a.slice_off[q] = run;
-        run += v;
-    }
-    __shared__ bool s_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(&a.side->colscan_done, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    slice_plan_body(a, total);
 }
 
 // Empties the table the build will claim slots in: the 16-byte table when the keys or row ids are too
 // wide for compact slots, the compact table when it is built by global CAS. A table built by slices
 // is written whole by nphj_slice_build.
-__device__ __forceinline__ void clear_table_body(const NphjArgs &a) {
-    const bool compact = use_compact(a);
-    if (compact && compact_sliced(a.side)) return;
+__device__ __forceinline__ void clear_table_body(const NphjArgs &a, bool sliced) {
+    const bool compact = a.compact_ok && nphj_compact(a.side) && (!a.lp || sliced);  // use_compact
+    if (compact && sliced) return;
     const unsigned long long words16 = compact ? a.ccap / 2 : a.cap;  // 16-byte units
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < words16;
          i += (unsigned long long)gridDim.x * blockDim.x)
         a.table[i] = make_ulonglong2(kEmpty, kEmpty);
 }
 
-__global__ void nphj_clear_table(NphjArgs a) { clear_table_body(a); }
+__global__ void nphj_clear_table(NphjArgs a) { clear_table_body(a, compact_sliced(a.side)); }
 
-// Build tuples in slice order as compact words (key << 32 | row id); block b writes its tuples of
-// slice s from start[s] + off[b][s] on, ranked by shared-memory counters.
+// The sliced build's one pass over R: block b takes a contiguous range of R, takes the width ORs of the
+// compact test and counts the range's tuples per slice in shared memory, claims each slice's space in
+// the staging array with one global atomic per slice (in any order across blocks: no join semantics here
+// depends on the order of tuples inside a slice), then reads its range again (from L2: it has just been
+// read) and writes each tuple as a compact word (key << 32 | row id; first-match joins: key << 32 | input
+// position) at its slice's claim plus its shared-memory rank. Claims past kSliceMaxFill mark the build
+// not sliced; their tuples are not staged.
 __global__ void __launch_bounds__(kSliceThreads) nphj_slice_scatter(NphjArgs a) {
-    extern __shared__ uint32_t sh_pos[];  // [nslices]
-    if (!compact_sliced(a.side)) {
-        if (a.fused_fallback) clear_table_body(a);
-        return;
-    }
-    const uint32_t *off = a.slice_off + (size_t)blockIdx.x * a.nslices;
-    for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) sh_pos[j] = a.slice_start[j] + off[j];
+    extern __shared__ uint32_t sh_cnt[];  // [nslices]: counts, then the next staging index of each slice
+    for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) sh_cnt[j] = 0;
     __syncthreads();
     unsigned long long lo, hi;
     block_range(a.nR, &lo, &hi);
     constexpr int U = 4;
+    unsigned long long kmax = 0, ror = 0;
     for (unsigned long long i0 = lo + threadIdx.x; i0 < hi; i0 += U * blockDim.x) {
         tuple_v t[U];
 #pragma unroll
@@ -294,29 +189,59 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_slice_scatter(NphjArgs a) 
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            if (i0 + u * blockDim.x >= hi) continue;
-            const uint32_t pos = atomicAdd(&sh_pos[slice_of(t[u].x, a.ccap)], 1u);
-            // Every match: key and row id. First match: key and input position (the slice build keeps
-            // the smallest position per key, then looks its row id up).
-            if (pos < a.nR)
-                a.stage[pos] = (t[u].x << 32) | (a.lp ? i0 + u * blockDim.x : t[u].y);
-            else
-                set_error(&a.acc->error, kErrBounds);
+            kmax = max(kmax, t[u].x);
+            ror |= t[u].y;
+            if (i0 + u * blockDim.x < hi && t[u].x < 0xffffffffull) atomicAdd(&sh_cnt[slice_of(t[u].x, a.ccap)], 1u);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+        ror |= __shfl_xor_sync(0xffffffffu, ror, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&a.side->kmax, kmax);
+        atomicOr(&a.side->ror, ror);
+    }
+    __syncthreads();
+    for (unsigned j = threadIdx.x; j < a.nslices; j += blockDim.x) {
+        const uint32_t c = sh_cnt[j];
+        if (!c) continue;
+        const uint32_t b = atomicAdd(&a.slice_fill[j], c);
+        if (b + c > kSliceMaxFill) atomicOr(&a.side->overflow, 1u);
+        sh_cnt[j] = b;
+    }
+    __syncthreads();
+    for (unsigned long long i0 = lo + threadIdx.x; i0 < hi; i0 += U * blockDim.x) {
+        tuple_v t[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned long long i = i0 + u * blockDim.x;
+            t[u] = i < hi ? a.R[i] : make_ulonglong2(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned long long i = i0 + u * blockDim.x;
+            if (i >= hi || t[u].x >= 0xffffffffull) continue;
+            const unsigned sl = slice_of(t[u].x, a.ccap);
+            const uint32_t p = atomicAdd(&sh_cnt[sl], 1u);
+            if (p < kSliceMaxFill) a.stage[(size_t)sl * kSliceMaxFill + p] = (t[u].x << 32) | (a.lp ? i : t[u].y);
         }
     }
 }
 
-// One slice at a time per CTA: its build tuples claim slots of a shared-memory table by CAS, probing
-// inside the slice; then the whole slice, empty slots included, is written to the global table.
-// First-match joins: a tuple whose key already has a slot lowers the slot's position (64-bit min on
-// key << 32 | position), and before the write-out each slot's position is replaced by the row id of
-// that build tuple.
 __device__ void build_body(const NphjArgs &a);
 
 __global__ void __launch_bounds__(kSliceThreads) nphj_slice_build(NphjArgs a) {
     extern __shared__ unsigned long long tab[];  // [kSliceSlots]
-    if (!compact_sliced(a.side)) {
-        if (a.fused_fallback) build_body(a);
+    // The mode of the build, now that the scatter has taken the widths and the slice fills: sliced when
+    // the table is compact and no slice overflowed. Every block decides the same; block 0 records it for
+    // the kernels after this one. Otherwise the table of the other form is cleared here for the build
+    // that follows (nphj_build).
+    const bool sliced = nphj_compact(a.side) && *reinterpret_cast<volatile unsigned int *>(&a.side->overflow) == 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.side->sliced = sliced ? 1u : 0u;
+    if (!sliced) {
+        clear_table_body(a, false);
         return;
     }
     bool seen_dup = false;
@@ -324,7 +249,7 @@ __global__ void __launch_bounds__(kSliceThreads) nphj_slice_build(NphjArgs a) {
     for (unsigned sl = blockIdx.x; sl < a.nslices; sl += gridDim.x) {
         for (unsigned j = threadIdx.x; j < kSliceSlots; j += blockDim.x) tab[j] = kCompactEmpty;
         __syncthreads();
-        const uint32_t lo = a.slice_start[sl], n = a.slice_start[sl + 1] - lo;
+        const uint32_t lo = sl * kSliceMaxFill, n = a.slice_fill[sl];
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
             const unsigned long long v = a.stage[lo + i];
             const unsigned long long k = v >> 32;
@@ -735,7 +660,6 @@ int nphj_prepare_device() {
     if (dev < 0 || dev >= 64) return HJ_E_INVAL;
     std::lock_guard<std::mutex> lk(g_nphj_attr_mu);
     if (g_nphj_attr_done[dev]) return HJ_OK;
-    HJ_CU(cudaFuncSetAttribute(nphj_widths, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kSliceMaxCount * 4)));
     HJ_CU(cudaFuncSetAttribute(nphj_slice_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(kSliceMaxCount * 4)));
     HJ_CU(cudaFuncSetAttribute(nphj_slice_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kSliceSlots * 8)));
@@ -773,22 +697,16 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     a.fused_fallback = 0;
     a.hist_blocks = (unsigned)num_sms * 2;
     a.stage = nullptr;
-    a.slice_hist = a.slice_off = a.slice_start = nullptr;
-    uint32_t *slice_total = nullptr;
+    a.slice_fill = nullptr;
     if (a.compact_ok) {
         const unsigned long long ns = a.ccap / kSliceSlots;
         char *p = reinterpret_cast<char *>(table) + ((a.ccap * 8 + 255) & ~255ull);
         char *const end = reinterpret_cast<char *>(table) + cap * 16;
-        char *q = p + ((nR * 8 + 255) & ~255ull);
-        const size_t hist_bytes = ((size_t)a.hist_blocks * ns * 4 + 255) & ~(size_t)255;
-        char *q_end = q + 2 * hist_bytes + 2 * (((ns + 1) * 4 + 255) & ~(size_t)255);
-        if (ns <= kSliceMaxCount && q_end <= end) {
+        char *q = p + ((ns * kSliceMaxFill * 8 + 255) & ~255ull);
+        if (ns <= kSliceMaxCount && q + ns * 4 <= end) {
             a.nslices = (unsigned)ns;
             a.stage = reinterpret_cast<unsigned long long *>(p);
-            a.slice_hist = reinterpret_cast<uint32_t *>(q);
-            a.slice_off = reinterpret_cast<uint32_t *>(q + hist_bytes);
-            a.slice_start = reinterpret_cast<uint32_t *>(q + 2 * hist_bytes);
-            slice_total = reinterpret_cast<uint32_t *>(q + 2 * hist_bytes + (((ns + 1) * 4 + 255) & ~(size_t)255));
+            a.slice_fill = reinterpret_cast<uint32_t *>(q);
             a.fused_fallback = 1;
         }
     }
@@ -809,24 +727,24 @@ int nphj_enqueue(bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulon
     // Phase slots: build spans [0, 1], probe spans [4, 5]; the others stay empty.
     if (ph) HJ_CU(record_event(ph[0], st));
     if (a.compact_ok) {
-        const size_t hist_smem = (size_t)a.nslices * 4;
-        nphj_widths<<<a.hist_blocks, kSliceThreads, hist_smem, st>>>(a);
-        nl++;
         if (a.nslices) {
-            nphj_slice_colscan<<<(a.nslices + 31) / 32, 1024, 0, st>>>(a, slice_total);
-            nphj_slice_scatter<<<a.hist_blocks, kSliceThreads, hist_smem, st>>>(a);
+            // One pass over R (widths, per-slice claims, staging), the slice build (or, when the table
+            // is not built by slices, the clear of the table the fallback build needs).
+            HJ_CU(cudaMemsetAsync(a.slice_fill, 0, (size_t)a.nslices * 4, st));
+            nphj_slice_scatter<<<a.hist_blocks, kSliceThreads, (size_t)a.nslices * 4, st>>>(a);
             const unsigned bgrid = a.nslices < (unsigned)num_sms * 3 ? a.nslices : (unsigned)num_sms * 3;
             nphj_slice_build<<<bgrid, kSliceThreads, kSliceSlots * 8, st>>>(a);
-            nl += 3;
+            nl += 2;
         } else {
+            nphj_widths<<<a.hist_blocks, kSliceThreads, 0, st>>>(a);
             nphj_clear_table<<<num_sms * 2, 256, 0, st>>>(a);
-            nl++;
+            nl += 2;
         }
     }
-    if (!a.fused_fallback) {
-        nphj_build<<<fb_grid, 256, 0, st>>>(a);
-        nl++;
-    }
+    // The build of the other table forms (a compact table by global CAS, or the 16-byte table); it
+    // returns at once when the table was built by slices.
+    nphj_build<<<fb_grid, 256, 0, st>>>(a);
+    nl++;
     if (lp) {
         nphj_lp_refill<<<fb_grid, 256, 0, st>>>(a);
         nphj_lp_dedup_build<<<fb_grid, 256, 0, st>>>(a);

@@ -1,9 +1,11 @@
 """CPU restatement of the index arithmetic of the non-partitioned join's sliced build (hj_nphj.cu:
-nphj_widths, nphj_slice_colscan, nphj_slice_plan, nphj_slice_scatter, nphj_slice_build and the probe's
-slice wrap), run before the kernels ever touch a GPU: every staging write lands inside [0, |R|) exactly
-once, each slice holds only its own keys, no slice overflows its slots, and probing inside slices gives
-the oracle's result, for every-match joins (staged key and row id) and first-match joins (staged key and
-input position, smallest position kept per key, then its row id)."""
+nphj_slice_scatter, nphj_slice_build and the probe's slice wrap), run before the kernels ever touch a
+GPU: each block counts its contiguous range of R per slice, claims space in every slice's staging area
+(kSliceMaxFill words) in whatever order the blocks reach the atomic, and writes at its claim plus a rank;
+every staging write lands inside its slice's area exactly once, each slice holds only its own keys, and
+probing inside slices gives the oracle's result whatever the claim order, for every-match joins (staged
+key and row id) and first-match joins (staged key and input position, smallest position kept per key,
+then its row id)."""
 import numpy as np
 import pytest
 
@@ -21,7 +23,18 @@ def table_hash(key, cap):
     return (h * cap) >> 64
 
 
-def sliced_join(R, S, hist_blocks, lp=False):
+def staging_fits(nR):
+    """The host's test (nphj_enqueue): the compact table, the staging areas and the fill counters fit in the
+    16-byte table's bytes. True for every table the sliced build is used for (above 64 MB the rounding of
+    the capacity to whole slices is below 0.2%); small or badly rounded tables build without slices."""
+    a256 = lambda x: (x + 255) // 256 * 256
+    cap = int(nR / 0.5) + 2
+    ccap = (cap + SLICE - 1) // SLICE * SLICE
+    ns = ccap // SLICE
+    return a256(ccap * 8) + a256(ns * MAX_FILL * 8) + ns * 4 <= cap * 16
+
+
+def sliced_join(R, S, hist_blocks, lp=False, claim_seed=0):
     nR = R.shape[0]
     cap = int(nR / 0.5) + 2
     ccap = (cap + SLICE - 1) // SLICE * SLICE
@@ -30,33 +43,37 @@ def sliced_join(R, S, hist_blocks, lp=False):
     rids = [int(r) for r in R[:, 1]]
     sl = [table_hash(k, ccap) >> SLICE_LOG for k in keys]
     assert all(0 <= x < ns for x in sl)
-    # nphj_widths: block b counts its contiguous range [b*per, min(nR, (b+1)*per))
+    assert staging_fits(nR)  # otherwise the host builds without slices
+    # pass 1 of nphj_slice_scatter: block b counts its contiguous range [b*per, min(nR, (b+1)*per))
     per = (nR + hist_blocks - 1) // hist_blocks
     hist = np.zeros((hist_blocks, ns), dtype=np.int64)
     for b in range(hist_blocks):
         lo, hi = min(nR, b * per), min(nR, b * per + per)
         for i in range(lo, hi):
             hist[b, sl[i]] += 1
-    # nphj_slice_colscan: exclusive scan down each column; nphj_slice_plan: slice starts
-    off = np.cumsum(hist, axis=0) - hist
-    total = hist.sum(axis=0)
-    start = np.concatenate([[0], np.cumsum(total)])
-    assert start[-1] == nR and total.max() <= MAX_FILL
-    # nphj_slice_scatter: block b writes its tuples of slice s from start[s] + off[b][s] on
-    stage = [None] * nR
+    # claims: one atomic per (block, slice), blocks in an arbitrary order
+    fill = np.zeros(ns, dtype=np.int64)
+    base = np.zeros((hist_blocks, ns), dtype=np.int64)
+    for b in np.random.default_rng(claim_seed).permutation(hist_blocks):
+        base[b] = fill
+        fill += hist[b]
+    assert fill.sum() == nR and fill.max() <= MAX_FILL  # no overflow: the build is sliced
+    # pass 2: block b writes its tuples of slice s at s * MAX_FILL + its claim + a rank
+    stage = [None] * (ns * MAX_FILL)
     for b in range(hist_blocks):
-        pos = start[:-1] + off[b]
+        pos = base[b].copy()
         lo, hi = min(nR, b * per), min(nR, b * per + per)
         for i in range(lo, hi):
-            p = int(pos[sl[i]])
-            pos[sl[i]] += 1
-            assert 0 <= p < nR and stage[p] is None
-            stage[p] = (keys[i] << 32) | (i if lp else rids[i])
-    assert all(v is not None for v in stage)
+            s = sl[i]
+            p = int(pos[s])
+            pos[s] += 1
+            assert 0 <= p < MAX_FILL and stage[s * MAX_FILL + p] is None
+            stage[s * MAX_FILL + p] = (keys[i] << 32) | (i if lp else rids[i])
+    assert sum(v is not None for v in stage) == nR
     # nphj_slice_build: per slice, linear probing inside the slice
     table = [None] * ccap
     for s in range(ns):
-        for v in stage[start[s]:start[s + 1]]:
+        for v in stage[s * MAX_FILL:s * MAX_FILL + int(fill[s])]:
             k = v >> 32
             assert table_hash(k, ccap) >> SLICE_LOG == s
             h = table_hash(k, ccap) & (SLICE - 1)
@@ -94,8 +111,8 @@ def sliced_join(R, S, hist_blocks, lp=False):
 
 
 @pytest.mark.parametrize("lp", [False, True])
-@pytest.mark.parametrize("nR,nS,hist_blocks,dups", [(20_000, 50_000, 7, False), (30_001, 40_000, 296, True),
-                                                    (8_192, 20_000, 1, True)])
+@pytest.mark.parametrize("nR,nS,hist_blocks,dups", [(20_478, 50_000, 7, False), (28_670, 40_000, 296, True),
+                                                    (8_190, 20_000, 1, True)])
 def test_sliced_build_index_arithmetic(oracle, nR, nS, hist_blocks, dups, lp):
     rng = np.random.default_rng(nR)
     R = np.empty((nR, 2), dtype=np.uint64)
@@ -105,4 +122,13 @@ def test_sliced_build_index_arithmetic(oracle, nR, nS, hist_blocks, dups, lp):
     S[:, 0] = R[rng.integers(0, nR, nS), 0]
     S[::9, 0] = rng.integers(1, 1 << 33, S[::9].shape[0], dtype=np.uint64)
     S[:, 1] = rng.integers(0, 1 << 40, nS, dtype=np.uint64)
-    assert sliced_join(R, S, hist_blocks, lp) == oracle.join("nphj_lp" if lp else "nphj_sc", R, S)
+    want = oracle.join("nphj_lp" if lp else "nphj_sc", R, S)
+    for seed in (0, 1):  # two claim orders
+        assert sliced_join(R, S, hist_blocks, lp, seed) == want
+
+
+def test_staging_fits_every_table_the_sliced_build_is_used_for():
+    # compact tables are used above 64 MB of 16-byte slots (nR > 2^21)
+    for nR in (1 << 21, (1 << 21) + 1, 3_000_001, 1 << 22, 10**7 + 7, 1 << 26):
+        assert staging_fits(nR), nR
+    assert not staging_fits(30_001)  # a small, badly rounded table: the host builds without slices
