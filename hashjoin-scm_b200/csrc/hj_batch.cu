@@ -14,9 +14,10 @@
 //      and runs each wave as one set of multi-join kernels over a flattened index space (build over all
 //      build tuples of the wave, then probe over all probe tuples), so the tables are still in L2 when
 //      probed;
-//   3. enqueues the partitioned joins one after another on a second stream forked from the first
-//      (sharing one scratch area), so they overlap the waves;
-//   4. captures the whole sequence in a CUDA graph once (two parallel branches), so a run is one graph
+//   3. enqueues the partitioned joins on kPhjLanes streams forked from the first (each with its own
+//      scratch area; largest joins first, each on the least loaded stream), so they overlap the waves
+//      and each other;
+//   4. captures the whole sequence in a CUDA graph once (parallel branches), so a run is one graph
 //      launch.
 #include <algorithm>
 #include <chrono>
@@ -300,6 +301,11 @@ unsigned long long nphj_slots(size_t nR) { return hj::mj_slots(nR); }
 
 }  // namespace
 
+// Partitioned joins of a batch run on this many parallel branches (streams forked from the batch's
+// stream, each with its own scratch), so that small pipelines overlap instead of running one after
+// another; the largest joins are placed first, each on the branch with the fewest tuples so far.
+constexpr int kPhjLanes = 4;
+
 struct hj_batch {
     hj_ctx *ctx = nullptr;
     int njobs = 0;
@@ -311,10 +317,11 @@ struct hj_batch {
     size_t mem_bytes = 0;
     JoinAccum *accs = nullptr;      // device, one per job
     JoinAccum *accs_host = nullptr; // pinned
-    char *phj_scratch = nullptr;
+    char *phj_scratch = nullptr;                  // kPhjLanes areas of phj_lane_bytes
+    size_t phj_lane_bytes = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t stream_phj = nullptr;            // partitioned joins, forked from `stream`
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t stream_phj[kPhjLanes] = {};      // partitioned joins, forked from `stream`
+    cudaEvent_t ev_fork = nullptr, ev_join[kPhjLanes] = {};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -378,14 +385,15 @@ int enqueue_batch(hj_batch *b) {
     cudaStream_t st = b->stream;
     BCU(cudaMemsetAsync(b->accs, 0, sizeof(JoinAccum) * b->njobs, st));
     uint32_t launches = 0;
-    // The partitioned joins run on a second stream forked here and joined at the end: they share
-    // nothing with the waves of non-partitioned joins, and their kernels fill the SMs that a wave's
-    // small kernels leave idle (in the captured graph these become two parallel branches).
+    // The partitioned joins run on streams forked here and joined at the end: they share nothing with
+    // the waves of non-partitioned joins or with each other, and their kernels fill the SMs that a
+    // wave's small kernels, or a small pipeline's, leave idle (in the captured graph these become
+    // parallel branches).
     const bool fork = !b->phj_jobs.empty();
-    cudaStream_t sp = fork ? b->stream_phj : st;
+    const int lanes = fork ? (int)std::min<size_t>(kPhjLanes, b->phj_jobs.size()) : 0;
     if (fork) {
         BCU(cudaEventRecord(b->ev_fork, st));
-        BCU(cudaStreamWaitEvent(sp, b->ev_fork, 0));
+        for (int l = 0; l < lanes; l++) BCU(cudaStreamWaitEvent(b->stream_phj[l], b->ev_fork, 0));
     }
     for (const Wave &w : b->waves) {
         if (w.total_r == 0 && w.total_s == 0) continue;
@@ -406,23 +414,32 @@ int enqueue_batch(hj_batch *b) {
         const int rc = hj::mj_launch_wave(wd, sms, st, &launches);
         if (rc) return rc;
     }
-    for (int j : b->phj_jobs) {
+    std::vector<int> order(b->phj_jobs);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return b->jobs[x].nR + b->jobs[x].nS > b->jobs[y].nR + b->jobs[y].nS;
+    });
+    unsigned long long load[kPhjLanes] = {};
+    for (int j : order) {
         const hj_batch_job_t &J = b->jobs[j];
         if (J.nR == 0 || J.nS == 0) continue;
+        int l = 0;
+        for (int q = 1; q < lanes; q++)
+            if (load[q] < load[l]) l = q;
+        load[l] += J.nR + J.nS;
         hj::RadixGeom g;
         if (hj::radix_geom(b->bits[j], b->passes[j], &g)) return HJ_E_INVAL;
         hj::PhjScratch s;
-        hj::phj_carve(g, J.nR, J.nS, sms, b->phj_scratch, &s);
-        uint32_t l = 0;
+        hj::phj_carve(g, J.nR, J.nS, sms, b->phj_scratch + (size_t)l * b->phj_lane_bytes, &s);
+        uint32_t nl = 0;
         int rc = hj::phj_enqueue(g, sem_lp(J.algo), sem_skip0(J.algo), reinterpret_cast<const ulonglong2 *>(J.R), J.nR,
-                                 reinterpret_cast<const ulonglong2 *>(J.S), J.nS, s, b->accs + j, sp, nullptr, sms,
-                                 nullptr, &l);
+                                 reinterpret_cast<const ulonglong2 *>(J.S), J.nS, s, b->accs + j, b->stream_phj[l],
+                                 nullptr, sms, nullptr, &nl);
         if (rc) return rc;
-        launches += l;
+        launches += nl;
     }
-    if (fork) {
-        BCU(cudaEventRecord(b->ev_join, sp));
-        BCU(cudaStreamWaitEvent(st, b->ev_join, 0));
+    for (int l = 0; l < lanes; l++) {
+        BCU(cudaEventRecord(b->ev_join[l], b->stream_phj[l]));
+        BCU(cudaStreamWaitEvent(st, b->ev_join[l], 0));
     }
     b->launches = launches;
     return HJ_OK;
@@ -578,7 +595,9 @@ static int plan_one(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj
     }
     const size_t acc_bytes = a256(sizeof(JoinAccum) * (njobs ? njobs : 1));
     // All waves share one table area (they run one after another); descriptors are per wave.
-    b->mem_bytes = acc_bytes + max_wave_tables + desc_bytes + a256(phj_bytes);
+    b->phj_lane_bytes = a256(phj_bytes);
+    const size_t phj_lanes = std::min<size_t>(kPhjLanes, b->phj_jobs.size() ? b->phj_jobs.size() : 1);
+    b->mem_bytes = acc_bytes + max_wave_tables + desc_bytes + phj_lanes * b->phj_lane_bytes;
     int dev_prev = -1;
     cudaGetDevice(&dev_prev);
     cudaSetDevice(c->device);
@@ -594,10 +613,12 @@ static int plan_one(hj_ctx_t *c, const hj_batch_job_t *jobs, int njobs, const hj
     }
     if (cudaMallocHost(&b->accs_host, sizeof(JoinAccum) * (njobs ? njobs : 1)) != cudaSuccess) return fail(HJ_E_OOM);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->stream_phj, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess)
         return fail(HJ_E_DEVICE);
+    for (int l = 0; l < kPhjLanes; l++)
+        if (cudaStreamCreateWithFlags(&b->stream_phj[l], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->ev_join[l], cudaEventDisableTiming) != cudaSuccess)
+            return fail(HJ_E_DEVICE);
     if (cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) return fail(HJ_E_DEVICE);
     char *cur = b->mem;
     b->accs = reinterpret_cast<JoinAccum *>(cur);
@@ -740,9 +761,11 @@ int hj_batch_destroy(hj_batch_t *b) {
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     if (b->stream) cudaStreamDestroy(b->stream);
-    if (b->stream_phj) cudaStreamDestroy(b->stream_phj);
+    for (int l = 0; l < kPhjLanes; l++) {
+        if (b->stream_phj[l]) cudaStreamDestroy(b->stream_phj[l]);
+        if (b->ev_join[l]) cudaEventDestroy(b->ev_join[l]);
+    }
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
-    if (b->ev_join) cudaEventDestroy(b->ev_join);
     delete b;
     return HJ_OK;
 }
