@@ -14,7 +14,7 @@
 //      and runs each wave as one set of multi-join kernels over a flattened index space (build over all
 //      build tuples of the wave, then probe over all probe tuples), so the tables are still in L2 when
 //      probed;
-//   3. enqueues the partitioned joins on kPhjLanes streams forked from the first (each with its own
+//   3. enqueues the partitioned joins on up to kPhjLanes streams forked from the first (each with its own
 //      scratch area; largest joins first, each on the least loaded stream), so they overlap the waves
 //      and each other;
 //   4. captures the whole sequence in a CUDA graph once (parallel branches), so a run is one graph
