@@ -44,6 +44,21 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
     return pol;
 }
 
+// Read-only load that L2 keeps as long as it can (a relation read twice in a row: the second read is
+// served from L2).
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ tuple_v ld_keep(const tuple_v *p) {
+    tuple_v v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+                 : "=l"(v.x), "=l"(v.y)
+                 : "l"(p), "l"(policy_evict_last()));
+    return v;
+}
+
 // Streaming 16-byte load that skips L1 and marks the L2 line evict-first: every input tuple of a
 // partition pass or probe is read exactly once.
 __device__ __forceinline__ tuple_v ld_stream(const tuple_v *p) {
