@@ -366,36 +366,48 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
         CU_OR(cudaGraphLaunch(ge->exec, st), out->status = HJ_E_DEVICE);
         launches = ge->launches;
     } else if (graphable && key == c->last_key) {
-        // Second identical call in a row: capture, instantiate, launch; keep the graph.
-        CU_OR(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), out->status = HJ_E_DEVICE);
-        rc = enqueue();
-        cudaGraph_t graph = nullptr;
-        const cudaError_t ce = cudaStreamEndCapture(st, &graph);
-        cudaGraphExec_t exec = nullptr;
-        if (!rc && ce == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
-            if (c->graphs.size() >= kMaxJoinGraphs) {
-                size_t lru = 0;
-                for (size_t i = 1; i < c->graphs.size(); i++)
-                    if (c->graphs[i].used < c->graphs[lru].used) lru = i;
-                cudaGraphExecDestroy(c->graphs[lru].exec);
-                c->graphs.erase(c->graphs.begin() + (long)lru);
+        // Second identical call in a row: capture, instantiate, launch; keep the graph. If the capture
+        // or the instantiation fails, the join runs its kernels directly instead.
+        bool ran = false;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const int crc = enqueue();
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            cudaGraphExec_t exec = nullptr;
+            if (!crc && ce == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess &&
+                cudaGraphLaunch(exec, st) == cudaSuccess) {
+                if (c->graphs.size() >= kMaxJoinGraphs) {
+                    size_t lru = 0;
+                    for (size_t i = 1; i < c->graphs.size(); i++)
+                        if (c->graphs[i].used < c->graphs[lru].used) lru = i;
+                    cudaGraphExecDestroy(c->graphs[lru].exec);
+                    c->graphs.erase(c->graphs.begin() + (long)lru);
+                }
+                hj_graph_entry e;
+                e.key = key;
+                e.exec = exec;
+                e.launches = launches;
+                e.used = ++c->graph_tick;
+                c->graphs.push_back(e);
+                ran = true;
+            } else if (exec) {
+                cudaGraphExecDestroy(exec);
             }
-            hj_graph_entry e;
-            e.key = key;
-            e.exec = exec;
-            e.launches = launches;
-            e.used = ++c->graph_tick;
-            c->graphs.push_back(e);
-        } else if (!rc) {
-            rc = HJ_E_DEVICE;
+            if (graph) cudaGraphDestroy(graph);
+            if (crc && crc != HJ_E_DEVICE) {  // an argument the enqueue rejects: the same without a graph
+                cudaGetLastError();
+                return out->status = crc;
+            }
         }
-        if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
-        if (rc) {
-            if (exec) cudaGraphExecDestroy(exec);
-            return out->status = rc;
+        if (!ran) {
+            launches = 0;
+            rc = enqueue();
+            if (rc) {
+                cudaStreamSynchronize(st);
+                return out->status = rc;
+            }
         }
-        CU_OR(cudaGraphLaunch(exec, st), out->status = HJ_E_DEVICE);
     } else {
         rc = enqueue();
         if (rc) {
