@@ -62,11 +62,13 @@ HJ_F_NO_TIMING = 0x1
 HJ_F_PINNED_HOST = 0x2
 HJ_RES_COMPACT_PARTITIONS = 0x1
 HJ_RES_WORD_PASS1 = 0x2
+HJ_RES_ORDERED_PASSES = 0x4  # phj_radix_lp ran with ordered partition passes
 HJ_F_PHASE_TIMES = 0x4
 HJ_F_SEGMENTS = 0x20  # radix joins counting every match: segment mode at any size
 HJ_F_EXACT = 0x40     # radix joins: always the histogram pass and exact pass-1 offsets
 HJ_F_WIDE = 0x80      # radix joins: 16-byte tuples in every partition pass (no 8-byte words)
 HJ_F_WORDS = 0x200    # radix joins: 8-byte words in every pass whenever the widths allow
+HJ_F_ORDERED = 0x400  # phj_radix_lp: ordered partition passes at once (no unordered first run)
 PHASES = ("hist", "plan", "pass1", "pass2", "join", "large")
 
 
@@ -196,7 +198,7 @@ def _ptr_len(rel, on_device: bool):
 
 
 def make_params(bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
-                stream: int | None = None, flags: int = 0, load: float = 0.5, bits_pass1: int = 0,
+                stream: int | None = None, flags: int = 0, load: float = 0.0, bits_pass1: int = 0,
                 watchdog_ms: int = 0) -> Params:
     p = Params()
     lib().hj_params_init(ctypes.byref(p))
@@ -211,7 +213,7 @@ def make_params(bits: int = 14, passes: int = 2, device: int = 0, on_device: boo
 
 
 def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, on_device: bool = False,
-         stream: int | None = None, flags: int = 0, load: float = 0.5, ctx: "Context | None" = None,
+         stream: int | None = None, flags: int = 0, load: float = 0.0, ctx: "Context | None" = None,
          check: bool = True, bits_pass1: int | None = None, watchdog_ms: int = 0) -> Result:
     """Run one join (synchronous). Raises JoinError on a non-zero status when check is set.
     bits_pass1: pass-1 radix bits of a two-pass join (None: 11 for phj_asymm_radix_* names, as the
@@ -236,7 +238,7 @@ def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, o
 
 def join_mat(algo: str, R, S, *, pairs=None, pair_cap: int | None = None, bits: int = 14, passes: int = 2,
              device: int = 0, on_device: bool = False, stream: int | None = None, flags: int = 0,
-             load: float = 0.5, ctx: "Context | None" = None, check: bool = True,
+             load: float = 0.0, ctx: "Context | None" = None, check: bool = True,
              bits_pass1: int | None = None) -> Result:
     """Materialising join (the reference's ptr_* joins; a "ptr_" prefix on algo is accepted): one
     (r.row_id, s.row_id) pair per match, checksum recomputed by the retrieve phase. pairs: None (kept
@@ -266,7 +268,7 @@ def join_mat(algo: str, R, S, *, pairs=None, pair_cap: int | None = None, bits: 
 
 
 def join_streamed(algo: str, R, S, ctx: "Context", *, chunk_tuples: int = 0, bits: int = 14, passes: int = 2,
-                  flags: int = 0, load: float = 0.5, check: bool = True, bits_pass1: int | None = None) -> Result:
+                  flags: int = 0, load: float = 0.0, check: bool = True, bits_pass1: int | None = None) -> Result:
     """Streamed join (hj_join_streamed): R stays on the device, S streams from host memory in chunks.
     R and S are host relations: numpy (n, 2) uint64 arrays or (pointer, n) pairs (pinned memory copies
     at full link speed)."""

@@ -53,7 +53,7 @@ void resolve_params(const hj_params_t *p, hj_params_t *out) {
     if (p) *out = *p;
     if (out->num_radix_bits == 0) out->num_radix_bits = 14;
     if (out->num_passes == 0) out->num_passes = 2;
-    if (!(out->table_load > 0.0)) out->table_load = 0.5;
+    if (!(out->table_load > 0.0)) out->table_load = 0.0;  // the size-dependent default (nphj_default_load)
 }
 
 bool is_phj(hj_algo_t a) { return hj::algo_is_phj(a); }
@@ -134,7 +134,7 @@ void hj_params_init(hj_params_t *p) {
     memset(p, 0, sizeof(*p));
     p->num_radix_bits = 14;
     p->num_passes = 2;
-    p->table_load = 0.5;
+    p->table_load = 0.0;
 }
 
 const char *hj_status_str(int s) {
@@ -321,6 +321,14 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
         dR = r;
         dS = s;
     }
+    // phj_radix_lp: first with unordered partition passes (phj_radix_bc's ranks), then, only if a probe
+    // tuple matched two build tuples (the first match then depends on the order inside a partition),
+    // again with ordered ones. The second run needs the first one's flag on the host, so these joins
+    // are not captured into a graph; a build relation that needed it runs ordered at once next time.
+    const bool lp_try = is_phj(algo) && hj::algo_lp(algo) && !(p.flags & (HJ_F_ORDERED | HJ_F_TEST_STALL)) &&
+                        p.watchdog_ms <= 0 && !(c->lp_ordered_R == (const void *)R && c->lp_ordered_nR == nR);
+    const bool lp_ordered = is_phj(algo) && hj::algo_lp(algo) && !lp_try;
+    bool lp_rerun = false;
     // Everything from the result reset to the result copy; a repeated device-resident join replays it
     // from a CUDA graph (the key holds every input of the enqueued work).
     auto enqueue = [&]() -> int {
@@ -330,10 +338,23 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
         if (is_phj(algo)) {
             hj::PhjScratch s;
             hj::phj_carve(geom, nR, nS, c->num_sms, cur, &s, seg);
-            erc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
-                                  timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches, nullptr,
-                                  ((p.flags & HJ_F_TEST_STALL) ? 1 : 0) | ((p.flags & HJ_F_WIDE) ? 2 : 0) |
-                                      ((p.flags & HJ_F_WORDS) ? 4 : 0));
+            const int tf = ((p.flags & HJ_F_TEST_STALL) ? 1 : 0) | ((p.flags & HJ_F_WIDE) ? 2 : 0) |
+                           ((p.flags & HJ_F_WORDS) ? 4 : 0);
+            uint32_t first = 0;
+            if (lp_try) {
+                erc = hj::phj_enqueue(geom, true, hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
+                                      timing ? c->ev_mid : nullptr, c->num_sms, ph, &first, nullptr, tf, false);
+                if (erc) return erc;
+                if (cudaMemcpyAsync(c->acc_host, acc, sizeof(JoinAccum), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess)
+                    return HJ_E_DEVICE;
+                lp_rerun = c->acc_host->dup_flag != 0;
+                if (lp_rerun && cudaMemsetAsync(acc, 0, sizeof(JoinAccum), st) != cudaSuccess) return HJ_E_DEVICE;
+            }
+            if (!lp_try || lp_rerun)
+                erc = hj::phj_enqueue(geom, hj::algo_lp(algo), hj::algo_skip0(algo), dR, nR, dS, nS, s, acc, st,
+                                      timing ? c->ev_mid : nullptr, c->num_sms, ph, &launches, nullptr, tf);
+            launches += first;
         } else {
             const size_t tb = c->arena_bytes - (size_t)(cur - c->arena);
             erc = hj::nphj_enqueue(hj::algo_lp(algo), false, dR, nR, dS, nS, cur, tb, p.table_load, acc, st,
@@ -346,7 +367,7 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
         return HJ_OK;
     };
     hj_graph_key key;
-    const bool graphable = !host_in && st == c->stream && !(p.flags & HJ_F_TEST_STALL);
+    const bool graphable = !host_in && st == c->stream && !(p.flags & HJ_F_TEST_STALL) && !lp_try;
     if (graphable) {
         key.algo = (int)algo;
         key.R = R;
@@ -434,6 +455,11 @@ int hj_join_ctx(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *pin, const hj_tu
     out->checksum = c->acc_host->checksum;
     out->large_partitions = c->acc_host->large_parts;
     out->flags = (uint32_t)c->acc_host->flags;
+    if (lp_ordered || lp_rerun) out->flags |= HJ_RES_ORDERED_PASSES;
+    if (lp_rerun) {
+        c->lp_ordered_R = R;
+        c->lp_ordered_nR = nR;
+    }
     if (timing) {
         float a = 0, b = 0, h = 0;
         cudaEventElapsedTime(&a, c->ev_start, c->ev_mid);

@@ -55,5 +55,9 @@ struct hj_ctx {
     std::vector<hj_graph_entry> graphs;
     hj_graph_key last_key;              // the previous join's key (a repeat triggers the capture)
     uint64_t graph_tick = 0;
+    // phj_radix_lp: the last build relation whose unordered first run found a probe tuple with two
+    // build matches; its next joins on this context run with ordered passes at once.
+    const void *lp_ordered_R = nullptr;
+    size_t lp_ordered_nR = 0;
     std::mutex mu;
 };

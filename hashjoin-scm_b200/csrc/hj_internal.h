@@ -106,15 +106,19 @@ void phj_carve(const RadixGeom &g, size_t nR, size_t nS, int num_sms, char *base
 // ev_mid, if non-null, is recorded between the partition phase and the join phase.
 // ph, if non-null, holds HJ_PH_COUNT + 1 events recorded at the phase boundaries (in segment mode,
 // see phj_phase_span, in a different order); *launches receives the number of kernels enqueued.
-// A scratch carved for segment mode runs in segment mode unless lp is set; lp then runs the
-// exact-offset pipeline, which a segment-mode scratch does not fit: carve it with seg = false.
+// A scratch carved for segment mode runs in segment mode, else the exact-offset pipeline.
 // mat, if non-null, makes the join write one (r.row_id, s.row_id) pair per match into mat->pairs
 // (slots counted in acc->pairs) instead of summing row ids. test_flags bit 0: the partition pass's
-// first CTA withholds one tile load, so its bounded wait expires (failure-detection tests).
+// first CTA withholds one tile load, so its bounded wait expires (failure-detection tests); bit 1:
+// 16-byte tuples in every pass; bit 2: 8-byte words in every pass the widths allow.
+// ordered (first-match joins, lp): true keeps each final build partition in input order (stable ranks),
+// so the lowest position among equal keys is the first in input order. false ranks the build relation
+// as the all-matches joins do; the result is then right unless a probe tuple matched two build tuples,
+// which the joins record in acc->dup_flag: the caller then runs the join again with ordered = true.
 int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
                 int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat = nullptr,
-                int test_flags = 0);
+                int test_flags = 0, bool ordered = true);
 
 // The events of phase slot i (HJ_PH_*) that phj_enqueue recorded: elapsed(ph[*from], ph[*to]);
 // false for a slot that the mode does not time (segment mode has no histogram pass).
@@ -135,6 +139,8 @@ inline bool phj_phase_span(bool seg_mode, int i, int *from, int *to) {
 // Non-partitioned joins on a global open-addressing table.
 // mat: as for phj_enqueue; a materialising join needs nphj_scratch_bytes(nR, load, true).
 size_t nphj_scratch_bytes(size_t nR, double load, bool mat = false);
+// The load factor a table_load of 0 (or outside (0.05, 0.95)) selects for a build relation of nR tuples.
+double nphj_default_load(size_t nR);
 // Shared-memory attributes of the non-partitioned join's kernels on the current device (idempotent;
 // call before capturing nphj_enqueue in a graph).
 int nphj_prepare_device();

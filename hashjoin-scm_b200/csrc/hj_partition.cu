@@ -1117,9 +1117,9 @@ __global__ void __launch_bounds__(THREADS, MINB) scatter_kernel(ScatterArgs a) {
         // compact final partitions). Full tiles load their staged tuples in two halves so that the stores
         // issue back to back.
         // A destination outside the output (negative included) fails the unsigned bound check. Build
-        // key-0 words (first-match joins) exist only in the stable launches of the build relation.
+        // key-0 words exist only for first-match joins (ci_z0), in the launches of the build relation.
         unsigned long long *out8 = sl.out == a.outS ? a.outS8 : a.outR8;
-        const bool z0 = STABLE && a.ci_z0 && sl.out == a.outR;
+        const bool z0 = a.ci_z0 && sl.out == a.outR;
         if (full) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
@@ -1262,7 +1262,9 @@ __device__ __forceinline__ void seg_flush(uint32_t *jh, uint32_t *row, int nbins
 // their tiles stably (warp-ordered ballots, as the stable scatter does), so pass 2, which writes each
 // digit's chains in CTA order and each chain in order, leaves every final build partition in input
 // order. Probe tiles keep the atomic rank: their order inside a partition changes no result.
-template <int THREADS, int ITEMS, int K, bool W8 = false, bool STABLE_R = false>
+// Z0R: build words of key 0 may take the high part 0x80000000 (a.z0, first-match joins, ordered or
+// not); a compile-time switch, since the select per word costs the all-matches joins' pass 1 3%.
+template <int THREADS, int ITEMS, int K, bool W8 = false, bool STABLE_R = false, bool Z0R = STABLE_R>
 __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegArgs a) {
     constexpr int T = THREADS * ITEMS;
     static_assert(T == kTile, "a tile fills one segment of tuples");
@@ -1593,7 +1595,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         __syncthreads();
         // Write each digit run: consecutive threads write consecutive 16-byte tuples (8-byte words).
         // A destination outside the segment storage (negative included) fails the unsigned bound check.
-        const bool z0 = STABLE_R && a.z0 && sl.rel == 0;
+        const bool z0 = Z0R && a.z0 && sl.rel == 0;
         if (cnt == (uint32_t)T) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
@@ -1727,6 +1729,14 @@ __device__ __forceinline__ bool compact_applies(const JoinArgs &a) {
 
 constexpr size_t kCompactSmem = (size_t)kCompactCap * (4 + 4 + 2 + 2);
 
+// First-match joins: record (acc->dup_flag) that some probe tuple of this block matched two or more
+// build tuples. Only then does the first match depend on the order inside a build partition; a join
+// whose partition passes ranked the build relation without keeping its input order is then run again
+// with ordered passes. Called by every thread of the block.
+__device__ __forceinline__ void flag_multi(bool multi, unsigned int *flag) {
+    if (__syncthreads_or(multi) && threadIdx.x == 0) atomicOr(flag, 1u);
+}
+
 // Partition join with 4-byte keys (key >> bits) and 4-byte row ids in shared memory, packed into one
 // 8-byte word per build tuple (key-high << 32 | row id: one load per visited node): 96 KiB per CTA,
 // two CTAs per SM, so one CTA's build overlaps the other's probe. Same results as join_small_kernel;
@@ -1755,6 +1765,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
     constexpr bool lp = LP;
     const bool skip0 = a.skip0 != 0;
     unsigned long long cnt = 0, sum = 0;
+    bool multi = false;  // first-match joins: a probe tuple matched two build tuples
     for (;;) {
         if (tid == 0) s_item = atomicAdd(&a.counters[kCtrItemA], 1u);
         __syncthreads();
@@ -1855,12 +1866,13 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 if (j >= ns) continue;
                 const uint64_t khi = sv[u].x >> B;
                 uint32_t e = head[khi & hmask];
-                uint32_t best = 0, steps = 0;
+                uint32_t best = 0, steps = 0, nm = 0;
                 while (e) {
                     const unsigned long long w = rw[e - 1];
                     if ((w >> 32) == khi) {
                         if (lp) {
                             if (best == 0 || e < best) best = e;
+                            nm++;
                         } else {
                             cnt++;
                             sum += (w & 0xffffffffull) + sv[u].y;
@@ -1875,12 +1887,14 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 if (lp && best) {
                     cnt++;
                     sum += (rw[best - 1] & 0xffffffffull) + sv[u].y;
+                    multi |= nm > 1;
                 }
             }
         }
         __syncthreads();
     }
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
+    if (LP && !MAT) flag_multi(multi, &a.acc->dup_flag);
 }
 
 template <bool MAT, bool CI = false>
@@ -1913,7 +1927,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
     const uint32_t first_item = compact_applies(a) ? a.counters[kCtrNItemsA] : 0u;
     unsigned long long cnt = 0, sum = 0;
     uint32_t phase = 0;
-    bool ok = true;
+    bool ok = true, multi = false;
     for (;;) {
         if (tid == 0) s_item = first_item + atomicAdd(&a.counters[kCtrItem], 1u);
         __syncthreads();
@@ -2028,13 +2042,14 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
                 if (j >= ns) continue;
                 const uint64_t k = s[u].x;
                 uint32_t e = head[(k >> B) & hmask];
-                uint32_t best = 0;
+                uint32_t best = 0, nm = 0;
                 uint32_t steps = 0;
                 while (e) {
                     const tuple_v r = rt[e - 1];
                     if (r.x == k) {
                         if (lp) {
                             if (best == 0 || e < best) best = e;
+                            nm++;
                         } else {
                             cnt++;
                             sum += r.y + s[u].y;
@@ -2049,12 +2064,14 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
                 if (lp && best) {
                     cnt++;
                     sum += rt[best - 1].y + s[u].y;
+                    multi |= nm > 1;
                 }
             }
         }
         __syncthreads();
     }
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
+    if (!MAT) flag_multi(multi, &a.acc->dup_flag);
 }
 
 // Large partitions: chained tables in global memory, one flattened index space for all of them.
@@ -2200,6 +2217,7 @@ __global__ void join_large_probe(JoinArgs a) {
     const int nl = (int)a.counters[kCtrNLarge];
     const uint64_t total = ld_u64_pair(&a.counters[kCtrLargeS]);
     unsigned long long cnt = 0, sum = 0;
+    bool multi = false;  // first-match joins: a probe tuple matched two build tuples
     const bool ci = !MAT && a.ci && ci_applies(a.counters, a.bits);
     const int bshift = ci ? 0 : a.bits;
     if constexpr (MAT) {
@@ -2264,6 +2282,7 @@ __global__ void join_large_probe(JoinArgs a) {
             if (!e) continue;
             if (a.lp) {
                 const uint32_t first = ~t.negpos[e - 1];
+                multi |= t.cnt[e - 1] > 1;
                 if (first < L.r_len) {
                     cnt++;
                     sum += fin_r(a, ci, L.r_begin + first).y + s.y;
@@ -2285,13 +2304,14 @@ __global__ void join_large_probe(JoinArgs a) {
         const uint32_t *head = a.large_table + L.table_off;
         const uint32_t *nxt = head + (1ull << L.nb_log);
         uint32_t e = head[(s.x >> bshift) & ((1ull << L.nb_log) - 1)];
-        uint32_t best = 0;
+        uint32_t best = 0, nm = 0;
         uint64_t steps = 0;
         while (e) {
             const tuple_v r = fin_r(a, ci, L.r_begin + e - 1);
             if (r.x == s.x) {
                 if (a.lp) {
                     if (best == 0 || e < best) best = e;
+                    nm++;
                 } else {
                     cnt++;
                     sum += r.y + s.y;
@@ -2306,9 +2326,11 @@ __global__ void join_large_probe(JoinArgs a) {
         if (a.lp && best) {
             cnt++;
             sum += fin_r(a, ci, L.r_begin + best - 1).y + s.y;
+            multi |= nm > 1;
         }
     }
     block_sum2_to(cnt, sum, red, &a.acc->matched, &a.acc->checksum);
+    if (!MAT) flag_multi(multi, &a.acc->dup_flag);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (nl) atomicAdd(&a.acc->large_parts, (unsigned long long)nl);
         if (ci) atomicOr(&a.acc->flags, (unsigned long long)HJ_RES_COMPACT_PARTITIONS);
@@ -2519,18 +2541,20 @@ int phj_prepare_device() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
-#define HJ_SEG_ATTR(KK, W, ST)                                                                             \
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, ST>,                  \
+#define HJ_SEG_ATTR(KK, W, ST, Z)                                                                          \
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, ST, Z>,               \
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits, ST)))
-#define HJ_SEG_ATTR4(W, ST) \
-    HJ_SEG_ATTR(1, W, ST);  \
-    HJ_SEG_ATTR(2, W, ST);  \
-    HJ_SEG_ATTR(4, W, ST);  \
-    HJ_SEG_ATTR(8, W, ST)
-    HJ_SEG_ATTR4(false, false);
-    HJ_SEG_ATTR4(true, false);
-    HJ_SEG_ATTR4(false, true);
-    HJ_SEG_ATTR4(true, true);
+#define HJ_SEG_ATTR4(W, ST, Z) \
+    HJ_SEG_ATTR(1, W, ST, Z);  \
+    HJ_SEG_ATTR(2, W, ST, Z);  \
+    HJ_SEG_ATTR(4, W, ST, Z);  \
+    HJ_SEG_ATTR(8, W, ST, Z)
+    HJ_SEG_ATTR4(false, false, false);
+    HJ_SEG_ATTR4(true, false, false);
+    HJ_SEG_ATTR4(false, false, true);
+    HJ_SEG_ATTR4(true, false, true);
+    HJ_SEG_ATTR4(false, true, true);
+    HJ_SEG_ATTR4(true, true, true);
 #undef HJ_SEG_ATTR4
 #undef HJ_SEG_ATTR
     HJ_CU(cudaFuncSetAttribute(
@@ -2561,8 +2585,11 @@ int phj_prepare_device() {
 
 int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, size_t nR, const ulonglong2 *S,
                 size_t nS, const PhjScratch &s, JoinAccum *acc, cudaStream_t st, cudaEvent_t ev_mid,
-                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat, int test_flags) {
+                int num_sms, cudaEvent_t *ph, uint32_t *launches, const MatOut *mat, int test_flags,
+                bool ordered) {
     uint32_t nlaunch = 0;
+    // Stable ranks of the build relation: first-match joins that keep the input order.
+    const bool stable = lp && ordered;
 #define HJ_PH(i) \
     if (ph) HJ_CU(record_event(ph[i], st))
     if (nR >= (1ull << 32) || nS >= (1ull << 32)) return HJ_E_INVAL;
@@ -2626,12 +2653,15 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         ga.b1 = g.b1;
         ga.w8_first = 0;
         ga.z0 = skip0 ? 1 : 0;
-        // First-match joins keep every build partition in input order (the stable build-relation form).
-        const size_t sm = seg_smem_bytes(g.bits, lp);
+        // Ordered first-match joins keep every build partition in input order (the stable build-relation form).
+        const size_t sm = seg_smem_bytes(g.bits, stable);
         auto launch_pass1 = [&](bool words) {
 #define HJ_SEG_LAUNCH_W(KK, W)                                                                                   \
-    if (lp)                                                                                                      \
+    if (stable)                                                                                                  \
         seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, true><<<s.seg_grid, kScatterThreads, sm, st>>>(ga); \
+    else if (skip0)                                                                                              \
+        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, false, true>                                     \
+            <<<s.seg_grid, kScatterThreads, sm, st>>>(ga);                                                       \
     else                                                                                                         \
         seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, false><<<s.seg_grid, kScatterThreads, sm, st>>>(ga)
 #define HJ_SEG_LAUNCH(KK)         \
@@ -2761,9 +2791,9 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
             }
 #undef HJ_SCATTER
         };
-        if (lp) {
-            // First-match joins need each final build partition in input order (the join keeps the
-            // lowest position among equal keys), so the build relation's items take the stable rank.
+        if (stable) {
+            // Ordered first-match joins need each final build partition in input order (the join keeps
+            // the lowest position among equal keys), so the build relation's items take the stable rank.
             // The probe relation's order inside a partition changes nothing (each probe tuple finds its
             // first match on its own), so its items take the cheaper atomic rank, in a second launch.
             const uint32_t per_chunk = pass == 0 ? cg.spc : (uint32_t)F1;

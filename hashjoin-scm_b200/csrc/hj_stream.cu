@@ -32,7 +32,7 @@ size_t stream_need(hj_algo_t algo, const hj_params_t &p, const hj::RadixGeom &g,
     if (hj::algo_is_phj(algo))
         need += hj::phj_scratch_bytes(g, nR, chunk, num_sms);
     else
-        need += a256(hj::nphj_scratch_bytes(nR, p.table_load > 0 ? p.table_load : 0.5));
+        need += a256(hj::nphj_scratch_bytes(nR, p.table_load));
     return need;
 }
 
@@ -49,7 +49,7 @@ extern "C" int hj_join_streamed(hj_ctx_t *c, hj_algo_t algo, const hj_params_t *
     if (pin) p = *pin;
     if (p.num_radix_bits == 0) p.num_radix_bits = 14;
     if (p.num_passes == 0) p.num_passes = 2;
-    if (!(p.table_load > 0.0)) p.table_load = 0.5;
+    if (!(p.table_load > 0.0)) p.table_load = 0.0;  // the size-dependent default
     if (p.device != c->device || p.inputs_on_device) return out->status = HJ_E_INVAL;  // host relations only
     hj::RadixGeom g = {};
     if (hj::algo_is_phj(algo)) {

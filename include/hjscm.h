@@ -87,7 +87,9 @@ typedef struct {
     int inputs_on_device; /* 1: R and S are device pointers; 0: host pointers (copied inside) */
     void *stream;         /* cudaStream_t to run on; NULL selects the context's own stream */
     uint32_t flags;       /* HJ_F_* bits */
-    double table_load;    /* NPHJ global table load factor (0 selects 0.5) */
+    double table_load;    /* NPHJ global table load factor; 0 selects 0.4 for build relations of up to
+                             5 M tuples (about L2-sized tables, where shorter probe chains pay) and 0.5
+                             above */
     int radix_bits_pass1; /* two passes: bits of pass 1 (NUM_RADIX_BITS_PASS1 of phj_asymm_radix,
                              src/algo/phj_asymm_radix.h:10-19); 0 selects bits / 2. Clamped to the
                              split where each pass has 1..8 bits. */
@@ -116,6 +118,13 @@ typedef struct {
 /* Test hook for failure detection: the first partition pass of a radix join withholds one tile load,
  * so a bounded device wait (2 s) expires and the join returns HJ_E_TIMEOUT; the context stays usable. */
 #define HJ_F_TEST_STALL  0x100u
+/* phj_radix_lp keeps the first match in input order among equal build keys. It first runs with the
+ * partition passes of phj_radix_bc (no order kept), and the joins note whether any probe tuple matched
+ * two build tuples; only then is the first match order-dependent, and the join runs again with ordered
+ * passes (each build partition in input order, stable ranks). A build relation that needed this runs
+ * ordered at once in its next joins on the same context (same pointer and size). Both runs together
+ * are one join: one result, and its times include both. HJ_F_ORDERED runs the ordered passes at once. */
+#define HJ_F_ORDERED     0x400u
 
 /* hj_result_t.phase[] slots (seconds), filled with HJ_F_PHASE_TIMES. PHJ: histogram, plan, partition
  * pass 1, partition pass 2, shared-memory partition joins, global-memory (large) partition joins
@@ -152,6 +161,9 @@ typedef struct {
  * row id as well (every build key >> pass-1 bits below 2^31, every row id below 2^32), so pass 1 wrote
  * 8 bytes per tuple and pass 2 read 8. */
 #define HJ_RES_WORD_PASS1 0x2u
+/* hj_result_t.flags: phj_radix_lp ran with ordered partition passes (see HJ_F_ORDERED): asked for, a
+ * probe tuple with two build matches in the first run, or an earlier join of the same build relation. */
+#define HJ_RES_ORDERED_PASSES 0x4u
 
 typedef struct hj_ctx hj_ctx_t;
 

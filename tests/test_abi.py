@@ -47,7 +47,7 @@ def test_params_defaults(hj):
     p = hj.Params()
     hj.lib().hj_params_init(ctypes.byref(p))
     assert (p.num_radix_bits, p.num_passes, p.device, p.inputs_on_device, p.flags) == (14, 2, 0, 0, 0)
-    assert p.table_load == 0.5
+    assert p.table_load == 0.0  # the size-dependent default
 
 
 @pytest.mark.parametrize("dup,payload", [(1, False), (1, True), (4, False)])
