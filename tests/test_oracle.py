@@ -162,6 +162,40 @@ def test_key_zero_rule(oracle):
     assert oracle.join(oracle.FIRST_NP, R, S) == (2, 5 + 100 + 7 + 200)
 
 
+def test_first_match_needs_order_only_for_multi_match_probes(oracle):
+    """The invariant phj_radix_lp's unordered first run rests on: when no probe tuple matches two build
+    tuples (key 0 never matches), the first-match result equals the all-matches result over the build
+    relation without key 0, in every build order; when one does, some order changes it."""
+    rng = np.random.default_rng(17)
+    for case in range(6):
+        nR, nS = 3000, 7000
+        R = np.empty((nR, 2), dtype=np.uint64)
+        R[:, 0] = rng.permutation(np.arange(1, 2 * nR + 1, dtype=np.uint64))[:nR]
+        R[:, 1] = rng.integers(0, 1 << 40, nR, dtype=np.uint64)
+        R[::41, 0] = 0
+        if case >= 3:  # duplicate build keys; the probes of cases 3 and 4 avoid them
+            R[nR // 2: nR // 2 + 50, 0] = R[1:51, 0]
+        S = np.empty((nS, 2), dtype=np.uint64)
+        S[:, 0] = R[rng.integers(0, nR, nS), 0]
+        S[::9, 0] = 0
+        S[:, 1] = rng.integers(0, 1 << 40, nS, dtype=np.uint64)
+        keys, counts = np.unique(R[R[:, 0] != 0, 0], return_counts=True)
+        dups = keys[counts > 1]
+        if case in (3, 4):
+            S = S[~np.isin(S[:, 0], dups)]
+        multi = bool(np.isin(S[:, 0], dups).any())
+        assert multi == (case == 5)
+        nz = R[R[:, 0] != 0]
+        want = oracle.join(oracle.FIRST, R, S)
+        for _ in range(3):
+            perm = rng.permutation(nR)
+            got = oracle.join(oracle.FIRST, R[perm], S)
+            if not multi:
+                assert got == want == oracle.join(oracle.ALL, nz, S)
+        if multi:  # reversing the build relation picks the other tuple of a probed duplicate key
+            assert oracle.join(oracle.FIRST, R[::-1], S) != want
+
+
 @pytest.mark.skipif(not _REF_SOURCES, reason="reference sources absent")
 def test_oracle_matches_reference_binary_random(oracle):
     """Random keys with heavy duplication, straight through the reference's own joins."""
