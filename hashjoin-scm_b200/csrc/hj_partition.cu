@@ -57,7 +57,8 @@ struct JoinItem {
     uint64_t s_begin;  // index into the final S buffer
     uint32_t r_len;
     uint32_t s_len;
-    uint32_t pad[2];
+    uint32_t part0;    // 1: the partition of the keys whose radix bits are 0 (key 0's partition)
+    uint32_t pad;
 };
 
 struct LargePart {
@@ -66,7 +67,7 @@ struct LargePart {
     uint64_t table_off;  // u32 words into the large table: head[nb] then next[r_len]
     uint64_t r_flat, s_flat;
     uint32_t nb_log;
-    uint32_t pad;
+    uint32_t part0;  // as JoinItem::part0
 };
 
 // counters[] slots
@@ -97,9 +98,11 @@ enum : int {
 // word, (key >> bits) << 32 | row id, and the joins read 8 bytes per tuple instead of 16. Inside a
 // final partition the low `bits` key bits are equal, so comparing key >> bits compares keys. A probe
 // key whose high part is 2^31 or more is stored as 0xffffffff: no build key has that high part. Joins
-// where a build key 0 never matches (lp_join's empty-slot rule) store that key's words with high part
-// 0x80000000, which no build key and no probe word has (ci_word_z0). The
-// widths are ORed together by the pass that reads the relations first (hist_chunk_kernel or
+// where a build key 0 never matches (lp_join's empty-slot rule): a last pass that reads tuples stores
+// that key's words with high part 0x80000000, which no build key and no probe word has (ci_word_z0);
+// from segment-mode pass-1 words it keeps high part 0, and since key 0 lies in the partition of the
+// keys whose radix bits are 0, where a high part of 0 means key 0, the joins skip such build words
+// there (JoinItem::part0). The widths are ORed together by the pass that reads the relations first (hist_chunk_kernel or
 // seg_pass1_kernel), so the choice is made on the device, before the last pass.
 __device__ __forceinline__ bool ci_applies(const uint32_t *counters, int bits) {
     const unsigned long long *mx = reinterpret_cast<const unsigned long long *>(counters + kCtrMaxKey);
@@ -122,9 +125,10 @@ __device__ __forceinline__ unsigned long long w8_word(unsigned long long key, un
     return (h32 << 32) | (rid & 0xffffffffull);
 }
 
-// Build relations whose key 0 never matches (z0): key 0's word takes the high part 0x80000000, which no
-// other build word has; the last pass keeps it (store_elem) and stores every probe word whose high part
-// has bit 31 set as 0xffffffff, so nothing matches it.
+// Build relations whose key 0 never matches (z0), in the exact-offset pipeline's word pass 1: key 0's
+// word takes the high part 0x80000000, which no other build word has; the last pass keeps it
+// (store_elem) and stores every probe word whose high part has bit 31 set as 0xffffffff, so nothing
+// matches it. (Segment mode's pass 1 stores key 0 as any key; the joins skip it in its partition.)
 __device__ __forceinline__ unsigned long long w8_word_z0(unsigned long long key, unsigned long long rid, int b1,
                                                          bool z0) {
     return z0 && key == 0 ? (0x80000000ull << 32) | (rid & 0xffffffffull) : w8_word(key, rid, b1);
@@ -478,7 +482,8 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
                     it.r_len = (uint32_t)nr;
                     const uint64_t rem = ns - (uint64_t)q * kProbeChunk;
                     it.s_len = (uint32_t)(rem < (uint64_t)kProbeChunk ? rem : (uint64_t)kProbeChunk);
-                    it.pad[0] = it.pad[1] = 0;
+                    it.part0 = v == 0 ? 1u : 0u;
+                    it.pad = 0;
                     a.items[item_idx] = it;
                 } else {
                     atomicOr(&a.counters[kCtrErr], kErrCapacity);
@@ -494,7 +499,7 @@ __global__ void __launch_bounds__(1024, 1) plan_kernel(PlanArgs a) {
                 uint32_t nb_log = 0;
                 while ((1ull << nb_log) < nr) nb_log++;
                 lp.nb_log = nb_log;
-                lp.pad = 0;
+                lp.part0 = v == 0 ? 1u : 0u;
                 lp.table_off = 0;
                 lp.r_flat = lp.s_flat = 0;
                 a.large[large_idx] = lp;
@@ -1191,7 +1196,6 @@ struct SegArgs {
     uint32_t *hist;            // [2*grid][2^bits]: row c = R tuples of CTA c, row grid + c = its S tuples
     uint32_t *counters;        // kCtrItem1 (items), kCtrSegAlloc, kCtrErr, kCtrMaxKey/kCtrMaxRid
     int test_stall;            // test hook: CTA 0 withholds its first tile load (its wait must expire)
-    int z0;                    // build key 0 never matches: its words take the high part 0x80000000
 };
 
 struct SegSlot {
@@ -1262,9 +1266,9 @@ __device__ __forceinline__ void seg_flush(uint32_t *jh, uint32_t *row, int nbins
 // their tiles stably (warp-ordered ballots, as the stable scatter does), so pass 2, which writes each
 // digit's chains in CTA order and each chain in order, leaves every final build partition in input
 // order. Probe tiles keep the atomic rank: their order inside a partition changes no result.
-// Z0R: build words of key 0 may take the high part 0x80000000 (a.z0, first-match joins, ordered or
-// not); a compile-time switch, since the select per word costs the all-matches joins' pass 1 3%.
-template <int THREADS, int ITEMS, int K, bool W8 = false, bool STABLE_R = false, bool Z0R = STABLE_R>
+// Build key 0 of first-match joins needs nothing here: its word (high part 0) reaches key 0's final
+// partition, whose joins skip it (JoinItem::part0); a select per word cost pass 1 3%.
+template <int THREADS, int ITEMS, int K, bool W8 = false, bool STABLE_R = false>
 __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegArgs a) {
     constexpr int T = THREADS * ITEMS;
     static_assert(T == kTile, "a tile fills one segment of tuples");
@@ -1595,7 +1599,6 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
         __syncthreads();
         // Write each digit run: consecutive threads write consecutive 16-byte tuples (8-byte words).
         // A destination outside the segment storage (negative included) fails the unsigned bound check.
-        const bool z0 = Z0R && a.z0 && sl.rel == 0;
         if (cnt == (uint32_t)T) {
 #pragma unroll
             for (int hh = 0; hh < 2; hh++) {
@@ -1613,7 +1616,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 for (int i = 0; i < ITEMS / 2; i++) {
                     if ((uint64_t)dst[i] < cap) {
                         if (W8)
-                            st_stream8(out8 + dst[i], w8_word_z0(t[i].x, t[i].y, a.b1, z0));
+                            st_stream8(out8 + dst[i], w8_word(t[i].x, t[i].y, a.b1));
                         else
                             st_stream(a.out + dst[i], t[i]);
                     } else {
@@ -1628,7 +1631,7 @@ __global__ void __launch_bounds__(THREADS, kSegCtasPerSm) seg_pass1_kernel(SegAr
                 const long long dst = (j < r.split ? r.base : r.base2) + (long long)j;
                 if ((uint64_t)dst < cap) {
                     if (W8)
-                        st_stream8(out8 + dst, w8_word_z0(t.x, t.y, a.b1, z0));
+                        st_stream8(out8 + dst, w8_word(t.x, t.y, a.b1));
                     else
                         st_stream(a.out + dst, t);
                 } else {
@@ -1794,7 +1797,7 @@ __global__ void __launch_bounds__(kCompactThreads, 2) join_compact_kernel(JoinAr
                 const uint32_t i = i0 + u * kCompactThreads;
                 if (i >= nr) continue;
                 rw[i] = ((t[u].x >> B) << 32) | (t[u].y & 0xffffffffull);
-                if (!ci && skip0 && t[u].x == 0) continue;
+                if (skip0 && t[u].x == 0 && (!ci || item.part0)) continue;
                 nxt[i] = (uint16_t)atomic_exch_u16(&head[(t[u].x >> B) & hmask], i + 1);
             }
         }
@@ -1973,7 +1976,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1) join_small_kernel(JoinArgs a)
         // Build: chain every R tuple (lp_join skips key 0, which reads as an empty slot there).
         for (uint32_t i = tid; i < nr; i += kJoinThreads) {
             const uint64_t k = rt[i].x;
-            if (!ci && skip0 && k == 0) continue;
+            if (skip0 && k == 0 && (!ci || item.part0)) continue;
             const uint32_t h = (uint32_t)((k >> B) & hmask);
             nxt[i] = (uint16_t)atomic_exch_u16(&head[h], i + 1);
         }
@@ -2168,7 +2171,7 @@ __global__ void join_large_build(JoinArgs a) {
                 l = find_large(a.large, nl, g, true);
                 i = g - a.large[l].r_flat;
                 r = fin_r(a, ci, a.large[l].r_begin + i);
-                act = !(a.skip0 && !ci && r.x == 0);
+                act = !(a.skip0 && r.x == 0 && (!ci || a.large[l].part0));
             }
             const unsigned act_mask = __ballot_sync(0xffffffffu, act);
             if (!act) continue;
@@ -2201,7 +2204,7 @@ __global__ void join_large_build(JoinArgs a) {
         const LargePart &L = a.large[l];
         const uint64_t i = g - L.r_flat;
         const uint64_t k = fin_r(a, ci, L.r_begin + i).x;
-        if (a.skip0 && !ci && k == 0) continue;
+        if (a.skip0 && k == 0 && (!ci || L.part0)) continue;
         uint32_t *head = a.large_table + L.table_off;
         uint32_t *nxt = head + (1ull << L.nb_log);
         const uint64_t h = (k >> bshift) & ((1ull << L.nb_log) - 1);
@@ -2541,20 +2544,18 @@ int phj_prepare_device() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
     HJ_CU(cudaFuncSetAttribute(scatter_kernel<kScatterThreads, kScatterItems, false, kScatterBufs, kScatterCtasPerSm>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scatter_smem));
-#define HJ_SEG_ATTR(KK, W, ST, Z)                                                                          \
-    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, ST, Z>,               \
+#define HJ_SEG_ATTR(KK, W, ST)                                                                             \
+    HJ_CU(cudaFuncSetAttribute(seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, ST>,                  \
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_smem_bytes(kSegMaxBits, ST)))
-#define HJ_SEG_ATTR4(W, ST, Z) \
-    HJ_SEG_ATTR(1, W, ST, Z);  \
-    HJ_SEG_ATTR(2, W, ST, Z);  \
-    HJ_SEG_ATTR(4, W, ST, Z);  \
-    HJ_SEG_ATTR(8, W, ST, Z)
-    HJ_SEG_ATTR4(false, false, false);
-    HJ_SEG_ATTR4(true, false, false);
-    HJ_SEG_ATTR4(false, false, true);
-    HJ_SEG_ATTR4(true, false, true);
-    HJ_SEG_ATTR4(false, true, true);
-    HJ_SEG_ATTR4(true, true, true);
+#define HJ_SEG_ATTR4(W, ST) \
+    HJ_SEG_ATTR(1, W, ST);  \
+    HJ_SEG_ATTR(2, W, ST);  \
+    HJ_SEG_ATTR(4, W, ST);  \
+    HJ_SEG_ATTR(8, W, ST)
+    HJ_SEG_ATTR4(false, false);
+    HJ_SEG_ATTR4(true, false);
+    HJ_SEG_ATTR4(false, true);
+    HJ_SEG_ATTR4(true, true);
 #undef HJ_SEG_ATTR4
 #undef HJ_SEG_ATTR
     HJ_CU(cudaFuncSetAttribute(
@@ -2652,16 +2653,12 @@ int phj_enqueue(const RadixGeom &g, bool lp, bool skip0, const ulonglong2 *R, si
         ga.test_stall = (test_flags & 1) ? 1 : 0;
         ga.b1 = g.b1;
         ga.w8_first = 0;
-        ga.z0 = skip0 ? 1 : 0;
         // Ordered first-match joins keep every build partition in input order (the stable build-relation form).
         const size_t sm = seg_smem_bytes(g.bits, stable);
         auto launch_pass1 = [&](bool words) {
 #define HJ_SEG_LAUNCH_W(KK, W)                                                                                   \
     if (stable)                                                                                                  \
         seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, true><<<s.seg_grid, kScatterThreads, sm, st>>>(ga); \
-    else if (skip0)                                                                                              \
-        seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, false, true>                                     \
-            <<<s.seg_grid, kScatterThreads, sm, st>>>(ga);                                                       \
     else                                                                                                         \
         seg_pass1_kernel<kScatterThreads, kScatterItems, KK, W, false><<<s.seg_grid, kScatterThreads, sm, st>>>(ga)
 #define HJ_SEG_LAUNCH(KK)         \

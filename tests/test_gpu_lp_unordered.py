@@ -82,22 +82,29 @@ def test_duplicates_no_probe_hits_stay_unordered(hj, oracle, cuda):
     assert not r.flags & hj.HJ_RES_ORDERED_PASSES
 
 
-def test_key_zero_never_matches_in_the_unordered_run(hj, oracle, cuda):
-    """Build key 0 is lp_join's empty slot: it never matches, in the unordered run too, also when it
-    occurs many times and probes carry it (no order dependence: none of them matches)."""
+@pytest.mark.parametrize("pipeline", list(PIPELINES))
+def test_key_zero_never_matches(hj, oracle, cuda, pipeline):
+    """Build key 0 is lp_join's empty slot: it never matches, in the unordered and the ordered passes,
+    also when it occurs many times and probes carry it (no order dependence: none of them matches).
+    Other keys of key 0's partition (radix bits 0, small high parts) must still match."""
     rng = np.random.default_rng(44)
     R = unique_build(rng, 120_000, 1 << 22)
     R[::97, 0] = 0
+    # 2^22 + k * 2^14: radix bits 0 (key 0's partition), high parts 2^8 + k, no other build key
+    R[5:25, 0] = np.uint64(1 << 22) + (np.arange(1, 21, dtype=np.uint64) << np.uint64(14))
     S = probes(rng, R, 400_000, kmax=1 << 22)
     S[::13, 0] = 0
+    S[::17, 0] = R[5 + (np.arange(S[::17].shape[0]) % 20), 0]
     for rid_bits in (32, 48):  # compact words; 16-byte final partitions
         R2 = R.copy()
         R2[:, 1] = rng.integers(0, 1 << rid_bits, R.shape[0], dtype=np.uint64)
-        with hj.Context(0) as ctx:
-            r = run(hj, cuda, ctx, R2, S, 0)
-        assert (r.matched_cnt, r.checksum) == oracle.join("phj_radix_lp", R2, S), rid_bits
-        assert not r.flags & hj.HJ_RES_ORDERED_PASSES
-        assert bool(r.flags & hj.HJ_RES_COMPACT_PARTITIONS) == (rid_bits == 32)
+        want = oracle.join("phj_radix_lp", R2, S)
+        for flags in (0, hj.HJ_F_ORDERED, hj.HJ_F_WORDS, hj.HJ_F_ORDERED | hj.HJ_F_WORDS):
+            with hj.Context(0) as ctx:
+                r = run(hj, cuda, ctx, R2, S, flags | PIPELINES[pipeline])
+            assert (r.matched_cnt, r.checksum) == want, (rid_bits, flags)
+            assert bool(r.flags & hj.HJ_RES_ORDERED_PASSES) == bool(flags & hj.HJ_F_ORDERED)
+            assert bool(r.flags & hj.HJ_RES_COMPACT_PARTITIONS) == (rid_bits == 32)
 
 
 def test_ordered_flag_and_wide_tuples(hj, oracle, cuda):
