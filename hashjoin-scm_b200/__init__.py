@@ -217,7 +217,8 @@ def join(algo: str, R, S, *, bits: int = 14, passes: int = 2, device: int = 0, o
          check: bool = True, bits_pass1: int | None = None, watchdog_ms: int = 0) -> Result:
     """Run one join (synchronous). Raises JoinError on a non-zero status when check is set.
     bits_pass1: pass-1 radix bits of a two-pass join (None: 11 for phj_asymm_radix_* names, as the
-    reference's NUM_RADIX_BITS_PASS1 default, else an even split)."""
+    reference's NUM_RADIX_BITS_PASS1 default, else an even split). load: the non-partitioned joins'
+    table load factor (0: 0.4 for build relations up to 5 M tuples, 0.5 above)."""
     L = lib()
     a = ALGOS[algo]
     if bits_pass1 is None:
