@@ -170,8 +170,13 @@ def test_python_flag_constants_match_header(hj):
     import re
     text = (hj.HERE.parent / "include" / "hjscm.h").read_text()
     defs = {m.group(1): int(m.group(2), 16) for m in re.finditer(r"#define (HJ_F_\w+)\s+0x([0-9a-fA-F]+)u", text)}
-    assert {"HJ_F_SEGMENTS", "HJ_F_EXACT", "HJ_F_PHASE_TIMES", "HJ_F_TEST_STALL"} <= set(defs)
+    assert {"HJ_F_SEGMENTS", "HJ_F_EXACT", "HJ_F_PHASE_TIMES", "HJ_F_TEST_STALL", "HJ_F_ORDERED"} <= set(defs)
     for name, value in defs.items():
         if hasattr(hj, name):
             assert getattr(hj, name) == value, name
     assert len(set(defs.values())) == len(defs)  # no two flags share a bit
+    res = {m.group(1): int(m.group(2), 16) for m in re.finditer(r"#define (HJ_RES_\w+)\s+0x([0-9a-fA-F]+)u", text)}
+    assert {"HJ_RES_COMPACT_PARTITIONS", "HJ_RES_WORD_PASS1", "HJ_RES_ORDERED_PASSES"} <= set(res)
+    for name, value in res.items():
+        assert getattr(hj, name) == value, name
+    assert len(set(res.values())) == len(res)
