@@ -398,6 +398,7 @@ def run_ours(a, rank, world, local_rank):
     step_s = ms / 1e3 / a.steps
     compact = bool(results[-1].flags & hj.HJ_RES_COMPACT_PARTITIONS)
     words1 = bool(results[-1].flags & hj.HJ_RES_WORD_PASS1)
+    ordered = bool(results[-1].flags & hj.HJ_RES_ORDERED_PASSES)
     if a.algo.startswith("phj"):
         P = results[-1].physical_passes
         # bytes per tuple of each pass: read + write; 8-byte words halve what a pass writes (and what the
@@ -446,6 +447,7 @@ def run_ours(a, rank, world, local_rank):
     pipe_bytes = per_tuple * (nR + nS)
     pipeline = {"algorithmic_bytes_per_tuple": per_tuple, "bytes_per_step": pipe_bytes,
                 "compact_final_partitions": compact, "word_pass1": words1 if a.algo.startswith("phj") else False,
+                "ordered_passes": ordered,
                 "achieved_gbs": pipe_bytes / step_s / 1e9, "frac": pipe_bytes / step_s / 1e9 / peak,
                 "phase_ms": {k: v * 1e3 for k, v in phases.items()}}
 
