@@ -23,27 +23,43 @@ def table_hash(key, cap):
     return (h * cap) >> 64
 
 
-def staging_fits(nR):
+def default_load(nR):
+    """nphj_default_load: the table load factor a table_load of 0 selects."""
+    return 0.4 if nR <= 5_000_000 else 0.5
+
+
+def table_cap(nR, load):
+    """nphj_cap: 16-byte table slots for nR build tuples."""
+    return int(nR / load) + 2
+
+
+def compact_used(nR, load):
+    """nphj_enqueue's compact_ok for a join without per-match output or the key-0 rule: the 16-byte table
+    would exceed 64 MB."""
+    return table_cap(nR, load) * 16 > (64 << 20)
+
+
+def staging_fits(nR, load=0.5):
     """The host's test (nphj_enqueue): the compact table, the staging areas and the fill counters fit in the
     16-byte table's bytes. True for every table the sliced build is used for (above 64 MB the rounding of
     the capacity to whole slices is below 0.2%); small or badly rounded tables build without slices."""
     a256 = lambda x: (x + 255) // 256 * 256
-    cap = int(nR / 0.5) + 2
+    cap = table_cap(nR, load)
     ccap = (cap + SLICE - 1) // SLICE * SLICE
     ns = ccap // SLICE
     return a256(ccap * 8) + a256(ns * MAX_FILL * 8) + ns * 4 <= cap * 16
 
 
-def sliced_join(R, S, hist_blocks, lp=False, claim_seed=0):
+def sliced_join(R, S, hist_blocks, lp=False, claim_seed=0, load=0.5):
     nR = R.shape[0]
-    cap = int(nR / 0.5) + 2
+    cap = table_cap(nR, load)
     ccap = (cap + SLICE - 1) // SLICE * SLICE
     ns = ccap // SLICE
     keys = [int(k) for k in R[:, 0]]
     rids = [int(r) for r in R[:, 1]]
     sl = [table_hash(k, ccap) >> SLICE_LOG for k in keys]
     assert all(0 <= x < ns for x in sl)
-    assert staging_fits(nR)  # otherwise the host builds without slices
+    assert staging_fits(nR, load)  # otherwise the host builds without slices
     # pass 1 of nphj_slice_scatter: block b counts its contiguous range [b*per, min(nR, (b+1)*per))
     per = (nR + hist_blocks - 1) // hist_blocks
     hist = np.zeros((hist_blocks, ns), dtype=np.int64)
@@ -128,7 +144,39 @@ def test_sliced_build_index_arithmetic(oracle, nR, nS, hist_blocks, dups, lp):
 
 
 def test_staging_fits_every_table_the_sliced_build_is_used_for():
-    # compact tables are used above 64 MB of 16-byte slots (nR > 2^21)
+    # compact tables are used above 64 MB of 16-byte slots (nR > 2^21 at load 0.5)
     for nR in (1 << 21, (1 << 21) + 1, 3_000_001, 1 << 22, 10**7 + 7, 1 << 26):
         assert staging_fits(nR), nR
     assert not staging_fits(30_001)  # a small, badly rounded table: the host builds without slices
+    # the default load factors (0.4 up to 5 M build tuples, 0.5 above) and a few others, over sizes
+    # from 2^20 to 2^30: wherever the compact table is used, the staging fits
+    for load in (None, 0.3, 0.4, 0.5, 0.7):
+        for nR in np.unique(np.geomspace(1 << 20, 1 << 30, 400).astype(np.int64)).tolist() + [5_000_000, 5_000_001]:
+            ld = default_load(nR) if load is None else load
+            if compact_used(nR, ld):
+                assert staging_fits(nR, ld), (nR, ld)
+
+
+def test_expected_slice_fill_at_the_default_loads():
+    """A slice holds kSliceSlots * load build tuples on average; its staging area holds 7/8 of the slice.
+    With uniform hashing over many slices the fill is about Poisson, so at load 0.5 the area's bound lies
+    48 standard deviations above the mean and at 0.4 68: only repeated keys overflow a slice (then the
+    global-CAS build runs)."""
+    for load, sigmas in ((0.4, 68), (0.5, 48)):
+        mean = SLICE * load
+        assert round((MAX_FILL - mean) / mean ** 0.5) == sigmas, load
+
+
+def test_sliced_build_at_load_0_4(oracle):
+    """The index arithmetic at the small-table default load, on a table large enough for its staging."""
+    rng = np.random.default_rng(5)
+    nR, nS = 60_000, 90_000
+    assert staging_fits(nR, 0.4)
+    R = np.empty((nR, 2), dtype=np.uint64)
+    R[:, 0] = rng.integers(1, 1 << 31, nR, dtype=np.uint64)
+    R[:, 1] = rng.integers(0, 1 << 32, nR, dtype=np.uint64)
+    S = np.empty((nS, 2), dtype=np.uint64)
+    S[:, 0] = R[rng.integers(0, nR, nS), 0]
+    S[:, 1] = rng.integers(0, 1 << 40, nS, dtype=np.uint64)
+    for lp in (False, True):
+        assert sliced_join(R, S, 37, lp, 3, load=0.4) == oracle.join("nphj_lp" if lp else "nphj_sc", R, S)
