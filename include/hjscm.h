@@ -121,9 +121,10 @@ typedef struct {
 /* phj_radix_lp keeps the first match in input order among equal build keys. It first runs with the
  * partition passes of phj_radix_bc (no order kept), and the joins note whether any probe tuple matched
  * two build tuples; only then is the first match order-dependent, and the join runs again with ordered
- * passes (each build partition in input order, stable ranks). A build relation that needed this runs
- * ordered at once in its next joins on the same context (same pointer and size). Both runs together
- * are one join: one result, and its times include both. HJ_F_ORDERED runs the ordered passes at once. */
+ * passes (each build partition in input order, stable ranks). The context remembers the last build
+ * relation (pointer and size) that needed this; its next joins there run ordered at once. Both runs
+ * together are one join: one result, and its times include both. Such joins are not replayed from a
+ * CUDA graph. HJ_F_ORDERED runs the ordered passes at once. */
 #define HJ_F_ORDERED     0x400u
 
 /* hj_result_t.phase[] slots (seconds), filled with HJ_F_PHASE_TIMES. PHJ: histogram, plan, partition
